@@ -1,0 +1,448 @@
+#!/usr/bin/env python
+"""Benchmark of the per-step microenvironment update on B200 GPUs.
+
+One step is the reference driver's loop body (paraBioFVM src/main.cpp:68-107): LOD diffusion
+(x, y, z Thomas sweeps with the Dirichlet overwrites), the central-difference gradient, and
+secretion/uptake, with the agent binning rebuilt every 10th step.  The default workload is the
+large plain configuration: a 320 x 320 x 320 mesh (dx = 20 um), 16 FP32 substrates, 1,000,000 agents
+in 32 Gaussian clusters, Dirichlet 1.0 for substrate 0 on every face and 1 % of the interior voxels
+pinned to U(0,1) values; all data seeded and synthetic.
+
+Reported: ``value`` = voxel*substrate updates per second over all GPUs, device-timed with CUDA
+events on the solver's stream over ``--steps`` graph-replayed steps (inputs stay resident; the 2.1
+GB field is far larger than L2, so no flush is needed); ``e2e`` = the same metric through the C ABI
+with pinned host buffers (state stored, steps called one solver at a time, field, gradients and
+internalized substrates loaded back, all inside the timed region); ``roofline`` of the dominant
+kernel; ``cpu_baseline`` = the CPU oracle on the host cores.  ``--impl reference`` times the CPU
+restatement of the reference's host solvers (the reference itself cannot be built in this image).
+
+Multi-GPU: the plain single-mesh step does not shard (its z sweep couples the whole mesh), so
+``--gpus N`` runs N independent replicas, one per GPU (weak scaling, no collective on the data
+path); the device time is the maximum over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # the large plain configuration (headline)
+    "plain-320": dict(edge=320, S=16, agents=1_000_000, clustered=True, sigma=200.0, interior_fraction=0.01,
+                      seed=20261203,
+                      text="320^3 voxels (dx 20 um) x 16 FP32 substrates, 1,000,000 agents in 32 Gaussian clusters "
+                           "(sigma 200 um), 1% interior Dirichlet voxels, Dirichlet 1.0 on substrate 0 at all faces, "
+                           "dt 0.01 min, binning rebuilt every 10th step"),
+    # the CPU-runnable configuration (parity case, L2-resident)
+    "plain-50": dict(edge=50, S=4, agents=5000, clustered=False, sigma=0.0, interior_fraction=0.0, seed=11,
+                     text="50^3 voxels x 4 FP32 substrates, 5,000 uniform agents, Dirichlet 1.0 on substrate 0 at "
+                          "all faces, dt 0.01 min"),
+}
+
+METRIC = "voxel·substrate steps/s, % HBM peak; speedup vs plain GPU at ≤1e-3 rel L2"
+UNIT = "voxel*substrate updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(name, seed_offset=0):
+    from parabiofvm_b200.workloads import synthetic
+
+    w = WORKLOADS[name]
+    return synthetic(w["edge"], w["S"], w["agents"], w["seed"] + seed_offset, clustered=w["clustered"],
+                     sigma=w["sigma"] or 200.0, interior_fraction=w["interior_fraction"])
+
+
+def algorithmic_step_bytes(w, recompute_fraction=0.1):
+    """Bytes a step must move at minimum: 3 sweeps x (read + write) + gradient written, 4 B each
+    per voxel*substrate (36 B), plus the agent terms (per-voxel reductions read, density
+    read-modify-write, internalized intermediates and read-modify-write) and the Dirichlet data."""
+    VS = w.voxel_count * w.S
+    A = w.agents.count if w.agents is not None else 0
+    n_d = 0 if w.interior_voxels is None else len(w.interior_voxels)
+    agent = A * w.S * (20 + (20 if w.compute_internalized else 0)) + 16 * A
+    recompute = recompute_fraction * A * w.S * (16 + 24)
+    return 36 * VS + agent + recompute + 5 * n_d * w.S
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"bfvm_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [t.strip() for t in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+def physical_gpu_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [t.strip() for t in vis.split(",") if t.strip()]
+        if local_rank < len(ids):
+            return ids[local_rank]
+    return str(local_rank)
+
+
+def cpu_oracle_rate(w, budget_s=20.0, max_steps=3):
+    """Time the CPU oracle (all host threads) on the workload: voxel*substrate updates/s."""
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    from oracle import Oracle
+
+    o = Oracle(w.dims, w.bbox_min, w.bbox_max, w.voxel_shape, w.diffusion_coefficients, w.decay_rates, w.time_step,
+               w.initial_conditions, w.compute_internalized, dtype=np.float32)
+    for (dim, is_max), (vals, conds) in w.boundary.items():
+        o.set_boundary_dirichlet(dim, is_max, vals, conds)
+    if w.interior_voxels is not None:
+        o.set_interior_dirichlet(w.interior_voxels, w.interior_values, w.interior_conditions)
+    o.set_densities(w.densities)
+    a = w.agents
+    o.set_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates, a.internalized,
+                 a.fraction_released, a.volumes, a.positions)
+    o.initialize()
+    times = []
+    total = 0.0
+    step = 0
+    while step < max_steps and (total < budget_s or step == 0):
+        t0 = time.perf_counter()
+        o.run_steps(1, step)
+        dt = time.perf_counter() - t0
+        times.append(dt)
+        total += dt
+        step += 1
+    o.close()
+    VS = w.voxel_count * w.S
+    return VS * len(times) / total, threads, times
+
+
+def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's host step on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    t_setup = time.perf_counter()
+    w = make_workload(args.workload)
+    log(f"reference arm: workload built in {time.perf_counter() - t_setup:.1f}s")
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    from oracle import Oracle
+
+    o = Oracle(w.dims, w.bbox_min, w.bbox_max, w.voxel_shape, w.diffusion_coefficients, w.decay_rates, w.time_step,
+               w.initial_conditions, w.compute_internalized, dtype=np.float32)
+    for (dim, is_max), (vals, conds) in w.boundary.items():
+        o.set_boundary_dirichlet(dim, is_max, vals, conds)
+    if w.interior_voxels is not None:
+        o.set_interior_dirichlet(w.interior_voxels, w.interior_values, w.interior_conditions)
+    o.set_densities(w.densities)
+    a = w.agents
+    o.set_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates, a.internalized,
+                 a.fraction_released, a.volumes, a.positions)
+    o.initialize()
+    # warm-up steps, then as many timed steps of --steps as fit in the time budget
+    t_step = None
+    for i in range(args.warmup):
+        t0 = time.perf_counter()
+        o.run_steps(1, i)
+        t_step = time.perf_counter() - t0
+    budget = args.reference_budget_s
+    timed = args.steps if t_step is None else max(1, min(args.steps, int(budget // max(t_step, 1e-9))))
+    t0 = time.perf_counter()
+    o.run_steps(timed, args.warmup)
+    elapsed = time.perf_counter() - t0
+    VS = w.voxel_count * w.S
+    value = VS * timed / elapsed
+    sample = (f"{timed} of {args.steps} requested full steps of the workload after {args.warmup} warm-up steps "
+              f"(time budget {budget:.0f}s)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(args.gpus),
+        "steps": timed, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / timed, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['text']}",
+                   "implementation": "CPU restatement of src/solver/host (OpenMP, -O3, no FP contraction)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        log(f"note: WORLD_SIZE={world} differs from --gpus {args.gpus}; using WORLD_SIZE")
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+
+    from parabiofvm_b200.workloads import make_solver
+
+    t_setup = time.perf_counter()
+    w = make_workload(args.workload, seed_offset=rank)
+    log(f"rank {rank}: workload built in {time.perf_counter() - t_setup:.1f}s")
+    stream = torch.cuda.Stream()
+    s = make_solver(w, device=local_rank)
+    s.set_stream(stream.cuda_stream)
+    VS = w.voxel_count * w.S
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident steps, graph replay
+    s.run_steps(args.warmup, 0)
+    s.synchronize()
+    sampler = ClockSampler(physical_gpu_index(local_rank))
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = s.launch_count
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.run_steps(args.steps, args.warmup)
+    ev1.record(stream)
+    s.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = s.launch_count - launches0
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * VS * args.steps / (ms / 1e3)
+
+    # ---- per-kernel timing on the same stream (the roofline numerator)
+    kernels = {}
+    reps = args.kernel_reps
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    names = ["sweep_x", "sweep_y", "sweep_z"]
+    for axis in range(w.dims):
+        kernels[names[axis]] = {"ms": timed(lambda: s.sweep(axis)), "bytes": 8 * VS}
+    kernels["gradient"] = {"ms": timed(s.gradient), "bytes": (4 + 4 * w.dims) * VS}
+    A = w.agents.count
+    kernels["secretion"] = {"ms": timed(lambda: s.secretion(False)),
+                            "bytes": A * w.S * (12 + 8 + (20 if w.compute_internalized else 0))}
+    kernels["secretion_rebin"] = {"ms": timed(lambda: s.secretion(True)), "bytes": None}
+    s.synchronize()
+    peak, peak_kind = measured_peak()
+    for k in kernels.values():
+        k["gbs"] = (k["bytes"] / (k["ms"] / 1e3) / 1e9) if k["bytes"] else None
+    dom = max((n for n in kernels if n.startswith("sweep") or n == "gradient"), key=lambda n: kernels[n]["ms"])
+    traffic = committed_traffic().get(dom)
+    achieved = kernels[dom]["gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs (copy)",
+                "algorithmic_bytes_per_launch": kernels[dom]["bytes"]}
+    step_bytes = algorithmic_step_bytes(w)
+    step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
+    step_hbm = {"algorithmic_bytes": step_bytes, "achieved_gbs": step_gbs, "frac_of_measured": step_gbs / peak,
+                "frac_of_8000": step_gbs / 8000.0}
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.skip_e2e:
+        pinned = lambda n: torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()  # noqa: E731
+        field_in = pinned(VS)
+        field_in[:] = w.densities
+        a = w.agents
+        ag = {}
+        for key in ("secretion_rates", "saturation_densities", "uptake_rates", "net_export_rates", "internalized",
+                    "fraction_released", "volumes", "positions"):
+            arr = np.asarray(getattr(a, key), np.float32).reshape(-1)
+            ag[key] = pinned(arr.size)
+            ag[key][:] = arr
+        field_out = pinned(VS)
+        grad_out = pinned(VS * w.dims)
+        intern_out = pinned(A * w.S)
+        h2d = field_in.nbytes + sum(v.nbytes for v in ag.values())
+        d2h = field_out.nbytes + grad_out.nbytes + intern_out.nbytes
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.store_densities(field_in)
+        s.store_agents(ag["secretion_rates"], ag["saturation_densities"], ag["uptake_rates"], ag["net_export_rates"],
+                       ag["internalized"], ag["fraction_released"], ag["volumes"], ag["positions"])
+        for k in range(args.steps):
+            s.diffusion()
+            s.gradient()
+            s.secretion(k % 10 == 0)
+        s.load_densities(field_out)
+        s.load_gradients(grad_out)
+        s.load_internalized(intern_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": world * VS * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+               "ms_total": e2e_ms,
+               "what": "store field + agents from pinned memory, per step diffusion/gradient/secretion calls through "
+                       "the C ABI, load field + gradients + internalized substrates; totals divided over the steps"}
+        del field_in, field_out, grad_out, intern_out, ag
+
+    s.close()
+    del s
+    torch.cuda.empty_cache()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        rate, threads, times = cpu_oracle_rate(w, budget_s=args.cpu_budget_s)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{len(times)} full step(s) of the same workload on {threads} host threads "
+                         f"({', '.join(f'{t:.2f}s' for t in times)})"}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    w_text = WORKLOADS[args.workload]["text"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.workload}: {w_text}", "grid": list(w.grid), "substrates": w.S,
+                   "agents": w.agents.count,
+                   "interior_dirichlet_voxels": 0 if w.interior_voxels is None else len(w.interior_voxels),
+                   "l2": "inputs larger than L2 (2.1 GB field per sweep), no flush" if VS * 4 > 126e6 else
+                         "L2-resident parity workload",
+                   "parallelism": f"{world} independent replica(s), one per GPU"},
+        "roofline": roofline,
+        "step_hbm": step_hbm,
+        "kernels": kernels,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plain-320")
+    ap.add_argument("--kernel-reps", type=int, default=5)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    ap.add_argument("--reference-budget-s", type=float, default=150.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        log("warm-up raised to 3 steps")
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

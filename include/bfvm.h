@@ -1,0 +1,145 @@
+/*
+ * bfvm.h -- C ABI of the B200 microenvironment solver (libbfvm_cuda.so).
+ *
+ * One bfvm_solver holds one microenvironment on one GPU: the substrate field, its gradients, the
+ * Dirichlet conditions, the agents' secretion/uptake data and the precomputed solver state.  The
+ * entry points mirror the device solver of paraBioFVM (paths relative to that project's root):
+ *
+ *   solver::initialize / store_data_to_solver / load_data_from_solver / wait_for_all
+ *                                        src/solver/device/CUDA/solver.cpp:7-23
+ *   diffusion_solver::solve              src/solver/host/diffusion_solver.cpp:60-70, 512-544
+ *   dirichlet_solver::solve              src/solver/host/dirichlet_solver.cpp:143-151
+ *   gradient_solver::solve               src/solver/host/gradient_solver.cpp:275-291
+ *   cell_solver::simulate_secretion_and_uptake / release_internalized_substrates
+ *                                        src/solver/host/cell_solver.cpp:272-346
+ *
+ * Memory layouts are the reference's (src/traits.h:9-93): densities [z][y][x][s] with the
+ * substrate index fastest; gradients [x][s][1] (1D), [y][x][s][2] (2D), [3][z][y][x][s] (3D);
+ * agent arrays [agent][substrate], volumes [agent], positions [agent][dims].  All values are
+ * 32-bit floats (the reference's default real_t), indices 32-bit ints.
+ *
+ * Calls are ordered on the solver's CUDA stream and return before the GPU finishes unless they
+ * say otherwise; a solver is not safe to use from two host threads at once.  Every function
+ * returns a bfvm_status; on failure bfvm_last_error() describes the problem.  Nothing aborts the
+ * process.
+ */
+#ifndef BFVM_H
+#define BFVM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bfvm_solver bfvm_solver;
+
+typedef enum bfvm_status
+{
+	BFVM_OK = 0,
+	BFVM_ERR_INVALID_ARGUMENT = 1, /* bad size, index, pointer or mesh */
+	BFVM_ERR_OUT_OF_MEMORY = 2,    /* device or pinned host allocation failed */
+	BFVM_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+	BFVM_ERR_NO_DEVICE = 4,        /* no usable CUDA device / library built for another arch */
+	BFVM_ERR_STATE = 5,            /* call out of order (e.g. agents not stored) */
+	BFVM_ERR_AGENT_OUTSIDE = 6     /* an agent position maps outside the mesh */
+} bfvm_status;
+
+/* Message for the last failing call on this host thread ("" if none). */
+const char* bfvm_last_error(void);
+const char* bfvm_status_string(int status);
+/* Library version as major*10000 + minor*100 + patch. */
+int bfvm_version(void);
+
+/*
+ * Create a solver on CUDA device `device` (replaces microenvironment_builder::build + solver::
+ * initialize, src/microenvironment_builder.cpp:146-193, src/solver/device/CUDA/solver.cpp:7-13).
+ * The mesh follows cartesian_mesh (src/mesh.cpp:7-30): grid_shape[d] = ceil((max-min)/voxel).
+ * diffusion_coefficients and decay_rates hold `substrates` values.  The field starts at zero.
+ */
+int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_box_mins[3],
+				const int32_t bounding_box_maxs[3], const int32_t voxel_shape[3], int32_t substrates,
+				float time_step, const float* diffusion_coefficients, const float* decay_rates,
+				int compute_internalized_substrates);
+int bfvm_destroy(bfvm_solver* s);
+
+/* grid_shape[3] as computed from the mesh; voxel count; substrate count; dims. */
+int bfvm_get_shape(const bfvm_solver* s, int32_t grid_shape[3], int64_t* voxel_count, int32_t* substrates,
+				   int32_t* dims);
+
+/* Run the solver's work on `stream` (a cudaStream_t; NULL = the solver's own stream). */
+int bfvm_set_stream(bfvm_solver* s, void* stream);
+
+/*
+ * Boundary Dirichlet conditions of one face (microenvironment.h:47-50): `dim` 0..dims-1,
+ * `is_max` 0 for the min face.  values/conditions hold `substrates` entries; values == NULL removes
+ * the face.  Faces are applied x-min, x-max, y-min, y-max, z-min, z-max, later faces winning
+ * (src/solver/host/dirichlet_solver.cpp:91-141).
+ */
+int bfvm_set_boundary_dirichlet(bfvm_solver* s, int dim, int is_max, const float* values, const uint8_t* conditions);
+
+/*
+ * Interior Dirichlet voxels (microenvironment.h:41-44): voxels [count][dims], values and
+ * conditions [count][substrates].  Replaces any previous set; count == 0 clears.  Applied after
+ * the faces; a voxel listed twice takes, per substrate, the last listed condition that is set.
+ */
+int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* voxels, const float* values,
+								const uint8_t* conditions);
+
+/* Host <-> device copies of the field (solver::store/load_data_to/from_solver). load_* wait for
+ * the stream and check the device error flags before returning. */
+int bfvm_store_densities(bfvm_solver* s, const float* host_densities);
+int bfvm_load_densities(bfvm_solver* s, float* host_densities);
+int bfvm_load_gradients(bfvm_solver* s, float* host_gradients);
+
+/*
+ * Replace the agent set (device_context::copy_to_device, src/solver/device/CUDA/device_context.cpp:
+ * 56-97).  Arrays are [count][substrates] except volumes [count] and positions [count][dims].
+ * fraction_released_at_death may be NULL (taken as zero).  A new agent count forces the next
+ * secretion call to rebuild the voxel binning.
+ */
+int bfvm_store_agents(bfvm_solver* s, int32_t count, const float* secretion_rates, const float* saturation_densities,
+					  const float* uptake_rates, const float* net_export_rates, const float* internalized_substrates,
+					  const float* fraction_released_at_death, const float* volumes, const float* positions);
+int bfvm_load_internalized(bfvm_solver* s, float* host_internalized);
+
+/* One LOD diffusion-decay step with the Dirichlet overwrites between sweeps
+ * (diffusion_solver::solve). */
+int bfvm_diffusion_solve(bfvm_solver* s);
+/* One axis (0 = x, 1 = y, 2 = z) of the diffusion step: the Dirichlet overwrite, that axis's
+ * Thomas sweep, and for the last axis the closing overwrite.  bfvm_diffusion_solve is these calls
+ * for axes 0 .. dims-1 (diffusion_solver.cpp:512-544); one axis alone serves operator-split
+ * orderings and per-kernel timing. */
+int bfvm_diffusion_sweep(bfvm_solver* s, int axis);
+/* Dirichlet overwrite alone (dirichlet_solver::solve). */
+int bfvm_dirichlet_solve(bfvm_solver* s);
+/* Central-difference gradients of the current field (gradient_solver::solve). */
+int bfvm_gradient_solve(bfvm_solver* s);
+/* Secretion and uptake (cell_solver::simulate_secretion_and_uptake); recompute != 0 rebuilds the
+ * per-voxel reductions from the current agent data and positions. */
+int bfvm_secretion_solve(bfvm_solver* s, int recompute);
+/* cell_solver::release_internalized_substrates for agent `index`. */
+int bfvm_release_internalized(bfvm_solver* s, int32_t index);
+
+/*
+ * `steps` full steps of the reference driver's loop (src/main.cpp:68-107): diffusion, gradient,
+ * then secretion with recompute = ((first_step + i) % 10 == 0).  Replayed from CUDA graphs.
+ */
+int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step);
+
+/* Wait for the stream (solver::wait_for_all) and report device-side errors. */
+int bfvm_synchronize(bfvm_solver* s);
+
+/* Device pointers to the resident field and gradients, for zero-copy use by other GPU code. */
+int bfvm_device_densities(bfvm_solver* s, float** ptr, int64_t* count);
+int bfvm_device_gradients(bfvm_solver* s, float** ptr, int64_t* count);
+
+/* Number of this library's kernel launches issued so far on this solver (graph replays count
+ * every kernel node). */
+int bfvm_launch_count(const bfvm_solver* s, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BFVM_H */

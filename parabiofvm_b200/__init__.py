@@ -1,0 +1,176 @@
+"""B200-native microenvironment step for paraBioFVM models.
+
+``Solver`` is a thin Python face of the C ABI (include/bfvm.h): one microenvironment on one GPU
+with the reference solver's operations -- diffusion (LOD Thomas sweeps with the Dirichlet
+overwrites), Dirichlet, gradient, secretion/uptake, release of internalized substrates -- plus a
+graph-captured multi-step driver.  Arrays use the reference's layouts (src/traits.h): densities
+[z][y][x][s]; gradients [x][s][1], [y][x][s][2] or [3][z][y][x][s]; agents [agent][substrate].
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import BfvmError, check
+
+__all__ = ["Solver", "BfvmError", "library_path"]
+
+
+def library_path() -> str:
+    return _abi.LIB_PATH
+
+
+def _f32(a, n=None):
+    arr = np.ascontiguousarray(a, dtype=np.float32).reshape(-1)
+    if n is not None and arr.size != n:
+        raise ValueError(f"expected {n} values, got {arr.size}")
+    return arr
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class Solver:
+    """A microenvironment resident on one GPU (bfvm_create ... bfvm_destroy)."""
+
+    def __init__(self, dims, bbox_min, bbox_max, voxel_shape, diffusion_coefficients, decay_rates, time_step,
+                 compute_internalized=False, device=0):
+        self._lib = _abi.load()
+        self.dims = int(dims)
+        self.S = len(diffusion_coefficients)
+        i3 = lambda v: (ctypes.c_int32 * 3)(*[int(t) for t in list(v) + [0] * (3 - len(v))])  # noqa: E731
+        D = _f32(diffusion_coefficients)
+        lam = _f32(decay_rates, self.S)
+        h = ctypes.c_void_p()
+        check(self._lib.bfvm_create(ctypes.byref(h), int(device), self.dims, i3(bbox_min), i3(bbox_max),
+                                    i3(voxel_shape), self.S, float(time_step), _fp(D), _fp(lam),
+                                    int(bool(compute_internalized))))
+        self._h = h
+        g = (ctypes.c_int32 * 3)()
+        V = ctypes.c_int64()
+        check(self._lib.bfvm_get_shape(self._h, g, ctypes.byref(V), None, None))
+        self.grid = tuple(int(t) for t in g)
+        self.voxel_count = int(V.value)
+        self.agents_count = 0
+
+    # -- lifecycle ------------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bfvm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- Dirichlet ------------------------------------------------------------------------------
+    def set_boundary_dirichlet(self, dim, is_max, values, conditions):
+        if values is None:
+            check(self._lib.bfvm_set_boundary_dirichlet(self._h, int(dim), int(bool(is_max)), None, None))
+            return
+        v = _f32(values, self.S)
+        c = np.ascontiguousarray(conditions, dtype=np.uint8).reshape(-1)
+        check(self._lib.bfvm_set_boundary_dirichlet(self._h, int(dim), int(bool(is_max)), _fp(v),
+                                                    c.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
+    def set_interior_dirichlet(self, voxels, values, conditions):
+        vox = np.ascontiguousarray(voxels, dtype=np.int32).reshape(-1)
+        n = vox.size // self.dims
+        v = _f32(values, n * self.S)
+        c = np.ascontiguousarray(conditions, dtype=np.uint8).reshape(-1)
+        if c.size != n * self.S:
+            raise ValueError("conditions must have count * substrates entries")
+        check(self._lib.bfvm_set_interior_dirichlet(self._h, n, vox.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                    _fp(v), c.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
+    # -- data movement ----------------------------------------------------------------------------
+    def store_densities(self, densities):
+        self._dens_keep = _f32(densities, self.voxel_count * self.S)
+        check(self._lib.bfvm_store_densities(self._h, _fp(self._dens_keep)))
+
+    def load_densities(self, out=None):
+        out = np.empty(self.voxel_count * self.S, np.float32) if out is None else out
+        check(self._lib.bfvm_load_densities(self._h, _fp(out)))
+        return out
+
+    def load_gradients(self, out=None):
+        out = np.empty(self.voxel_count * self.S * self.dims, np.float32) if out is None else out
+        check(self._lib.bfvm_load_gradients(self._h, _fp(out)))
+        return out
+
+    def store_agents(self, secretion_rates, saturation_densities, uptake_rates, net_export_rates, internalized,
+                     fraction_released, volumes, positions):
+        vol = _f32(volumes)
+        n = vol.size
+        arrs = [_f32(a, n * self.S) for a in (secretion_rates, saturation_densities, uptake_rates, net_export_rates,
+                                                internalized)]
+        frac = None if fraction_released is None else _f32(fraction_released, n * self.S)
+        pos = _f32(positions, n * self.dims)
+        self._agents_keep = arrs + [frac, vol, pos]
+        check(self._lib.bfvm_store_agents(self._h, n, *[_fp(a) for a in arrs], _fp(frac) if frac is not None else None,
+                                          _fp(vol), _fp(pos)))
+        self.agents_count = n
+
+    def load_internalized(self, out=None):
+        out = np.empty(self.agents_count * self.S, np.float32) if out is None else out
+        check(self._lib.bfvm_load_internalized(self._h, _fp(out)))
+        return out
+
+    # -- solvers --------------------------------------------------------------------------------
+    def diffusion(self):
+        check(self._lib.bfvm_diffusion_solve(self._h))
+
+    def sweep(self, axis):
+        check(self._lib.bfvm_diffusion_sweep(self._h, int(axis)))
+
+    def dirichlet(self):
+        check(self._lib.bfvm_dirichlet_solve(self._h))
+
+    def gradient(self):
+        check(self._lib.bfvm_gradient_solve(self._h))
+
+    def secretion(self, recompute):
+        check(self._lib.bfvm_secretion_solve(self._h, int(bool(recompute))))
+
+    def release(self, index):
+        check(self._lib.bfvm_release_internalized(self._h, int(index)))
+
+    def run_steps(self, steps, first_step=0):
+        check(self._lib.bfvm_run_steps(self._h, int(steps), int(first_step)))
+
+    def synchronize(self):
+        check(self._lib.bfvm_synchronize(self._h))
+
+    # -- device access ------------------------------------------------------------------------------
+    def set_stream(self, stream_ptr):
+        check(self._lib.bfvm_set_stream(self._h, ctypes.c_void_p(int(stream_ptr)) if stream_ptr else None))
+
+    def device_densities(self):
+        p = ctypes.POINTER(ctypes.c_float)()
+        n = ctypes.c_int64()
+        check(self._lib.bfvm_device_densities(self._h, ctypes.byref(p), ctypes.byref(n)))
+        return ctypes.cast(p, ctypes.c_void_p).value, int(n.value)
+
+    def device_gradients(self):
+        p = ctypes.POINTER(ctypes.c_float)()
+        n = ctypes.c_int64()
+        check(self._lib.bfvm_device_gradients(self._h, ctypes.byref(p), ctypes.byref(n)))
+        return ctypes.cast(p, ctypes.c_void_p).value, int(n.value)
+
+    @property
+    def launch_count(self):
+        n = ctypes.c_int64()
+        check(self._lib.bfvm_launch_count(self._h, ctypes.byref(n)))
+        return int(n.value)

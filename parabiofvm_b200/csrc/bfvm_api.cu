@@ -1,0 +1,657 @@
+// C ABI entry points (include/bfvm.h): solver lifecycle, data movement, solver calls, step graphs.
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bfvm_internal.h"
+
+namespace bfvm {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int status, const std::string& msg)
+{
+	g_last_error = msg;
+	return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+	(void)cudaGetLastError();
+	return fail(BFVM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Sweep block capacity for a line of n elements: 32 registers per block while that keeps the
+// blocks of a line within one CTA (n <= 1024), 64 up to n = 2048.
+static int pick_block_capacity(int n) { return n <= 1024 ? 32 : 64; }
+
+static int upload_plan(bfvm_solver* s, int axis)
+{
+	sweep_plan& p = s->plan[axis];
+	const int n = s->grid[axis];
+	std::vector<float> bp, ep, g, G, c;
+	p.n = n;
+	p.M = pick_block_capacity(n);
+	precompute_axis(n, s->voxel[axis], s->dims, s->S, s->dt, s->D.data(), s->decay.data(), p.M, bp, ep, g, G, c,
+					p.P, p.base_len, p.extra);
+	int st;
+	const size_t nS = (size_t)n * s->S;
+	if ((st = device_alloc(&p.bp, nS)) || (st = device_alloc(&p.eprev, nS)) || (st = device_alloc(&p.g, nS))
+		|| (st = device_alloc(&p.G, nS)) || (st = device_alloc(&p.c, (size_t)s->S)))
+		return st;
+	BFVM_CUDA(cudaMemcpy(p.bp, bp.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(p.eprev, ep.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(p.g, g.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(p.G, G.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(p.c, c.data(), (size_t)s->S * sizeof(float), cudaMemcpyHostToDevice));
+	return BFVM_OK;
+}
+
+static void free_plan(sweep_plan& p)
+{
+	device_free(p.bp);
+	device_free(p.eprev);
+	device_free(p.g);
+	device_free(p.G);
+	device_free(p.c);
+}
+
+static void free_graphs(bfvm_solver* s)
+{
+	for (auto& g : s->step_graph)
+		if (g)
+		{
+			cudaGraphExecDestroy(g);
+			g = nullptr;
+		}
+	s->graphs_dirty = true;
+}
+
+static void free_dirichlet_interior(bfvm_solver* s)
+{
+	device_free(s->dir_bits);
+	device_free(s->dir_rank);
+	device_free(s->dir_vals);
+	device_free(s->dir_conds);
+	s->n_interior = 0;
+}
+
+static void destroy_all(bfvm_solver* s)
+{
+	if (s->device >= 0)
+		cudaSetDevice(s->device);
+	free_graphs(s);
+	for (auto& p : s->plan)
+		free_plan(p);
+	cell_free(s);
+	free_dirichlet_interior(s);
+	device_free(s->face_vals);
+	device_free(s->face_conds);
+	device_free(s->dens);
+	device_free(s->grad);
+	device_free(s->dev_error);
+	if (s->host_error)
+		cudaFreeHost(s->host_error);
+	if (s->own_stream)
+		cudaStreamDestroy(s->own_stream);
+}
+
+static int upload_faces(bfvm_solver* s)
+{
+	const size_t n = 6 * (size_t)s->S;
+	BFVM_CUDA(cudaMemcpyAsync(s->face_vals, s->face_vals_h.data(), n * sizeof(float), cudaMemcpyHostToDevice,
+							  s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(s->face_conds, s->face_conds_h.data(), n, cudaMemcpyHostToDevice, s->stream));
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	return BFVM_OK;
+}
+
+// error flags raised by kernels since the last check
+static int check_device_errors(bfvm_solver* s)
+{
+	BFVM_CUDA(cudaMemcpyAsync(s->host_error, s->dev_error, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	const int e = *s->host_error;
+	if (e)
+	{
+		BFVM_CUDA(cudaMemsetAsync(s->dev_error, 0, sizeof(int), s->stream));
+		if (e & DEVERR_AGENT_OUTSIDE)
+			return fail(BFVM_ERR_AGENT_OUTSIDE, "an agent position lies outside the mesh; it was left out of "
+												"secretion/uptake");
+	}
+	return BFVM_OK;
+}
+
+static int diffusion(bfvm_solver* s)
+{
+	int st;
+	for (int axis = 0; axis < s->dims; axis++)
+		if ((st = launch_sweep(s, axis, axis == s->dims - 1)))
+			return st;
+	return BFVM_OK;
+}
+
+static int one_step(bfvm_solver* s, bool recompute)
+{
+	int st;
+	if ((st = diffusion(s)) || (st = launch_gradient(s)) || (st = launch_secretion(s, recompute)))
+		return st;
+	return BFVM_OK;
+}
+
+} // namespace bfvm
+
+using namespace bfvm;
+
+#define CHECK_SOLVER(s)                                                                                                \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		if (!(s))                                                                                                      \
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "null solver");                                                     \
+		if (cudaSetDevice((s)->device) != cudaSuccess)                                                                 \
+			return cuda_fail(cudaGetLastError(), "cudaSetDevice");                                                     \
+	} while (0)
+
+extern "C" {
+
+const char* bfvm_last_error(void) { return g_last_error.c_str(); }
+
+const char* bfvm_status_string(int status)
+{
+	switch (status)
+	{
+	case BFVM_OK: return "ok";
+	case BFVM_ERR_INVALID_ARGUMENT: return "invalid argument";
+	case BFVM_ERR_OUT_OF_MEMORY: return "out of memory";
+	case BFVM_ERR_CUDA: return "CUDA error";
+	case BFVM_ERR_NO_DEVICE: return "no usable CUDA device";
+	case BFVM_ERR_STATE: return "invalid state";
+	case BFVM_ERR_AGENT_OUTSIDE: return "agent outside the mesh";
+	default: return "unknown status";
+	}
+}
+
+int bfvm_version(void) { return 10000; }
+
+int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_box_mins[3],
+				const int32_t bounding_box_maxs[3], const int32_t voxel_shape[3], int32_t substrates, float time_step,
+				const float* diffusion_coefficients, const float* decay_rates, int compute_internalized_substrates)
+{
+	g_last_error.clear();
+	if (!out)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "out is null");
+	*out = nullptr;
+	if (dims < 1 || dims > 3)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "dims must be 1, 2 or 3");
+	if (!bounding_box_mins || !bounding_box_maxs || !voxel_shape)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "mesh arrays must not be null");
+	if (substrates < 1)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "at least one substrate is required");
+	if (!diffusion_coefficients || !decay_rates)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "diffusion coefficients and decay rates are required");
+	int grid[3] = { 1, 1, 1 };
+	for (int d = 0; d < dims; d++)
+	{
+		if (voxel_shape[d] <= 0)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "voxel_shape must be positive along every used axis");
+		if (bounding_box_maxs[d] <= bounding_box_mins[d])
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "bounding box max must exceed min along every used axis");
+		grid[d] = (bounding_box_maxs[d] - bounding_box_mins[d] + voxel_shape[d] - 1) / voxel_shape[d];
+		if (grid[d] > 2048)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "a mesh axis longer than 2048 voxels is not supported");
+	}
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+	{
+		(void)cudaGetLastError();
+		return fail(BFVM_ERR_NO_DEVICE, "no CUDA device is available");
+	}
+	if (device < 0 || device >= ndev)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "device index out of range");
+
+	auto* s = new (std::nothrow) bfvm_solver();
+	if (!s)
+		return fail(BFVM_ERR_OUT_OF_MEMORY, "host allocation failed");
+	s->device = device;
+	s->dims = dims;
+	for (int d = 0; d < 3; d++)
+	{
+		s->bbox_min[d] = bounding_box_mins[d];
+		s->bbox_max[d] = bounding_box_maxs[d];
+		s->voxel[d] = voxel_shape[d];
+		s->grid[d] = grid[d];
+	}
+	s->S = substrates;
+	s->dt = time_step;
+	s->D.assign(diffusion_coefficients, diffusion_coefficients + substrates);
+	s->decay.assign(decay_rates, decay_rates + substrates);
+	s->internalized = compute_internalized_substrates != 0;
+	s->V = (long long)grid[0] * grid[1] * grid[2];
+	s->face_vals_h.assign(6 * (size_t)substrates, 0.f);
+	s->face_conds_h.assign(6 * (size_t)substrates, 0);
+
+	int st = BFVM_OK;
+	do
+	{
+		if (cudaSetDevice(device) != cudaSuccess)
+		{
+			st = cuda_fail(cudaGetLastError(), "cudaSetDevice");
+			break;
+		}
+		cudaDeviceProp prop;
+		if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+		{
+			st = cuda_fail(cudaGetLastError(), "cudaGetDeviceProperties");
+			break;
+		}
+		if (prop.major != 10)
+		{
+			st = fail(BFVM_ERR_NO_DEVICE, std::string("this library is built for sm_100a; device is ") + prop.name);
+			break;
+		}
+		if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+		{
+			st = cuda_fail(cudaGetLastError(), "cudaStreamCreate");
+			break;
+		}
+		s->stream = s->own_stream;
+		if ((st = device_alloc(&s->dens, (size_t)s->V * s->S)) || (st = device_alloc(&s->grad, (size_t)s->V * s->S * dims))
+			|| (st = device_alloc(&s->face_vals, 6 * (size_t)s->S)) || (st = device_alloc(&s->face_conds, 6 * (size_t)s->S))
+			|| (st = device_alloc(&s->dev_error, 1)))
+			break;
+		if (cudaMallocHost((void**)&s->host_error, sizeof(int)) != cudaSuccess)
+		{
+			(void)cudaGetLastError();
+			st = fail(BFVM_ERR_OUT_OF_MEMORY, "pinned host allocation failed");
+			break;
+		}
+		*s->host_error = 0;
+		if (cudaMemset(s->dens, 0, (size_t)s->V * s->S * sizeof(float)) != cudaSuccess
+			|| cudaMemset(s->grad, 0, (size_t)s->V * s->S * dims * sizeof(float)) != cudaSuccess
+			|| cudaMemset(s->dev_error, 0, sizeof(int)) != cudaSuccess)
+		{
+			st = cuda_fail(cudaGetLastError(), "cudaMemset");
+			break;
+		}
+		for (int d = 0; d < dims && !st; d++)
+			st = upload_plan(s, d);
+		if (st)
+			break;
+		st = upload_faces(s);
+	} while (0);
+
+	if (st)
+	{
+		destroy_all(s);
+		delete s;
+		return st;
+	}
+	*out = s;
+	return BFVM_OK;
+}
+
+int bfvm_destroy(bfvm_solver* s)
+{
+	if (!s)
+		return BFVM_OK;
+	destroy_all(s);
+	delete s;
+	return BFVM_OK;
+}
+
+int bfvm_get_shape(const bfvm_solver* s, int32_t grid_shape[3], int64_t* voxel_count, int32_t* substrates, int32_t* dims)
+{
+	if (!s)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null solver");
+	if (grid_shape)
+		for (int d = 0; d < 3; d++)
+			grid_shape[d] = s->grid[d];
+	if (voxel_count)
+		*voxel_count = s->V;
+	if (substrates)
+		*substrates = s->S;
+	if (dims)
+		*dims = s->dims;
+	return BFVM_OK;
+}
+
+int bfvm_set_stream(bfvm_solver* s, void* stream)
+{
+	CHECK_SOLVER(s);
+	cudaStream_t ns = stream ? (cudaStream_t)stream : s->own_stream;
+	if (ns != s->stream)
+	{
+		BFVM_CUDA(cudaStreamSynchronize(s->stream));
+		s->stream = ns;
+		free_graphs(s);
+	}
+	return BFVM_OK;
+}
+
+int bfvm_set_boundary_dirichlet(bfvm_solver* s, int dim, int is_max, const float* values, const uint8_t* conditions)
+{
+	CHECK_SOLVER(s);
+	if (dim < 0 || dim >= s->dims)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "dim must be in [0, dims)");
+	const int face = 2 * dim + (is_max ? 1 : 0);
+	if (!values)
+	{
+		s->face_mask &= ~(1 << face);
+		for (int k = 0; k < s->S; k++)
+		{
+			s->face_vals_h[(size_t)face * s->S + k] = 0.f;
+			s->face_conds_h[(size_t)face * s->S + k] = 0;
+		}
+	}
+	else
+	{
+		if (!conditions)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "conditions must accompany values");
+		s->face_mask |= 1 << face;
+		for (int k = 0; k < s->S; k++)
+		{
+			s->face_vals_h[(size_t)face * s->S + k] = values[k];
+			s->face_conds_h[(size_t)face * s->S + k] = conditions[k] ? 1 : 0;
+		}
+	}
+	free_graphs(s);
+	return upload_faces(s);
+}
+
+int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* voxels, const float* values,
+								const uint8_t* conditions)
+{
+	CHECK_SOLVER(s);
+	if (count < 0)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "count must not be negative");
+	if (count > 0 && (!voxels || !values || !conditions))
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "voxels, values and conditions are required");
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	free_graphs(s);
+	free_dirichlet_interior(s);
+	if (count == 0)
+		return BFVM_OK;
+
+	const int S = s->S;
+	// merge duplicates in list order: a later listed condition overwrites an earlier one
+	std::map<long long, int> row_of;
+	std::vector<float> vals;
+	std::vector<unsigned char> conds;
+	for (int i = 0; i < count; i++)
+	{
+		int c[3] = { 0, 0, 0 };
+		for (int d = 0; d < s->dims; d++)
+		{
+			c[d] = voxels[(size_t)i * s->dims + d];
+			if (c[d] < 0 || c[d] >= s->grid[d])
+				return fail(BFVM_ERR_INVALID_ARGUMENT, "interior Dirichlet voxel " + std::to_string(i) + " is outside the mesh");
+		}
+		const long long v = c[0] + (long long)s->grid[0] * (c[1] + (long long)s->grid[1] * c[2]);
+		auto it = row_of.find(v);
+		int row;
+		if (it == row_of.end())
+		{
+			row = (int)row_of.size();
+			row_of.emplace(v, row);
+			vals.resize((size_t)(row + 1) * S, 0.f);
+			conds.resize((size_t)(row + 1) * S, 0);
+		}
+		else
+			row = it->second;
+		for (int k = 0; k < S; k++)
+			if (conditions[(size_t)i * S + k])
+			{
+				vals[(size_t)row * S + k] = values[(size_t)i * S + k];
+				conds[(size_t)row * S + k] = 1;
+			}
+	}
+	// rows in voxel order, rank bitmap over linear voxel indices
+	const long long words = (s->V + 31) / 32;
+	std::vector<unsigned int> bits((size_t)words, 0u);
+	std::vector<int> rank((size_t)words, 0);
+	std::vector<float> svals(row_of.size() * (size_t)S);
+	std::vector<unsigned char> sconds(row_of.size() * (size_t)S);
+	int r = 0;
+	for (auto& kv : row_of)
+	{
+		bits[(size_t)(kv.first >> 5)] |= 1u << (kv.first & 31);
+		std::memcpy(&svals[(size_t)r * S], &vals[(size_t)kv.second * S], S * sizeof(float));
+		std::memcpy(&sconds[(size_t)r * S], &conds[(size_t)kv.second * S], S);
+		r++;
+	}
+	int acc = 0;
+	for (long long w = 0; w < words; w++)
+	{
+		rank[(size_t)w] = acc;
+		acc += __builtin_popcount(bits[(size_t)w]);
+	}
+	int st;
+	if ((st = device_alloc(&s->dir_bits, (size_t)words)) || (st = device_alloc(&s->dir_rank, (size_t)words))
+		|| (st = device_alloc(&s->dir_vals, svals.size())) || (st = device_alloc(&s->dir_conds, sconds.size())))
+	{
+		free_dirichlet_interior(s);
+		return st;
+	}
+	BFVM_CUDA(cudaMemcpy(s->dir_bits, bits.data(), bits.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(s->dir_rank, rank.data(), rank.size() * sizeof(int), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(s->dir_vals, svals.data(), svals.size() * sizeof(float), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(s->dir_conds, sconds.data(), sconds.size(), cudaMemcpyHostToDevice));
+	s->n_interior = (int)row_of.size();
+	return BFVM_OK;
+}
+
+int bfvm_store_densities(bfvm_solver* s, const float* host)
+{
+	CHECK_SOLVER(s);
+	if (!host)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
+	BFVM_CUDA(cudaMemcpyAsync(s->dens, host, (size_t)s->V * s->S * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+	return BFVM_OK;
+}
+
+int bfvm_load_densities(bfvm_solver* s, float* host)
+{
+	CHECK_SOLVER(s);
+	if (!host)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
+	BFVM_CUDA(cudaMemcpyAsync(host, s->dens, (size_t)s->V * s->S * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+	return check_device_errors(s);
+}
+
+int bfvm_load_gradients(bfvm_solver* s, float* host)
+{
+	CHECK_SOLVER(s);
+	if (!host)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
+	BFVM_CUDA(cudaMemcpyAsync(host, s->grad, (size_t)s->V * s->S * s->dims * sizeof(float), cudaMemcpyDeviceToHost,
+							  s->stream));
+	return check_device_errors(s);
+}
+
+int bfvm_store_agents(bfvm_solver* s, int32_t count, const float* secretion_rates, const float* saturation_densities,
+					  const float* uptake_rates, const float* net_export_rates, const float* internalized_substrates,
+					  const float* fraction_released_at_death, const float* volumes, const float* positions)
+{
+	CHECK_SOLVER(s);
+	if (count < 0)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "count must not be negative");
+	if (count > 0
+		&& (!secretion_rates || !saturation_densities || !uptake_rates || !net_export_rates || !internalized_substrates
+			|| !volumes || !positions))
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "agent arrays must not be null");
+	const bool resized = count != s->ag.count;
+	if (resized || count > s->ag.capacity)
+	{
+		BFVM_CUDA(cudaStreamSynchronize(s->stream));
+		free_graphs(s);
+	}
+	int st;
+	if (count == 0)
+	{
+		s->ag.count = 0;
+		s->ag.binned = false;
+		return BFVM_OK;
+	}
+	if ((st = cell_alloc(s, count)))
+		return st;
+	agent_state& a = s->ag;
+	const size_t AS = (size_t)count * s->S * sizeof(float);
+	BFVM_CUDA(cudaMemcpyAsync(a.sec, secretion_rates, AS, cudaMemcpyHostToDevice, s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(a.sat, saturation_densities, AS, cudaMemcpyHostToDevice, s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(a.upt, uptake_rates, AS, cudaMemcpyHostToDevice, s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(a.nex, net_export_rates, AS, cudaMemcpyHostToDevice, s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(a.intern, internalized_substrates, AS, cudaMemcpyHostToDevice, s->stream));
+	if (fraction_released_at_death)
+		BFVM_CUDA(cudaMemcpyAsync(a.frac, fraction_released_at_death, AS, cudaMemcpyHostToDevice, s->stream));
+	else
+		BFVM_CUDA(cudaMemsetAsync(a.frac, 0, AS, s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(a.vol, volumes, (size_t)count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(a.pos, positions, (size_t)count * s->dims * sizeof(float), cudaMemcpyHostToDevice,
+							  s->stream));
+	if (resized)
+		a.binned = false;
+	return BFVM_OK;
+}
+
+int bfvm_load_internalized(bfvm_solver* s, float* host)
+{
+	CHECK_SOLVER(s);
+	if (s->ag.count == 0)
+		return BFVM_OK;
+	if (!host)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
+	BFVM_CUDA(cudaMemcpyAsync(host, s->ag.intern, (size_t)s->ag.count * s->S * sizeof(float), cudaMemcpyDeviceToHost,
+							  s->stream));
+	return check_device_errors(s);
+}
+
+int bfvm_diffusion_solve(bfvm_solver* s)
+{
+	CHECK_SOLVER(s);
+	return diffusion(s);
+}
+
+int bfvm_diffusion_sweep(bfvm_solver* s, int axis)
+{
+	CHECK_SOLVER(s);
+	if (axis < 0 || axis >= s->dims)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "axis must be in [0, dims)");
+	return launch_sweep(s, axis, axis == s->dims - 1);
+}
+
+int bfvm_dirichlet_solve(bfvm_solver* s)
+{
+	CHECK_SOLVER(s);
+	return launch_dirichlet(s);
+}
+
+int bfvm_gradient_solve(bfvm_solver* s)
+{
+	CHECK_SOLVER(s);
+	return launch_gradient(s);
+}
+
+int bfvm_secretion_solve(bfvm_solver* s, int recompute)
+{
+	CHECK_SOLVER(s);
+	return launch_secretion(s, recompute != 0);
+}
+
+int bfvm_release_internalized(bfvm_solver* s, int32_t index)
+{
+	CHECK_SOLVER(s);
+	if (index < 0 || index >= s->ag.count)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "agent index out of range");
+	return launch_release(s, index);
+}
+
+int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
+{
+	CHECK_SOLVER(s);
+	if (steps < 0)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "steps must not be negative");
+	for (int i = 0; i < steps; i++)
+	{
+		const int rc = ((first_step + i) % 10 == 0) ? 1 : 0;
+		// the first non-recompute step after new agents needs a binning pass; run it eagerly
+		if (!rc && s->ag.count > 0 && !s->ag.binned)
+		{
+			int st = one_step(s, false);
+			if (st)
+				return st;
+			continue;
+		}
+		if (!s->step_graph[rc])
+		{
+			cudaGraph_t g = nullptr;
+			BFVM_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+			const long long before = s->launches;
+			int st = one_step(s, rc == 1);
+			cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+			if (st)
+			{
+				if (g)
+					cudaGraphDestroy(g);
+				return st;
+			}
+			if (ce != cudaSuccess)
+				return cuda_fail(ce, "cudaStreamEndCapture");
+			s->graph_kernels[rc] = s->launches - before;
+			s->launches = before;
+			ce = cudaGraphInstantiate(&s->step_graph[rc], g, 0);
+			cudaGraphDestroy(g);
+			if (ce != cudaSuccess)
+			{
+				s->step_graph[rc] = nullptr;
+				return cuda_fail(ce, "cudaGraphInstantiate");
+			}
+		}
+		BFVM_CUDA(cudaGraphLaunch(s->step_graph[rc], s->stream));
+		s->launches += s->graph_kernels[rc];
+	}
+	return BFVM_OK;
+}
+
+int bfvm_synchronize(bfvm_solver* s)
+{
+	CHECK_SOLVER(s);
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	return check_device_errors(s);
+}
+
+int bfvm_device_densities(bfvm_solver* s, float** ptr, int64_t* count)
+{
+	if (!s || !ptr)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null argument");
+	*ptr = s->dens;
+	if (count)
+		*count = s->V * s->S;
+	return BFVM_OK;
+}
+
+int bfvm_device_gradients(bfvm_solver* s, float** ptr, int64_t* count)
+{
+	if (!s || !ptr)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null argument");
+	*ptr = s->grad;
+	if (count)
+		*count = s->V * s->S * s->dims;
+	return BFVM_OK;
+}
+
+int bfvm_launch_count(const bfvm_solver* s, int64_t* launches)
+{
+	if (!s || !launches)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null argument");
+	*launches = s->launches;
+	return BFVM_OK;
+}
+
+} // extern "C"

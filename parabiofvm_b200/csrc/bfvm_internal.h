@@ -1,0 +1,216 @@
+// Internal state of a bfvm_solver and the launchers shared by the .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/bfvm.h"
+
+namespace bfvm {
+
+// ------------------------------------------------------------------------------------------------
+// errors
+
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define BFVM_CUDA(call)                                                                                                \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		cudaError_t e_ = (call);                                                                                       \
+		if (e_ != cudaSuccess)                                                                                         \
+			return ::bfvm::cuda_fail(e_, #call);                                                                       \
+	} while (0)
+
+// device-side error flag bits
+enum device_error_bits : int
+{
+	DEVERR_AGENT_OUTSIDE = 1,
+};
+
+// ------------------------------------------------------------------------------------------------
+// Dirichlet conditions as seen by the kernels.  Faces are indexed 2*axis + is_max and applied in
+// that order; interior voxels are found through a rank bitmap over linear voxel indices
+// (v = x + X*(y + Y*z)): bit v of `bits` marks a Dirichlet voxel, and its row in ivals/iconds is
+// rank[v/32] + popcount of the lower bits of its word.
+struct dirichlet_dev
+{
+	const float* face_vals;			  // [6][S]
+	const unsigned char* face_conds;  // [6][S]
+	int face_mask;					  // bit (2*axis + is_max) set when the face exists
+	const unsigned int* bits;		  // [ceil(V/32)]
+	const int* rank;				  // [ceil(V/32)]
+	const float* ivals;				  // [N][S]
+	const unsigned char* iconds;	  // [N][S]
+	int has_interior;
+};
+
+// One sweep axis: the precomputed Thomas coefficients of src/solver/host/diffusion_solver.cpp:72-142
+// plus the block-carry products of the partitioned solve.  Tables are [n][S] on the device.
+struct sweep_plan
+{
+	int n = 0;		   // line length
+	int P = 1;		   // blocks per line
+	int base_len = 0;  // blocks 0..extra-1 have base_len+1 elements, the rest base_len
+	int extra = 0;
+	int M = 32;		   // register block capacity (kernel template)
+	float* bp = nullptr;	// b'_i
+	float* eprev = nullptr; // e_{i-1} (0 at i = 0)
+	float* g = nullptr;		// forward carry products, relative to the block start
+	float* G = nullptr;		// backward carry products, relative to the block end
+	float* c = nullptr;		// [S] off-diagonal
+};
+
+// Radix-sort / scan scratch for the agent binning.
+struct scan_plan
+{
+	std::vector<long long> level_sizes; // element count at each level
+	std::vector<int*> level_sums;		// block sums per level (device)
+};
+
+struct agent_state
+{
+	int count = 0;
+	int capacity = 0;
+	float *sec = nullptr, *sat = nullptr, *upt = nullptr, *nex = nullptr, *intern = nullptr, *frac = nullptr;
+	float *vol = nullptr, *pos = nullptr;
+
+	// binning (rebuilt on recompute)
+	unsigned int *keys = nullptr, *keys_alt = nullptr;
+	int *vals = nullptr, *vals_alt = nullptr;
+	int* hist = nullptr;		 // [256][tiles]
+	int* flags = nullptr;		 // [A]
+	int* seg_id = nullptr;		 // [A]
+	int* seg_start = nullptr;	 // [A+1]
+	int* seg_count_dev = nullptr; // [2]: number of segments, number of valid agents
+	float *num = nullptr, *den = nullptr, *fac = nullptr;			 // [A][S]
+	float *red_num = nullptr, *red_den = nullptr, *red_fac = nullptr; // [A][S] by segment
+	int tiles = 0;
+	scan_plan hist_scan, flag_scan;
+	bool binned = false;		 // a recompute has run since the last store
+};
+
+} // namespace bfvm
+
+struct bfvm_solver
+{
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	cudaStream_t own_stream = nullptr;
+
+	int dims = 3;
+	int bbox_min[3] = { 0, 0, 0 }, bbox_max[3] = { 0, 0, 0 }, voxel[3] = { 1, 1, 1 }, grid[3] = { 1, 1, 1 };
+	int S = 1;
+	float dt = 0;
+	std::vector<float> D, decay;
+	bool internalized = false;
+	long long V = 0;
+
+	float* dens = nullptr;
+	float* grad = nullptr;
+
+	bfvm::sweep_plan plan[3];
+
+	// Dirichlet, host copies (for rebuilds) and device buffers
+	std::vector<float> face_vals_h;			 // [6][S]
+	std::vector<unsigned char> face_conds_h; // [6][S]
+	int face_mask = 0;
+	float* face_vals = nullptr;
+	unsigned char* face_conds = nullptr;
+	int n_interior = 0;
+	unsigned int* dir_bits = nullptr;
+	int* dir_rank = nullptr;
+	float* dir_vals = nullptr;
+	unsigned char* dir_conds = nullptr;
+
+	bfvm::agent_state ag;
+
+	int* dev_error = nullptr; // device error flags
+	int* host_error = nullptr; // pinned mirror
+
+	long long launches = 0;
+
+	// graphs for run_steps: [recompute]
+	cudaGraphExec_t step_graph[2] = { nullptr, nullptr };
+	long long graph_kernels[2] = { 0, 0 }; // kernel nodes per step graph
+	bool graphs_dirty = true;
+
+	bfvm::dirichlet_dev dirichlet() const
+	{
+		bfvm::dirichlet_dev d;
+		d.face_vals = face_vals;
+		d.face_conds = face_conds;
+		d.face_mask = face_mask;
+		d.bits = dir_bits;
+		d.rank = dir_rank;
+		d.ivals = dir_vals;
+		d.iconds = dir_conds;
+		d.has_interior = n_interior > 0;
+		return d;
+	}
+};
+
+namespace bfvm {
+
+// precompute.cpp
+void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, const float* decay, int M,
+					 std::vector<float>& bp, std::vector<float>& eprev, std::vector<float>& g, std::vector<float>& G,
+					 std::vector<float>& c, int& P, int& base_len, int& extra);
+
+// sweep.cu
+int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);
+int launch_dirichlet(bfvm_solver* s);
+
+// gradient.cu
+int launch_gradient(bfvm_solver* s);
+
+// cell.cu
+int cell_alloc(bfvm_solver* s, int count);
+void cell_free(bfvm_solver* s);
+int launch_secretion(bfvm_solver* s, bool recompute);
+int launch_release(bfvm_solver* s, int index);
+
+// scan.cu
+int scan_plan_build(scan_plan& p, long long n);
+void scan_plan_free(scan_plan& p);
+int launch_exclusive_scan(bfvm_solver* s, scan_plan& p, const int* in, int* out, long long n);
+
+template <typename T>
+int device_alloc(T** ptr, size_t count)
+{
+	*ptr = nullptr;
+	if (count == 0)
+		return BFVM_OK;
+	cudaError_t e = cudaMalloc((void**)ptr, count * sizeof(T));
+	if (e != cudaSuccess)
+	{
+		*ptr = nullptr;
+		(void)cudaGetLastError();
+		return fail(BFVM_ERR_OUT_OF_MEMORY, std::string("device allocation of ") + std::to_string(count * sizeof(T))
+												+ " bytes failed: " + cudaGetErrorString(e));
+	}
+	return BFVM_OK;
+}
+
+template <typename T>
+void device_free(T*& ptr)
+{
+	if (ptr)
+		cudaFree((void*)ptr);
+	ptr = nullptr;
+}
+
+inline int check_launch(bfvm_solver* s, const char* what)
+{
+	s->launches++;
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess)
+		return cuda_fail(e, what);
+	return BFVM_OK;
+}
+
+} // namespace bfvm
