@@ -53,6 +53,7 @@ struct oracle_state
 
 	// Dirichlet (include/BioFVM/microenvironment.h:41-50)
 	int n_interior = 0;
+	bool interior_duplicates = false; // a voxel listed twice
 	std::vector<int> interior_voxels;
 	std::vector<real_t> interior_values;
 	std::vector<uint8_t> interior_conds;
@@ -167,10 +168,30 @@ void solve_boundary_face(oracle_state<real_t>& m, int axis, bool is_max)
 }
 
 template <typename real_t>
+void apply_interior_entry(oracle_state<real_t>& m, int v)
+{
+	int idx[3] = { 0, 0, 0 };
+	for (int d = 0; d < m.dims; d++)
+		idx[d] = m.interior_voxels[(std::size_t)v * m.dims + d];
+	for (int s = 0; s < m.S; s++)
+		if (m.interior_conds[(std::size_t)v * m.S + s])
+			m.dens[m.dens_index(idx[0], idx[1], idx[2], s)] = m.interior_values[(std::size_t)v * m.S + s];
+}
+
+template <typename real_t>
 void solve_interior(oracle_state<real_t>& m)
 {
 	if (m.n_interior == 0)
 		return;
+	if (m.interior_duplicates)
+	{
+		// The reference distributes the list over threads (dirichlet_solver.cpp:63), so two entries
+		// for one voxel race; in list order the later entry wins, as with one thread.
+#pragma omp single
+		for (int v = 0; v < m.n_interior; v++)
+			apply_interior_entry(m, v);
+		return;
+	}
 #pragma omp for
 	for (int v = 0; v < m.n_interior; v++)
 	{
@@ -684,6 +705,18 @@ void run_steps(oracle_state<real_t>& m, int steps, int first_step)
 		auto& m = *static_cast<oracle_state<T>*>(h);                                                                   \
 		m.n_interior = count;                                                                                          \
 		m.interior_voxels.assign(voxels, voxels + (std::size_t)count * m.dims);                                        \
+		{                                                                                                              \
+			std::vector<long long> lin(count);                                                                         \
+			for (int v = 0; v < count; v++)                                                                            \
+			{                                                                                                          \
+				long long key = 0;                                                                                     \
+				for (int d = m.dims - 1; d >= 0; d--)                                                                  \
+					key = key * m.grid[d] + voxels[(std::size_t)v * m.dims + d];                                       \
+				lin[v] = key;                                                                                          \
+			}                                                                                                          \
+			std::sort(lin.begin(), lin.end());                                                                         \
+			m.interior_duplicates = std::adjacent_find(lin.begin(), lin.end()) != lin.end();                           \
+		}                                                                                                              \
 		m.interior_values.assign(values, values + (std::size_t)count * m.S);                                           \
 		m.interior_conds.assign(conds, conds + (std::size_t)count * m.S);                                              \
 	}                                                                                                                  \

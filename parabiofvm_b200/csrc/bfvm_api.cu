@@ -36,20 +36,19 @@ static int upload_plan(bfvm_solver* s, int axis)
 {
 	sweep_plan& p = s->plan[axis];
 	const int n = s->grid[axis];
-	std::vector<float> bp, ep, g, G, c;
+	std::vector<float> bp, ep, g, G, c, gq, Gp;
 	p.n = n;
 	p.M = pick_block_capacity(n);
-	precompute_axis(n, s->voxel[axis], s->dims, s->S, s->dt, s->D.data(), s->decay.data(), p.M, bp, ep, g, G, c,
-					p.P, p.base_len, p.extra);
+	precompute_axis(n, s->voxel[axis], s->dims, s->S, s->dt, s->D.data(), s->decay.data(), p.M, bp, ep, g, G, c, gq,
+					Gp, p.P, p.base_len, p.extra);
 	int st;
 	const size_t nS = (size_t)n * s->S;
-	if ((st = device_alloc(&p.bp, nS)) || (st = device_alloc(&p.eprev, nS)) || (st = device_alloc(&p.g, nS))
-		|| (st = device_alloc(&p.G, nS)) || (st = device_alloc(&p.c, (size_t)s->S)))
+	if ((st = device_alloc(&p.bp, nS)) || (st = device_alloc(&p.c, (size_t)s->S))
+		|| (st = device_alloc(&p.gq, gq.size())) || (st = device_alloc(&p.Gp, Gp.size())))
 		return st;
+	BFVM_CUDA(cudaMemcpy(p.gq, gq.data(), gq.size() * sizeof(float), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(p.Gp, Gp.data(), Gp.size() * sizeof(float), cudaMemcpyHostToDevice));
 	BFVM_CUDA(cudaMemcpy(p.bp, bp.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
-	BFVM_CUDA(cudaMemcpy(p.eprev, ep.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
-	BFVM_CUDA(cudaMemcpy(p.g, g.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
-	BFVM_CUDA(cudaMemcpy(p.G, G.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
 	BFVM_CUDA(cudaMemcpy(p.c, c.data(), (size_t)s->S * sizeof(float), cudaMemcpyHostToDevice));
 	return BFVM_OK;
 }
@@ -57,10 +56,9 @@ static int upload_plan(bfvm_solver* s, int axis)
 static void free_plan(sweep_plan& p)
 {
 	device_free(p.bp);
-	device_free(p.eprev);
-	device_free(p.g);
-	device_free(p.G);
 	device_free(p.c);
+	device_free(p.gq);
+	device_free(p.Gp);
 }
 
 static void free_graphs(bfvm_solver* s)

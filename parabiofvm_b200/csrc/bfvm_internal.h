@@ -50,7 +50,8 @@ struct dirichlet_dev
 };
 
 // One sweep axis: the precomputed Thomas coefficients of src/solver/host/diffusion_solver.cpp:72-142
-// plus the block-carry products of the partitioned solve.  Tables are [n][S] on the device.
+// (only b' is stored; e = c b' is recomputed) plus the whole-block carry products of the
+// partitioned solve.
 struct sweep_plan
 {
 	int n = 0;		   // line length
@@ -58,11 +59,10 @@ struct sweep_plan
 	int base_len = 0;  // blocks 0..extra-1 have base_len+1 elements, the rest base_len
 	int extra = 0;
 	int M = 32;		   // register block capacity (kernel template)
-	float* bp = nullptr;	// b'_i
-	float* eprev = nullptr; // e_{i-1} (0 at i = 0)
-	float* g = nullptr;		// forward carry products, relative to the block start
-	float* G = nullptr;		// backward carry products, relative to the block end
+	float* bp = nullptr;	// [n][S] b'_i
 	float* c = nullptr;		// [S] off-diagonal
+	float* gq = nullptr;	// [P][S] forward carry product of each whole block
+	float* Gp = nullptr;	// [P][S] backward carry product of each whole block
 };
 
 // Radix-sort / scan scratch for the agent binning.
@@ -159,7 +159,8 @@ namespace bfvm {
 // precompute.cpp
 void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, const float* decay, int M,
 					 std::vector<float>& bp, std::vector<float>& eprev, std::vector<float>& g, std::vector<float>& G,
-					 std::vector<float>& c, int& P, int& base_len, int& extra);
+					 std::vector<float>& c, std::vector<float>& gq, std::vector<float>& Gp, int& P, int& base_len,
+					 int& extra);
 
 // sweep.cu
 int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);

@@ -24,7 +24,8 @@ namespace bfvm {
 
 void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, const float* decay, int M,
 					 std::vector<float>& bp, std::vector<float>& eprev, std::vector<float>& g, std::vector<float>& G,
-					 std::vector<float>& c, int& P, int& base_len, int& extra)
+					 std::vector<float>& c, std::vector<float>& gq, std::vector<float>& Gp, int& P, int& base_len,
+					 int& extra)
 {
 	bp.assign((size_t)n * S, 0.f);
 	eprev.assign((size_t)n * S, 0.f);
@@ -40,6 +41,8 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 		P = 1;
 		base_len = 1;
 		extra = 0;
+		gq.assign(S, 0.f);
+		Gp.assign(S, 0.f);
 		return;
 	}
 
@@ -68,6 +71,10 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 	base_len = n / P;
 	extra = n % P;
 
+	// whole-block products used by the carry folds: gq[j] = g at the block end, Gp[j] = G at the
+	// block start
+	gq.assign((size_t)P * S, 0.f);
+	Gp.assign((size_t)P * S, 0.f);
 	for (int j = 0; j < P; j++)
 	{
 		const int p = j * base_len + std::min(j, extra);
@@ -83,6 +90,7 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 					acc *= -(double)eprev[(size_t)i * S + s];
 					g[(size_t)i * S + s] = (float)acc;
 				}
+				gq[(size_t)j * S + s] = (float)acc;
 			}
 			if (j < P - 1)
 			{
@@ -92,6 +100,7 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 					acc *= -(double)c[s] * (double)bp[(size_t)i * S + s];
 					G[(size_t)i * S + s] = (float)acc;
 				}
+				Gp[(size_t)j * S + s] = (float)acc;
 			}
 		}
 	}

@@ -36,6 +36,8 @@ struct sweep_args
 	float* data;
 	const float* bp; // [n][S] in global memory; staged into shared memory by the kernels
 	const float* c;	 // [S]
+	const float* gq; // [P][S] whole-block forward carry products
+	const float* Gp; // [P][S] whole-block backward carry products
 	int n, P, base_len, extra, S;
 	int X, Y, Z;
 	dirichlet_dev dir;
@@ -203,8 +205,9 @@ __device__ __forceinline__ void block_range(int j, int base_len, int extra, int&
 // CTA must call this (it contains __syncthreads).
 template <int M>
 __device__ __forceinline__ void solve_block(const sweep_args& a, float* __restrict__ line, long long stride,
-											const float* bp, int bstride, float cs, int s, int j, bool active,
-											float* carry_f, float* carry_t, int cstride, const line_dirichlet& ld)
+											const float* bp, const float* gq, const float* Gp, int bstride, float cs,
+											int s, int j, bool active, float* carry_f, float* carry_t, int cstride,
+											const line_dirichlet& ld)
 {
 	const int S = a.S;
 	int p, L;
@@ -250,14 +253,7 @@ __device__ __forceinline__ void solve_block(const sweep_args& a, float* __restri
 		// g^k_q = prod_{i=p_k-1}^{q_k-1} (-c b'_i)
 		float C = carry_f[0];
 		for (int k = 1; k < j; k++)
-		{
-			int pk, Lk;
-			block_range(k, a.base_len, a.extra, pk, Lk);
-			float gq = 1.f;
-			for (int i = pk - 1; i < pk + Lk - 1; i++)
-				gq = __fmul_rn(gq, -__fmul_rn(cs, bp[i * bstride]));
-			C = fmaf(gq, C, carry_f[k * cstride]);
-		}
+			C = fmaf(gq[k * bstride], C, carry_f[k * cstride]);
 		// d'_i = f_i + g_i C with the running product g_i = prod_{m=p-1}^{i-1} (-c b'_m)
 		float g = 1.f;
 #pragma unroll
@@ -293,14 +289,7 @@ __device__ __forceinline__ void solve_block(const sweep_args& a, float* __restri
 		// G^k_p = prod_{i=p_k}^{q_k} (-c b'_i)
 		float Xc = carry_t[(a.P - 1) * cstride];
 		for (int k = a.P - 2; k > j; k--)
-		{
-			int pk, Lk;
-			block_range(k, a.base_len, a.extra, pk, Lk);
-			float Gp = 1.f;
-			for (int i = pk + Lk - 1; i >= pk; i--)
-				Gp = __fmul_rn(Gp, -__fmul_rn(cs, bp[i * bstride]));
-			Xc = fmaf(Gp, Xc, carry_t[k * cstride]);
-		}
+			Xc = fmaf(Gp[k * bstride], Xc, carry_t[k * cstride]);
 		// x_i = t_i + G_i X with the running product G_i = prod_{m=i}^{q} (-c b'_m)
 		float G = 1.f;
 #pragma unroll
@@ -331,19 +320,33 @@ __device__ __forceinline__ void solve_block(const sweep_args& a, float* __restri
 	}
 }
 
-// Stage b' ([n][S] -> columns s0 .. s0+Sc-1, layout [n][Sc]) and c into shared memory.
-__device__ __forceinline__ void stage_table(const sweep_args& a, float* tab, float* ctab, int s0, int Sc)
+// Stage the coefficients of substrates s0 .. s0+Sc-1 into shared memory: b' [n][Sc], c [Sc],
+// gq [P][Sc], Gp [P][Sc] (consecutive in `tab`).
+__device__ __forceinline__ void stage_table(const sweep_args& a, float* tab, int s0, int Sc)
 {
-	const int total = a.n * Sc;
-	for (int t = threadIdx.x + threadIdx.y * blockDim.x; t < total; t += blockDim.x * blockDim.y)
+	const int nt = blockDim.x * blockDim.y;
+	const int t0 = threadIdx.x + threadIdx.y * blockDim.x;
+	for (int t = t0; t < a.n * Sc; t += nt)
 	{
 		const int i = t / Sc, sl = t % Sc;
 		tab[t] = (s0 + sl < a.S) ? a.bp[(size_t)i * a.S + s0 + sl] : 0.f;
 	}
-	for (int t = threadIdx.x + threadIdx.y * blockDim.x; t < Sc; t += blockDim.x * blockDim.y)
+	float* ctab = tab + a.n * Sc;
+	for (int t = t0; t < Sc; t += nt)
 		ctab[t] = (s0 + t < a.S) ? a.c[s0 + t] : 0.f;
+	float* gtab = ctab + Sc;
+	float* Gtab = gtab + a.P * Sc;
+	for (int t = t0; t < a.P * Sc; t += nt)
+	{
+		const int k = t / Sc, sl = t % Sc;
+		const bool ok = s0 + sl < a.S;
+		gtab[t] = ok ? a.gq[(size_t)k * a.S + s0 + sl] : 0.f;
+		Gtab[t] = ok ? a.Gp[(size_t)k * a.S + s0 + sl] : 0.f;
+	}
 	__syncthreads();
 }
+
+__host__ __device__ __forceinline__ int table_floats(int n, int P, int Sc) { return n * Sc + Sc + 2 * P * Sc; }
 
 // y (AXIS 1) and z (AXIS 2) sweeps.  Work item w = outer * col_tiles + tile; the grid strides over
 // items.  MAXT bounds the CTA size (32 * P) so the register budget follows the block count.
@@ -355,10 +358,12 @@ __global__ void __launch_bounds__(MAXT, MINB)
 {
 	extern __shared__ float sh[];
 	float* tab = sh;
-	float* ctab = tab + a.n * a.S;
-	float* carry_f = ctab + a.S;
+	const float* ctab = tab + a.n * a.S;
+	const float* gtab = ctab + a.S;
+	const float* Gtab = gtab + a.P * a.S;
+	float* carry_f = tab + table_floats(a.n, a.P, a.S);
 	float* carry_t = carry_f + a.P * 32;
-	stage_table(a, tab, ctab, 0, a.S);
+	stage_table(a, tab, 0, a.S);
 
 	const int lane = threadIdx.x;
 	const int j = threadIdx.y;
@@ -384,7 +389,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
 			}
 		}
 		float* line = a.data + outer * outer_stride + qq;
-		solve_block<M>(a, line, line_stride, tab + s, S, ctab[s], s, j, active, carry_f + lane, carry_t + lane, 32, ld);
+		solve_block<M>(a, line, line_stride, tab + s, gtab + s, Gtab + s, S, ctab[s], s, j, active, carry_f + lane,
+					   carry_t + lane, 32, ld);
 	}
 }
 
@@ -398,9 +404,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
 	extern __shared__ float sh[];
 	const int s0 = blockIdx.y * Sc;
 	float* tab = sh;
-	float* ctab = tab + a.n * Sc;
-	float* carries = ctab + Sc;
-	stage_table(a, tab, ctab, s0, Sc);
+	const float* ctab = tab + a.n * Sc;
+	const float* gtab = ctab + Sc;
+	const float* Gtab = gtab + a.P * Sc;
+	float* carries = tab + table_floats(a.n, a.P, Sc);
+	stage_table(a, tab, s0, Sc);
 
 	const int t = threadIdx.x;
 	const int P = a.P;
@@ -421,7 +429,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
 		if (a.pre_dirichlet)
 			ld.init<0>(a.dir, (int)(rr % a.Y), (int)(rr / a.Y), ss, a.S, a.X, a.Y, a.Z, a.n);
 		float* line = a.data + rr * (long long)a.X * a.S + ss;
-		solve_block<M>(a, line, a.S, tab + sl, Sc, ctab[sl], ss, j, active, carry_f, carry_t, Sc, ld);
+		solve_block<M>(a, line, a.S, tab + sl, gtab + sl, Gtab + sl, Sc, ctab[sl], ss, j, active, carry_f, carry_t, Sc,
+					   ld);
 	}
 }
 
@@ -476,7 +485,7 @@ static int launch_columns(bfvm_solver* st, const sweep_args& a)
 	const long long tiles = (ncols + 31) / 32;
 	const long long outers = AXIS == 1 ? Z : 1;
 	const long long items = outers * tiles;
-	const size_t smem = ((size_t)a.n * S + S + 2 * (size_t)a.P * 32) * sizeof(float);
+	const size_t smem = ((size_t)table_floats(a.n, a.P, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float);
 	auto kernel = sweep_columns<M, AXIS, MAXT, MINB>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
@@ -503,7 +512,7 @@ static int launch_sweep_m(bfvm_solver* st, int axis, const sweep_args& a)
 		const int threads = rows_per_cta * per_row;
 		const long long groups = (nrows + rows_per_cta - 1) / rows_per_cta;
 		const int chunks = (int)((S + Sc - 1) / Sc);
-		const size_t smem = ((size_t)a.n * Sc + Sc + 2 * (size_t)rows_per_cta * a.P * Sc) * sizeof(float);
+		const size_t smem = ((size_t)table_floats(a.n, a.P, Sc) + 2 * (size_t)rows_per_cta * a.P * Sc) * sizeof(float);
 		auto kernel = threads <= 320 ? sweep_rows<M, 320, 2> : sweep_rows<M, 512, 1>;
 		int rc = set_smem(kernel, smem);
 		if (rc)
@@ -528,6 +537,8 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 	a.data = st->dens;
 	a.bp = pl.bp;
 	a.c = pl.c;
+	a.gq = pl.gq;
+	a.Gp = pl.Gp;
 	a.n = pl.n;
 	a.P = pl.P;
 	a.base_len = pl.base_len;

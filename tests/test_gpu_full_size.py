@@ -1,0 +1,85 @@
+"""Checks at the benchmark's full size: 320^3 voxels x 16 substrates, 1,000,000 clustered agents.
+
+* One full step (diffusion, gradient, secretion with binning) against the FP32 oracle: the stated
+  1e-5 maximum relative error per step.
+* Size-independent properties of the implicit LOD step, checked on the GPU alone:
+  - with zero-flux boundaries and no decay every sweep matrix has unit column sums, so the total
+    of each substrate is conserved;
+  - a uniform field stays uniform and decays by (1 + dt*lambda/3)^-3 per step;
+  - the step is linear in the field when no Dirichlet condition or agent is present.
+"""
+
+import numpy as np
+import pytest
+
+from parabiofvm_b200.workloads import Workload, make_solver, synthetic
+from scenarios import make_oracle, rel_err, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+EDGE, S = 320, 16
+
+
+@pytest.fixture(scope="module")
+def big():
+    return synthetic(EDGE, S, 1_000_000, seed=20261203, clustered=True, sigma=200.0, interior_fraction=0.01)
+
+
+def test_one_full_step_matches_oracle(big):
+    g = make_solver(big)
+    g.run_steps(1, 0)
+    gd, gg, gi = g.load_densities(), g.load_gradients(), g.load_internalized()
+    g.close()
+    o = make_oracle(big, np.float32)
+    o.run_steps(1, 0)
+    e = rel_err(gd, o.densities())
+    print(f"320^3x16 one step: max rel err densities {e:.3e}")
+    assert e < 1e-5
+    assert rel_err(gg, o.gradients(), floor_frac=1e-3) < 1e-3
+    assert rel_l2(gi, o.internalized()) < 1e-6
+
+
+def _plain(field, D, decay):
+    L = EDGE * 20
+    w = Workload(dims=3, bbox_min=(0, 0, 0), bbox_max=(L, L, L), voxel_shape=(20, 20, 20),
+                 diffusion_coefficients=list(D), decay_rates=list(decay), time_step=0.01,
+                 initial_conditions=[0.0] * len(D))
+    w.densities = field
+    return w
+
+
+def test_mass_conserved_without_decay(big):
+    field = big.densities
+    w = _plain(field, big.diffusion_coefficients, [0.0] * S)
+    g = make_solver(w)
+    g.run_steps(2, 1)  # no agents: diffusion + gradient only
+    d = g.load_densities().reshape(-1, S).astype(np.float64)
+    g.close()
+    before = field.reshape(-1, S).astype(np.float64).sum(axis=0)
+    after = d.sum(axis=0)
+    assert np.max(np.abs(after - before) / before) < 1e-5
+
+
+def test_uniform_field_decays_exactly():
+    decay = np.linspace(0.01, 1.0, S)
+    field = np.tile(np.linspace(0.5, 2.0, S, dtype=np.float32), EDGE ** 3)
+    w = _plain(field, np.geomspace(1e3, 1e5, S), decay)
+    g = make_solver(w)
+    g.diffusion()
+    d = g.load_densities().reshape(-1, S).astype(np.float64)
+    g.close()
+    expected = np.linspace(0.5, 2.0, S, dtype=np.float32).astype(np.float64) / (1 + 0.01 * decay / 3) ** 3
+    assert np.max(np.abs(d - expected) / expected) < 2e-6
+
+
+def test_linearity(big):
+    rng = np.random.default_rng(3)
+    u = big.densities
+    v = rng.uniform(0, 1, u.size).astype(np.float32)
+    out = []
+    for f in (u, v, (0.5 * u.astype(np.float64) + 2.0 * v.astype(np.float64)).astype(np.float32)):
+        g = make_solver(_plain(f, big.diffusion_coefficients, big.decay_rates))
+        g.diffusion()
+        out.append(g.load_densities().astype(np.float64))
+        g.close()
+    assert rel_l2(out[2], 0.5 * out[0] + 2.0 * out[1]) < 1e-6

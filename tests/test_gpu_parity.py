@@ -65,9 +65,14 @@ def test_cpu_runnable_config_100_steps():
     d = g.densities()
     e32 = rel_err(d, o32.densities())
     e64 = rel_err(d, o64.densities())
-    print(f"cfg 50^3x4: max rel err vs FP32 {e32:.3e}, vs FP64 {e64:.3e}, worst sampled {worst:.3e}")
+    # the FP64 build is the accuracy yardstick: the GPU may not be further from it than the FP32
+    # reference build is (with a small allowance for the different rounding path)
+    o32_64 = rel_l2(o32.densities(), o64.densities())
+    g_64 = rel_l2(d, o64.densities())
+    print(f"cfg 50^3x4: max rel err vs FP32 {e32:.3e}, vs FP64 {e64:.3e}, worst sampled {worst:.3e}; "
+          f"rel L2 vs FP64: GPU {g_64:.3e}, FP32 oracle {o32_64:.3e}")
     assert e32 < 1e-4
-    assert rel_l2(d, o64.densities()) < 1e-5
+    assert g_64 <= 1.5 * o32_64 + 1e-7
     assert rel_l2(g.internalized(), o32.internalized()) < 1e-5
     assert rel_err(g.gradients(), o32.gradients(), floor_frac=1e-3) < 1e-3
 
