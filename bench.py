@@ -44,6 +44,11 @@ WORKLOADS = {
                       text="320^3 voxels (dx 20 um) x 16 FP32 substrates, 1,000,000 agents in 32 Gaussian clusters "
                            "(sigma 200 um), 1% interior Dirichlet voxels, Dirichlet 1.0 on substrate 0 at all faces, "
                            "dt 0.01 min, binning rebuilt every 10th step"),
+    # the large configuration at half the edge, for ncu captures (262 MB field, still larger than L2)
+    "plain-160": dict(edge=160, S=16, agents=125_000, clustered=True, sigma=200.0, interior_fraction=0.01,
+                      seed=20261203,
+                      text="160^3 voxels (dx 20 um) x 16 FP32 substrates, 125,000 agents in 32 Gaussian clusters, "
+                           "1% interior Dirichlet voxels, Dirichlet 1.0 on substrate 0 at all faces (profiling size)"),
     # the CPU-runnable configuration (parity case, L2-resident)
     "plain-50": dict(edge=50, S=4, agents=5000, clustered=False, sigma=0.0, interior_fraction=0.0, seed=11,
                      text="50^3 voxels x 4 FP32 substrates, 5,000 uniform agents, Dirichlet 1.0 on substrate 0 at "
@@ -113,7 +118,7 @@ class ClockSampler:
         try:
             self.out = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.out,
+                                          "-i", str(self.gpu), "-lms", "50"], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -284,7 +289,7 @@ def run_ours(args):
     s.synchronize()
     sampler = ClockSampler(physical_gpu_index(local_rank))
     sampler.start()
-    time.sleep(0.3)
+    time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
     barrier()
     torch.cuda.synchronize()
     launches0 = s.launch_count
@@ -426,7 +431,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plain-320")

@@ -42,7 +42,8 @@ typedef enum bfvm_status
 	BFVM_ERR_CUDA = 3,             /* a CUDA runtime call failed */
 	BFVM_ERR_NO_DEVICE = 4,        /* no usable CUDA device / library built for another arch */
 	BFVM_ERR_STATE = 5,            /* call out of order (e.g. agents not stored) */
-	BFVM_ERR_AGENT_OUTSIDE = 6     /* an agent position maps outside the mesh */
+	BFVM_ERR_AGENT_OUTSIDE = 6,    /* an agent position maps outside the mesh */
+	BFVM_ERR_TIMEOUT = 7           /* a kernel's bounded wait on an asynchronous copy gave up */
 } bfvm_status;
 
 /* Message for the last failing call on this host thread ("" if none). */

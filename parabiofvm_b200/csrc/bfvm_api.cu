@@ -74,6 +74,8 @@ static void free_graphs(bfvm_solver* s)
 
 static void free_dirichlet_interior(bfvm_solver* s)
 {
+	for (auto& m : s->dir_block_mask)
+		device_free(m);
 	device_free(s->dir_bits);
 	device_free(s->dir_rank);
 	device_free(s->dir_vals);
@@ -120,6 +122,8 @@ static int check_device_errors(bfvm_solver* s)
 	if (e)
 	{
 		BFVM_CUDA(cudaMemsetAsync(s->dev_error, 0, sizeof(int), s->stream));
+		if (e & DEVERR_TIMEOUT)
+			return fail(BFVM_ERR_TIMEOUT, "a sweep kernel timed out waiting for a tile copy; the field is not valid");
 		if (e & DEVERR_AGENT_OUTSIDE)
 			return fail(BFVM_ERR_AGENT_OUTSIDE, "an agent position lies outside the mesh; it was left out of "
 												"secretion/uptake");
@@ -172,6 +176,7 @@ const char* bfvm_status_string(int status)
 	case BFVM_ERR_NO_DEVICE: return "no usable CUDA device";
 	case BFVM_ERR_STATE: return "invalid state";
 	case BFVM_ERR_AGENT_OUTSIDE: return "agent outside the mesh";
+	case BFVM_ERR_TIMEOUT: return "device wait timed out";
 	default: return "unknown status";
 	}
 }
@@ -441,6 +446,34 @@ int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* vo
 	BFVM_CUDA(cudaMemcpy(s->dir_rank, rank.data(), rank.size() * sizeof(int), cudaMemcpyHostToDevice));
 	BFVM_CUDA(cudaMemcpy(s->dir_vals, svals.data(), svals.size() * sizeof(float), cudaMemcpyHostToDevice));
 	BFVM_CUDA(cudaMemcpy(s->dir_conds, sconds.data(), sconds.size(), cudaMemcpyHostToDevice));
+
+	// per-axis block masks for the sweeps
+	const long long X = s->grid[0], Y = s->grid[1], Z = s->grid[2];
+	for (int axis = 0; axis < s->dims; axis++)
+	{
+		const sweep_plan& pl = s->plan[axis];
+		const long long lines = axis == 0 ? Y * Z : (axis == 1 ? X * Z : X * Y);
+		std::vector<unsigned long long> mask((size_t)(lines * pl.P), 0ull);
+		for (auto& kv : row_of)
+		{
+			const long long v = kv.first;
+			const long long x = v % X, y = (v / X) % Y, z = v / (X * Y);
+			const long long line = axis == 0 ? y + Y * z : (axis == 1 ? x + X * z : x + X * y);
+			const int i = (int)(axis == 0 ? x : (axis == 1 ? y : z));
+			// block of element i: the first `extra` blocks have base_len + 1 elements
+			const int big = pl.extra * (pl.base_len + 1);
+			const int j = i < big ? i / (pl.base_len + 1) : pl.extra + (i - big) / pl.base_len;
+			const int pj = j * pl.base_len + std::min(j, pl.extra);
+			mask[(size_t)(line * pl.P + j)] |= 1ull << (i - pj);
+		}
+		if ((st = device_alloc(&s->dir_block_mask[axis], mask.size())))
+		{
+			free_dirichlet_interior(s);
+			return st;
+		}
+		BFVM_CUDA(cudaMemcpy(s->dir_block_mask[axis], mask.data(), mask.size() * sizeof(unsigned long long),
+							 cudaMemcpyHostToDevice));
+	}
 	s->n_interior = (int)row_of.size();
 	return BFVM_OK;
 }

@@ -30,6 +30,7 @@ int cuda_fail(cudaError_t e, const char* what);
 enum device_error_bits : int
 {
 	DEVERR_AGENT_OUTSIDE = 1,
+	DEVERR_TIMEOUT = 2, // a bounded wait on an asynchronous copy gave up
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -47,6 +48,9 @@ struct dirichlet_dev
 	const float* ivals;				  // [N][S]
 	const unsigned char* iconds;	  // [N][S]
 	int has_interior;
+	// per sweep axis: bit k of block_mask[axis][line * P + j] marks element k of block j of a line
+	// as an interior Dirichlet voxel (lines: x sweep y + Y*z, y sweep x + X*z, z sweep x + X*y)
+	const unsigned long long* block_mask[3];
 };
 
 // One sweep axis: the precomputed Thomas coefficients of src/solver/host/diffusion_solver.cpp:72-142
@@ -126,6 +130,7 @@ struct bfvm_solver
 	int* dir_rank = nullptr;
 	float* dir_vals = nullptr;
 	unsigned char* dir_conds = nullptr;
+	unsigned long long* dir_block_mask[3] = { nullptr, nullptr, nullptr };
 
 	bfvm::agent_state ag;
 
@@ -133,6 +138,7 @@ struct bfvm_solver
 	int* host_error = nullptr; // pinned mirror
 
 	long long launches = 0;
+	bool use_tma = true; // stage sweeps through shared memory with the TMA where the shape allows
 
 	// graphs for run_steps: [recompute]
 	cudaGraphExec_t step_graph[2] = { nullptr, nullptr };
@@ -150,6 +156,8 @@ struct bfvm_solver
 		d.ivals = dir_vals;
 		d.iconds = dir_conds;
 		d.has_interior = n_interior > 0;
+		for (int a = 0; a < 3; a++)
+			d.block_mask[a] = dir_block_mask[a];
 		return d;
 	}
 };

@@ -24,185 +24,14 @@
 //     substrate s = t % Sc of block j = (t / Sc) % P of row t / (Sc*P).  A warp touches S
 //     consecutive floats of one or two blocks per element step.
 
-#include <algorithm>
-#include <string>
-
-#include "bfvm_internal.h"
+#include "sweep_common.cuh"
 
 namespace bfvm {
 
-struct sweep_args
-{
-	float* data;
-	const float* bp; // [n][S] in global memory; staged into shared memory by the kernels
-	const float* c;	 // [S]
-	const float* gq; // [P][S] whole-block forward carry products
-	const float* Gp; // [P][S] whole-block backward carry products
-	int n, P, base_len, extra, S;
-	int X, Y, Z;
-	dirichlet_dev dir;
-	int pre_dirichlet;
-	int post_dirichlet;
-};
+int sm_count(int device) { return sm_count_impl(device); }
 
-__device__ __forceinline__ float apply_dirichlet(const dirichlet_dev& d, float v, int x, int y, int z, int s, int S,
-												 int X, int Y, int Z)
-{
-	// faces: x-min, x-max, y-min, y-max, z-min, z-max; the later write wins
-	// (src/solver/host/dirichlet_solver.cpp:122-141)
-	const int fm = d.face_mask;
-	if (fm)
-	{
-		if ((fm & 1) && x == 0 && d.face_conds[0 * S + s])
-			v = d.face_vals[0 * S + s];
-		if ((fm & 2) && x == X - 1 && d.face_conds[1 * S + s])
-			v = d.face_vals[1 * S + s];
-		if ((fm & 4) && y == 0 && d.face_conds[2 * S + s])
-			v = d.face_vals[2 * S + s];
-		if ((fm & 8) && y == Y - 1 && d.face_conds[3 * S + s])
-			v = d.face_vals[3 * S + s];
-		if ((fm & 16) && z == 0 && d.face_conds[4 * S + s])
-			v = d.face_vals[4 * S + s];
-		if ((fm & 32) && z == Z - 1 && d.face_conds[5 * S + s])
-			v = d.face_vals[5 * S + s];
-	}
-	// interior voxels last (dirichlet_solver.cpp:53-75)
-	if (d.has_interior)
-	{
-		const long long vid = (long long)x + (long long)X * ((long long)y + (long long)Y * z);
-		const unsigned int w = __ldg(&d.bits[vid >> 5]);
-		const unsigned int b = (unsigned int)(vid & 31);
-		if ((w >> b) & 1u)
-		{
-			const long long row = (long long)__ldg(&d.rank[vid >> 5]) + __popc(w & ((1u << b) - 1u));
-			if (d.iconds[row * S + s])
-				v = d.ivals[row * S + s];
-		}
-	}
-	return v;
-}
-
-// The Dirichlet overwrite seen by one (line, substrate): faces of the other two axes cover a line
-// either entirely or not at all, faces of the sweep axis touch only its first and last element, and
-// interior voxels are looked up in the rank bitmap.  Resolved once per thread so the per-element
-// cost is a select plus one bitmap probe.
-struct line_dirichlet
-{
-	bool any;			 // anything to apply on this line
-	bool line_face;		 // a face of another axis covers the line (after own faces in precedence)
-	float line_val;
-	bool own_min, own_max; // sweep-axis faces at element 0 / n-1 (already merged with line faces)
-	float min_val, max_val;
-	long long base_vid, vid_stride;
-	int n;
-
-	template <int AXIS>
-	__device__ __forceinline__ void init(const dirichlet_dev& d, int i0, int i1, int s, int S, int X, int Y, int Z,
-										 int n_)
-	{
-		// (i0, i1) are the line's fixed coordinates: AXIS 0 -> (y, z); 1 -> (x, z); 2 -> (x, y)
-		n = n_;
-		const int cx = AXIS == 0 ? 0 : i0;
-		const int cy = AXIS == 0 ? i0 : (AXIS == 1 ? 0 : i1);
-		const int cz = AXIS == 2 ? 0 : i1;
-		// last applicable face of another axis, in precedence order x-min .. z-max
-		int order = -1;
-		line_val = 0.f;
-#pragma unroll
-		for (int f = 0; f < 6; f++)
-		{
-			const int ax = f >> 1;
-			if (ax == AXIS || !(d.face_mask & (1 << f)))
-				continue;
-			const int c = ax == 0 ? cx : (ax == 1 ? cy : cz);
-			const int e = ax == 0 ? X : (ax == 1 ? Y : Z);
-			const bool on = (f & 1) ? c == e - 1 : c == 0;
-			if (on && d.face_conds[f * S + s])
-			{
-				order = f;
-				line_val = d.face_vals[f * S + s];
-			}
-		}
-		line_face = order >= 0;
-		// own-axis faces apply only where they come later than the covering face
-		const int fmin = 2 * AXIS, fmax = 2 * AXIS + 1;
-		own_min = (d.face_mask & (1 << fmin)) && d.face_conds[fmin * S + s];
-		own_max = (d.face_mask & (1 << fmax)) && d.face_conds[fmax * S + s];
-		min_val = own_min ? d.face_vals[fmin * S + s] : 0.f;
-		max_val = own_max ? d.face_vals[fmax * S + s] : 0.f;
-		if (n == 1)
-		{
-			// one voxel along the axis: min and max face hit the same element, max written last
-			if (own_max)
-				min_val = max_val;
-			own_min = own_min || own_max;
-			own_max = false;
-		}
-		if (line_face)
-		{
-			if (order > fmin)
-			{
-				own_min = true;
-				min_val = line_val;
-			}
-			if (order > fmax && n > 1)
-			{
-				own_max = true;
-				max_val = line_val;
-			}
-		}
-		if (AXIS == 0)
-		{
-			vid_stride = 1;
-			base_vid = (long long)X * ((long long)cy + (long long)Y * cz);
-		}
-		else if (AXIS == 1)
-		{
-			vid_stride = X;
-			base_vid = (long long)cx + (long long)X * Y * cz;
-		}
-		else
-		{
-			vid_stride = (long long)X * Y;
-			base_vid = (long long)cx + (long long)X * cy;
-		}
-		any = line_face || own_min || own_max || d.has_interior;
-	}
-
-	__device__ __forceinline__ float apply(const dirichlet_dev& d, int i, int s, int S, float v) const
-	{
-		if (line_face)
-			v = line_val;
-		if (i == 0 && own_min)
-			v = min_val;
-		if (i == n - 1 && own_max)
-			v = max_val;
-		if (d.has_interior)
-		{
-			const long long vid = base_vid + (long long)i * vid_stride;
-			const unsigned int w = __ldg(&d.bits[vid >> 5]);
-			const unsigned int b = (unsigned int)(vid & 31);
-			if ((w >> b) & 1u)
-			{
-				const long long row = (long long)__ldg(&d.rank[vid >> 5]) + __popc(w & ((1u << b) - 1u));
-				if (d.iconds[row * S + s])
-					v = d.ivals[row * S + s];
-			}
-		}
-		return v;
-	}
-};
-
-__device__ __forceinline__ void block_range(int j, int base_len, int extra, int& p, int& L)
-{
-	p = j * base_len + min(j, extra);
-	L = base_len + (j < extra ? 1 : 0);
-}
-
-// Solve block j of one line.  `line` points at element 0 of the line, `stride` is the element
-// stride in floats.  `bp` is the b' column of this line's substrate (bp[i * bstride]).
-// carry_f / carry_t hold one value per block of this line at index k*cstride.  All threads of the
-// CTA must call this (it contains __syncthreads).
+// Solve block j of one line read from and written to global memory.  `line` points at element 0
+// of the line, `stride` is its element stride in floats.
 template <int M>
 __device__ __forceinline__ void solve_block(const sweep_args& a, float* __restrict__ line, long long stride,
 											const float* bp, const float* gq, const float* Gp, int bstride, float cs,
@@ -225,89 +54,12 @@ __device__ __forceinline__ void solve_block(const sweep_args& a, float* __restri
 		}
 	}
 	if (a.pre_dirichlet && active && ld.any)
-	{
-#pragma unroll
-		for (int k = 0; k < M; k++)
-			if (k < L)
-				d[k] = ld.apply(a.dir, p + k, s, S, d[k]);
-	}
+		dirichlet_block<M, false>(ld, a.dir, d, p, L, s, S);
 
-	// forward elimination from a zero carry: f_i = d_i - e_{i-1} f_{i-1},  e_{i-1} = c b'_{i-1}
-#pragma unroll
-	for (int k = 1; k < M; k++)
-		if (active && k < L)
-			d[k] = __fsub_rn(d[k], __fmul_rn(__fmul_rn(cs, bp[(p + k - 1) * bstride]), d[k - 1]));
-
-	if (active)
-	{
-#pragma unroll
-		for (int k = 0; k < M; k++)
-			if (k == L - 1)
-				carry_f[j * cstride] = d[k];
-	}
-	__syncthreads();
-
-	if (active && j > 0)
-	{
-		// d'_{p-1} = C_{j-1}: fold the blocks to the left, C_k = f^k_q + g^k_q C_{k-1}, where
-		// g^k_q = prod_{i=p_k-1}^{q_k-1} (-c b'_i)
-		float C = carry_f[0];
-		for (int k = 1; k < j; k++)
-			C = fmaf(gq[k * bstride], C, carry_f[k * cstride]);
-		// d'_i = f_i + g_i C with the running product g_i = prod_{m=p-1}^{i-1} (-c b'_m)
-		float g = 1.f;
-#pragma unroll
-		for (int k = 0; k < M; k++)
-			if (k < L)
-			{
-				g = __fmul_rn(g, -__fmul_rn(cs, bp[(p + k - 1) * bstride]));
-				d[k] = fmaf(g, C, d[k]);
-			}
-	}
-
-	// backward substitution from a zero carry: t_q = d'_q b'_q, t_i = (d'_i - c t_{i+1}) b'_i
-#pragma unroll
-	for (int k = M - 1; k >= 0; k--)
-	{
-		if (active && k < L)
-		{
-			const float bpk = bp[(p + k) * bstride];
-			if (k == L - 1)
-				d[k] = __fmul_rn(d[k], bpk);
-			else
-				d[k] = __fmul_rn(__fsub_rn(d[k], __fmul_rn(cs, d[k + 1 < M ? k + 1 : k])), bpk);
-		}
-	}
-
-	if (active)
-		carry_t[j * cstride] = d[0];
-	__syncthreads();
-
-	if (active && j < a.P - 1)
-	{
-		// x_{q+1} = X_{j+1}: fold the blocks to the right, X_k = t^k_p + G^k_p X_{k+1}, where
-		// G^k_p = prod_{i=p_k}^{q_k} (-c b'_i)
-		float Xc = carry_t[(a.P - 1) * cstride];
-		for (int k = a.P - 2; k > j; k--)
-			Xc = fmaf(Gp[k * bstride], Xc, carry_t[k * cstride]);
-		// x_i = t_i + G_i X with the running product G_i = prod_{m=i}^{q} (-c b'_m)
-		float G = 1.f;
-#pragma unroll
-		for (int k = M - 1; k >= 0; k--)
-			if (k < L)
-			{
-				G = __fmul_rn(G, -__fmul_rn(cs, bp[(p + k) * bstride]));
-				d[k] = fmaf(G, Xc, d[k]);
-			}
-	}
+	thomas_block<M, false>(d, L, p, j, a.P, bp, gq, Gp, bstride, cs, active, carry_f, carry_t, cstride);
 
 	if (a.post_dirichlet && active && ld.any)
-	{
-#pragma unroll
-		for (int k = 0; k < M; k++)
-			if (k < L)
-				d[k] = ld.apply(a.dir, p + k, s, S, d[k]);
-	}
+		dirichlet_block<M, false>(ld, a.dir, d, p, L, s, S);
 	{
 		float* ptr = line + (long long)(p + L - 1) * stride;
 #pragma unroll
@@ -319,34 +71,6 @@ __device__ __forceinline__ void solve_block(const sweep_args& a, float* __restri
 			}
 	}
 }
-
-// Stage the coefficients of substrates s0 .. s0+Sc-1 into shared memory: b' [n][Sc], c [Sc],
-// gq [P][Sc], Gp [P][Sc] (consecutive in `tab`).
-__device__ __forceinline__ void stage_table(const sweep_args& a, float* tab, int s0, int Sc)
-{
-	const int nt = blockDim.x * blockDim.y;
-	const int t0 = threadIdx.x + threadIdx.y * blockDim.x;
-	for (int t = t0; t < a.n * Sc; t += nt)
-	{
-		const int i = t / Sc, sl = t % Sc;
-		tab[t] = (s0 + sl < a.S) ? a.bp[(size_t)i * a.S + s0 + sl] : 0.f;
-	}
-	float* ctab = tab + a.n * Sc;
-	for (int t = t0; t < Sc; t += nt)
-		ctab[t] = (s0 + t < a.S) ? a.c[s0 + t] : 0.f;
-	float* gtab = ctab + Sc;
-	float* Gtab = gtab + a.P * Sc;
-	for (int t = t0; t < a.P * Sc; t += nt)
-	{
-		const int k = t / Sc, sl = t % Sc;
-		const bool ok = s0 + sl < a.S;
-		gtab[t] = ok ? a.gq[(size_t)k * a.S + s0 + sl] : 0.f;
-		Gtab[t] = ok ? a.Gp[(size_t)k * a.S + s0 + sl] : 0.f;
-	}
-	__syncthreads();
-}
-
-__host__ __device__ __forceinline__ int table_floats(int n, int P, int Sc) { return n * Sc + Sc + 2 * P * Sc; }
 
 // y (AXIS 1) and z (AXIS 2) sweeps.  Work item w = outer * col_tiles + tile; the grid strides over
 // items.  MAXT bounds the CTA size (32 * P) so the register budget follows the block count.
@@ -361,8 +85,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
 	const float* ctab = tab + a.n * a.S;
 	const float* gtab = ctab + a.S;
 	const float* Gtab = gtab + a.P * a.S;
-	float* carry_f = tab + table_floats(a.n, a.P, a.S);
+	float* fvals = const_cast<float*>(Gtab) + a.P * a.S;
+	unsigned char* fconds = reinterpret_cast<unsigned char*>(fvals + 6 * a.S);
+	float* carry_f = tab + table_floats(a.n, a.P, a.S, a.S);
 	float* carry_t = carry_f + a.P * 32;
+	stage_faces(a, fvals, fconds);
 	stage_table(a, tab, 0, a.S);
 
 	const int lane = threadIdx.x;
@@ -381,11 +108,17 @@ __global__ void __launch_bounds__(MAXT, MINB)
 		if (a.pre_dirichlet)
 		{
 			if (AXIS == 1)
-				ld.init<1>(a.dir, (int)(qq / S), (int)outer, s, S, a.X, a.Y, a.Z, a.n);
+			{
+				const int x = (int)(qq / S);
+				ld.init<1>(a.dir, fvals, fconds, x, (int)outer, s, S, a.X, a.Y, a.Z, a.n);
+				ld.load_mask<1>(a.dir, x + (long long)a.X * outer, j, a.P);
+			}
 			else
 			{
 				const long long XS = (long long)a.X * S;
-				ld.init<2>(a.dir, (int)((qq % XS) / S), (int)(qq / XS), s, S, a.X, a.Y, a.Z, a.n);
+				const int x = (int)((qq % XS) / S), y = (int)(qq / XS);
+				ld.init<2>(a.dir, fvals, fconds, x, y, s, S, a.X, a.Y, a.Z, a.n);
+				ld.load_mask<2>(a.dir, x + (long long)a.X * y, j, a.P);
 			}
 		}
 		float* line = a.data + outer * outer_stride + qq;
@@ -407,7 +140,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
 	const float* ctab = tab + a.n * Sc;
 	const float* gtab = ctab + Sc;
 	const float* Gtab = gtab + a.P * Sc;
-	float* carries = tab + table_floats(a.n, a.P, Sc);
+	float* fvals = const_cast<float*>(Gtab) + a.P * Sc;
+	unsigned char* fconds = reinterpret_cast<unsigned char*>(fvals + 6 * a.S);
+	float* carries = tab + table_floats(a.n, a.P, Sc, a.S);
+	stage_faces(a, fvals, fconds);
 	stage_table(a, tab, s0, Sc);
 
 	const int t = threadIdx.x;
@@ -427,54 +163,14 @@ __global__ void __launch_bounds__(MAXT, MINB)
 		line_dirichlet ld;
 		ld.any = false;
 		if (a.pre_dirichlet)
-			ld.init<0>(a.dir, (int)(rr % a.Y), (int)(rr / a.Y), ss, a.S, a.X, a.Y, a.Z, a.n);
+		{
+			ld.init<0>(a.dir, fvals, fconds, (int)(rr % a.Y), (int)(rr / a.Y), ss, a.S, a.X, a.Y, a.Z, a.n);
+			ld.load_mask<0>(a.dir, rr, j, a.P);
+		}
 		float* line = a.data + rr * (long long)a.X * a.S + ss;
 		solve_block<M>(a, line, a.S, tab + sl, gtab + sl, Gtab + sl, Sc, ctab[sl], ss, j, active, carry_f, carry_t, Sc,
 					   ld);
 	}
-}
-
-static int sm_count(int device)
-{
-	static int cached[64] = { 0 };
-	if (device >= 0 && device < 64 && cached[device])
-		return cached[device];
-	int n = 0;
-	cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
-	if (n <= 0)
-		n = 148;
-	if (device >= 0 && device < 64)
-		cached[device] = n;
-	return n;
-}
-
-template <typename K>
-static int persistent_grid(K kernel, int threads, size_t smem, long long items, int device)
-{
-	int per_sm = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
-	if (per_sm <= 0)
-		per_sm = 1;
-	const long long g = (long long)per_sm * sm_count(device);
-	return (int)std::max<long long>(1, std::min<long long>(g, items));
-}
-
-template <typename K>
-static int set_smem(K kernel, size_t smem)
-{
-	int dev = 0, optin = 0;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-	if (optin > 0 && smem > (size_t)optin)
-		return fail(BFVM_ERR_INVALID_ARGUMENT, "axis length x substrates too large for the staged coefficient table ("
-												   + std::to_string(smem) + " bytes of shared memory)");
-	if (smem > 48 * 1024)
-	{
-		cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		if (e != cudaSuccess)
-			return cuda_fail(e, "cudaFuncSetAttribute(max dynamic shared memory)");
-	}
-	return BFVM_OK;
 }
 
 template <int M, int AXIS, int MAXT, int MINB>
@@ -485,7 +181,7 @@ static int launch_columns(bfvm_solver* st, const sweep_args& a)
 	const long long tiles = (ncols + 31) / 32;
 	const long long outers = AXIS == 1 ? Z : 1;
 	const long long items = outers * tiles;
-	const size_t smem = ((size_t)table_floats(a.n, a.P, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float);
+	const size_t smem = ((size_t)table_floats(a.n, a.P, (int)S, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float);
 	auto kernel = sweep_columns<M, AXIS, MAXT, MINB>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
@@ -512,7 +208,8 @@ static int launch_sweep_m(bfvm_solver* st, int axis, const sweep_args& a)
 		const int threads = rows_per_cta * per_row;
 		const long long groups = (nrows + rows_per_cta - 1) / rows_per_cta;
 		const int chunks = (int)((S + Sc - 1) / Sc);
-		const size_t smem = ((size_t)table_floats(a.n, a.P, Sc) + 2 * (size_t)rows_per_cta * a.P * Sc) * sizeof(float);
+		const size_t smem =
+			((size_t)table_floats(a.n, a.P, Sc, (int)S) + 2 * (size_t)rows_per_cta * a.P * Sc) * sizeof(float);
 		auto kernel = threads <= 320 ? sweep_rows<M, 320, 2> : sweep_rows<M, 512, 1>;
 		int rc = set_smem(kernel, smem);
 		if (rc)
@@ -550,6 +247,14 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 	a.dir = st->dirichlet();
 	a.pre_dirichlet = (a.dir.face_mask != 0 || a.dir.has_interior) ? 1 : 0;
 	a.post_dirichlet = final_dirichlet ? a.pre_dirichlet : 0;
+	a.err = st->dev_error;
+	if (st->use_tma)
+	{
+		bool handled = false;
+		int rc = launch_sweep_tma(st, axis, a, handled);
+		if (rc || handled)
+			return rc;
+	}
 	if (pl.M == 32)
 		return launch_sweep_m<32>(st, axis, a);
 	return launch_sweep_m<64>(st, axis, a);

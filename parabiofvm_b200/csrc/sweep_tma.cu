@@ -1,0 +1,400 @@
+// Sweeps with the field staged through shared memory by the Tensor Memory Accelerator.
+//
+// A persistent CTA owns a tile of 32 lines at a time: 32 adjacent columns of the x*s plane (y
+// sweep) or of the y*x*s plane (z sweep), or R = 32/S whole rows (x sweep, R rows x S substrate
+// lines).  Warp j holds register block j of every line of the tile (blockDim = (32, P)).  Two
+// shared-memory stages alternate: while the CTA solves the tile in one stage, the TMA copies the
+// next tile into the other, so the HBM reads of the next tile overlap the recurrences of this one.
+// Results are written straight from registers with coalesced stores.
+//
+//   y sweep: 3D tensor map over [Z][Y][XS], boxes of 32 columns x box_h rows
+//   z sweep: 2D tensor map over [Z][Y*XS], boxes of 32 columns x box_h planes
+//   x sweep: one 1D bulk copy per row, into rows padded so the 32 lanes hit distinct banks
+//
+// Copies complete on an mbarrier per stage; every wait is bounded by a clock limit, after which
+// the kernel raises DEVERR_TIMEOUT, lets its copies in flight land (again bounded) and returns.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
+
+#include "sweep_common.cuh"
+
+namespace bfvm {
+
+static constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL; // about two seconds
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+				 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+	uint32_t ok;
+	asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+				 "selp.u32 %0, 1, 0, p;\n}"
+				 : "=r"(ok)
+				 : "r"(smem_addr(bar)), "r"(parity)
+				 : "memory");
+	return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+	const long long t0 = clock64();
+	while (!mbar_try_wait(bar, parity))
+		if (clock64() - t0 > WAIT_LIMIT_CYCLES)
+			return false;
+	return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar)
+{
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+				 ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_addr(bar))
+				 : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar)
+{
+	asm volatile(
+		"cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+		::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+		: "memory");
+}
+
+__device__ __forceinline__ void bulk_load(float* dst, const float* src, uint32_t bytes, uint64_t* bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+				 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+				 : "memory");
+}
+
+struct tma_tile
+{
+	int axis;			 // 0 x (rows), 1 y, 2 z
+	long long items;	 // tiles
+	long long ncols;	 // columns of the plane (y, z)
+	long long col_tiles; // 32-column tiles per plane (y, z)
+	long long outer_stride, line_stride;
+	int box_h, nbox;	 // TMA boxes along the line (y, z)
+	int R, row_pitch;	 // rows per tile and padded row length in floats (x)
+	long long nrows;
+	long long XS;
+	int stage_floats;
+};
+
+// Issue the copies of tile w into `dst`, completing on `bar` (one thread).
+__device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMap* map, const tma_tile& tt, long long w,
+										   float* dst, uint64_t* bar)
+{
+	if (tt.axis == 0)
+	{
+		const long long row0 = w * tt.R;
+		const int rows = (int)min((long long)tt.R, tt.nrows - row0);
+		const uint32_t row_bytes = (uint32_t)(tt.XS * sizeof(float));
+		mbar_expect_tx(bar, row_bytes * rows);
+		for (int r = 0; r < rows; r++)
+			bulk_load(dst + r * tt.row_pitch, a.data + (row0 + r) * tt.XS, row_bytes, bar);
+		return;
+	}
+	const long long outer = w / tt.col_tiles;
+	const int c0 = (int)((w % tt.col_tiles) * 32);
+	mbar_expect_tx(bar, (uint32_t)(tt.nbox * tt.box_h * 32 * sizeof(float)));
+	for (int b = 0; b < tt.nbox; b++)
+	{
+		if (tt.axis == 1)
+			tma_load_3d(dst + b * tt.box_h * 32, map, c0, b * tt.box_h, (int)outer, bar);
+		else
+			tma_load_2d(dst + b * tt.box_h * 32, map, c0, b * tt.box_h, bar);
+	}
+}
+
+template <bool UNI, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
+	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
+					 const __grid_constant__ tma_tile tt)
+{
+	constexpr int M = 32;
+	extern __shared__ __align__(128) unsigned char smem_raw[];
+	// stages on a 1024-byte boundary (TMA destinations), then tables, carries and the barriers
+	float* stage[2];
+	stage[0] = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+	stage[1] = stage[0] + tt.stage_floats;
+	float* tab = stage[1] + tt.stage_floats;
+	const int S = a.S;
+	const float* ctab = tab + a.n * S;
+	const float* gtab = ctab + S;
+	const float* Gtab = gtab + a.P * S;
+	float* fvals = const_cast<float*>(Gtab) + a.P * S;
+	unsigned char* fconds = reinterpret_cast<unsigned char*>(fvals + 6 * S);
+	float* carry_f = tab + table_floats(a.n, a.P, S, S);
+	float* carry_t = carry_f + a.P * 32;
+	uint64_t* bars =
+		reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(carry_t + a.P * 32) + 7) & ~uintptr_t(7));
+
+	const int lane = threadIdx.x;
+	const int j = threadIdx.y;
+	const bool leader = lane == 0 && j == 0;
+	if (leader)
+	{
+		mbar_init(&bars[0], 1);
+		mbar_init(&bars[1], 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	stage_faces(a, fvals, fconds);
+	stage_table(a, tab, 0, S); // ends with __syncthreads, which also publishes the barrier init
+
+	int p, L;
+	block_range(j, a.base_len, a.extra, p, L);
+
+	long long w = blockIdx.x;
+	if (leader && w < tt.items)
+		issue_tile(a, &map, tt, w, stage[0], &bars[0]);
+
+	bool failed = false;
+	int it = 0;
+	for (; w < tt.items; w += gridDim.x, it++)
+	{
+		const int st = it & 1;
+		const uint32_t parity = (uint32_t)((it >> 1) & 1);
+		if (leader && w + gridDim.x < tt.items)
+		{
+			// the other stage was released by the __syncthreads that ended the previous tile
+			asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+			issue_tile(a, &map, tt, w + gridDim.x, stage[st ^ 1], &bars[st ^ 1]);
+		}
+		const bool ok = mbar_wait(&bars[st], parity);
+		if (!__syncthreads_and(ok))
+		{
+			failed = true;
+			break;
+		}
+
+		// this thread's line in the tile
+		const float* cur = stage[st];
+		bool active;
+		int s, sbase, sstride;
+		float* line;
+		long long gstride;
+		line_dirichlet ld;
+		ld.any = false;
+		if (tt.axis == 0)
+		{
+			const int rl = lane / S;
+			s = lane - rl * S;
+			const long long row = w * tt.R + rl;
+			active = rl < tt.R && row < tt.nrows;
+			const long long rr = active ? row : 0;
+			sbase = (rl < tt.R ? rl : 0) * tt.row_pitch + s; // lanes past the last row read row 0
+			sstride = S;
+			line = a.data + rr * tt.XS + s;
+			gstride = S;
+			if (a.pre_dirichlet && active)
+			{
+				ld.init<0>(a.dir, fvals, fconds, (int)(rr % a.Y), (int)(rr / a.Y), s, S, a.X, a.Y, a.Z, a.n);
+				ld.load_mask<0>(a.dir, rr, j, a.P);
+			}
+		}
+		else
+		{
+			const long long outer = w / tt.col_tiles;
+			const long long q = (w % tt.col_tiles) * 32 + lane;
+			active = q < tt.ncols;
+			const long long qq = active ? q : 0;
+			s = (int)(qq % S);
+			sbase = lane;
+			sstride = 32;
+			line = a.data + outer * tt.outer_stride + qq;
+			gstride = tt.line_stride;
+			if (a.pre_dirichlet && active)
+			{
+				if (tt.axis == 1)
+				{
+					const int x = (int)(qq / S);
+					ld.init<1>(a.dir, fvals, fconds, x, (int)outer, s, S, a.X, a.Y, a.Z, a.n);
+					ld.load_mask<1>(a.dir, x + (long long)a.X * outer, j, a.P);
+				}
+				else
+				{
+					const int x = (int)((qq % tt.XS) / S), y = (int)(qq / tt.XS);
+					ld.init<2>(a.dir, fvals, fconds, x, y, s, S, a.X, a.Y, a.Z, a.n);
+					ld.load_mask<2>(a.dir, x + (long long)a.X * y, j, a.P);
+				}
+			}
+		}
+
+		float d[M];
+#pragma unroll
+		for (int k = 0; k < M; k++)
+			d[k] = (UNI || k < L) ? cur[sbase + (p + k) * sstride] : 0.f;
+		if (ld.any)
+			dirichlet_block<M, UNI>(ld, a.dir, d, p, L, s, S);
+
+		thomas_block<M, UNI>(d, L, p, j, a.P, tab + s, gtab + s, Gtab + s, S, ctab[s], active, carry_f + lane,
+							 carry_t + lane, 32);
+
+		if (a.post_dirichlet && ld.any)
+			dirichlet_block<M, UNI>(ld, a.dir, d, p, L, s, S);
+		if (active)
+		{
+			float* ptr = line + (long long)p * gstride;
+#pragma unroll
+			for (int k = 0; k < M; k++)
+				if (UNI || k < L)
+				{
+					*ptr = d[k];
+					ptr += gstride;
+				}
+		}
+		__syncthreads(); // stage st fully read before it is refilled
+	}
+
+	if (failed && leader)
+	{
+		atomicOr(a.err, DEVERR_TIMEOUT);
+		// let the copies already issued land before the CTA exits (bounded waits)
+		mbar_wait(&bars[it & 1], (uint32_t)((it >> 1) & 1));
+		if (w + gridDim.x < tt.items)
+			mbar_wait(&bars[(it & 1) ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+	}
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	static bool tried = false;
+	if (!tried)
+	{
+		tried = true;
+		cudaDriverEntryPointQueryResult q;
+		void* p = nullptr;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess
+			&& q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+		else
+			(void)cudaGetLastError();
+	}
+	return fn;
+}
+
+static constexpr int TMA_MAX_P = 16;
+
+template <bool UNI, int MAXT, int MINB>
+static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
+							  size_t smem)
+{
+	auto kernel = sweep_tma_kernel<UNI, MAXT, MINB>;
+	int rc = set_smem(kernel, smem);
+	if (rc)
+		return rc;
+	const int threads = 32 * a.P;
+	const int grid = persistent_grid(kernel, threads, smem, tt.items, st->device);
+	kernel<<<grid, dim3(32, a.P), smem, st->stream>>>(a, map, tt);
+	return check_launch(st, tt.axis == 0 ? "sweep_tma<x>" : (tt.axis == 1 ? "sweep_tma<y>" : "sweep_tma<z>"));
+}
+
+int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled)
+{
+	handled = false;
+	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2], S = st->S;
+	const long long XS = X * S;
+	const sweep_plan& pl = st->plan[axis];
+	// shapes the TMA path covers: 16-byte row strides, at most 16 blocks of 32 per line, and for
+	// the x sweep whole rows of at most 32 substrate lines per tile
+	if (pl.M != 32 || a.P > TMA_MAX_P || XS % 4 != 0 || (axis == 0 && S > 32) || a.n < 2)
+		return BFVM_OK;
+	auto encode = encode_fn();
+	if (!encode)
+		return BFVM_OK;
+
+	tma_tile tt;
+	std::memset(&tt, 0, sizeof(tt));
+	tt.axis = axis;
+	tt.XS = XS;
+	CUtensorMap map;
+	std::memset(&map, 0, sizeof(map));
+	if (axis == 0)
+	{
+		tt.R = (int)(32 / S);
+		tt.nrows = Y * Z;
+		tt.items = (tt.nrows + tt.R - 1) / tt.R;
+		// pad rows so that lane (r, s) = r*pitch + s spreads over the banks, keeping 16-byte rows
+		int pad = (int)(((S % 32) - (XS % 32) + 64) % 32);
+		pad = (pad + 3) / 4 * 4;
+		tt.row_pitch = (int)XS + pad;
+		tt.stage_floats = (tt.R * tt.row_pitch + 31) / 32 * 32;
+	}
+	else
+	{
+		const long long n = axis == 1 ? Y : Z;
+		tt.nbox = (int)((n + 255) / 256);
+		tt.box_h = (int)((n + tt.nbox - 1) / tt.nbox);
+		tt.ncols = axis == 1 ? XS : Y * XS;
+		tt.col_tiles = (tt.ncols + 31) / 32;
+		tt.items = (axis == 1 ? Z : 1) * tt.col_tiles;
+		tt.outer_stride = axis == 1 ? Y * XS : 0;
+		tt.line_stride = axis == 1 ? XS : Y * XS;
+		tt.stage_floats = tt.nbox * tt.box_h * 32;
+		cuuint64_t dims[3], strides[2];
+		cuuint32_t box[3], estr[3] = { 1, 1, 1 };
+		cuuint32_t rank;
+		if (axis == 1)
+		{
+			rank = 3;
+			dims[0] = (cuuint64_t)XS;
+			dims[1] = (cuuint64_t)Y;
+			dims[2] = (cuuint64_t)Z;
+			strides[0] = (cuuint64_t)(XS * sizeof(float));
+			strides[1] = (cuuint64_t)(Y * XS * sizeof(float));
+			box[0] = 32;
+			box[1] = (cuuint32_t)tt.box_h;
+			box[2] = 1;
+		}
+		else
+		{
+			rank = 2;
+			dims[0] = (cuuint64_t)(Y * XS);
+			dims[1] = (cuuint64_t)Z;
+			strides[0] = (cuuint64_t)(Y * XS * sizeof(float));
+			box[0] = 32;
+			box[1] = (cuuint32_t)tt.box_h;
+		}
+		CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, st->dens, dims, strides, box, estr,
+							CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+							CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+		if (r != CUDA_SUCCESS)
+			return BFVM_OK; // fall back to the direct kernels
+	}
+	const size_t smem =
+		1024 + (2 * (size_t)tt.stage_floats + table_floats(a.n, a.P, (int)S, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float)
+		+ 8 + 2 * sizeof(uint64_t);
+	int dev = 0, optin = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+	if (smem > (size_t)optin)
+		return BFVM_OK;
+
+	handled = true;
+	const bool uni = a.extra == 0 && a.base_len == 32;
+	if (a.P <= 10)
+		return uni ? launch_tma_variant<true, 320, 2>(st, a, map, tt, smem)
+				   : launch_tma_variant<false, 320, 2>(st, a, map, tt, smem);
+	return uni ? launch_tma_variant<true, 512, 1>(st, a, map, tt, smem)
+			   : launch_tma_variant<false, 512, 1>(st, a, map, tt, smem);
+}
+
+} // namespace bfvm

@@ -74,7 +74,12 @@ def test_cpu_runnable_config_100_steps():
     assert e32 < 1e-4
     assert g_64 <= 1.5 * o32_64 + 1e-7
     assert rel_l2(g.internalized(), o32.internalized()) < 1e-5
-    assert rel_err(g.gradients(), o32.gradients(), floor_frac=1e-3) < 1e-3
+    # the gradient operator is exactly rounded (bit-identical on identical fields, see
+    # test_secretion_bit_exact_on_multi_block_mesh), so its error is the field's carried through
+    # (u[i+1] - u[i-1]) / (2h): at most max|du| / h
+    du = np.max(np.abs(d.astype(np.float64) - o32.densities()))
+    dg = np.max(np.abs(g.gradients().astype(np.float64) - o32.gradients()))
+    assert dg <= du / min(scn.voxel_shape) * 1.001 + 1e-12
 
 
 @pytest.mark.parametrize("dims", [1, 2, 3])
