@@ -271,6 +271,9 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     s = make_solver(w, device=local_rank)
     s.set_stream(stream.cuda_stream)
+    for opt in args.option:
+        name, val = opt.split("=", 1)
+        s.set_option(name, int(val))
     VS = w.voxel_count * w.S
 
     def barrier():
@@ -407,6 +410,7 @@ def run_ours(args):
         return 0
     w_text = WORKLOADS[args.workload]["text"]
     line = {
+        "options": args.option,
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
@@ -436,6 +440,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plain-320")
     ap.add_argument("--kernel-reps", type=int, default=5)
+    ap.add_argument("--option", action="append", default=[],
+                    help="solver tuning option name=value (bfvm_set_option), e.g. sweep_ctas_per_sm=1")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)

@@ -131,6 +131,14 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step);
 /* Wait for the stream (solver::wait_for_all) and report device-side errors. */
 int bfvm_synchronize(bfvm_solver* s);
 
+/*
+ * Tuning options (no counterpart in the reference): "tma_sweeps" 0/1 stages sweep tiles through
+ * shared memory with the TMA (default 1); "sweep_ctas_per_sm" 0 (auto), 1 or 2 picks the TMA
+ * sweep occupancy for lines of up to 320 voxels; "sweep_uniform_blocks" 0/1 allows the kernel
+ * variant specialised for lines made of equal 32-voxel blocks.  Results do not depend on them.
+ */
+int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value);
+
 /* Device pointers to the resident field and gradients, for zero-copy use by other GPU code. */
 int bfvm_device_densities(bfvm_solver* s, float** ptr, int64_t* count);
 int bfvm_device_gradients(bfvm_solver* s, float** ptr, int64_t* count);

@@ -153,6 +153,9 @@ class Solver:
     def synchronize(self):
         check(self._lib.bfvm_synchronize(self._h))
 
+    def set_option(self, name, value):
+        check(self._lib.bfvm_set_option(self._h, name.encode(), int(value)))
+
     # -- device access ------------------------------------------------------------------------------
     def set_stream(self, stream_ptr):
         check(self._lib.bfvm_set_stream(self._h, ctypes.c_void_p(int(stream_ptr)) if stream_ptr else None))

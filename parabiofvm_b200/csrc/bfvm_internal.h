@@ -48,9 +48,13 @@ struct dirichlet_dev
 	const float* ivals;				  // [N][S]
 	const unsigned char* iconds;	  // [N][S]
 	int has_interior;
-	// per sweep axis: bit k of block_mask[axis][line * P + j] marks element k of block j of a line
-	// as an interior Dirichlet voxel (lines: x sweep y + Y*z, y sweep x + X*z, z sweep x + X*y)
-	const unsigned long long* block_mask[3];
+	// Per sweep axis, one descriptor per (line, block): .x has bit k set when element k of block j
+	// of the line is an interior Dirichlet voxel, .y is the row of its first such element in
+	// axis_vals / axis_conds, which list the marked elements in (line, block, element) order
+	// (lines: x sweep y + Y*z, y sweep x + X*z, z sweep x + X*y; descriptor index line * P + j).
+	const ulonglong2* block_desc[3];
+	const float* axis_vals[3];			// [marked elements][S]
+	const unsigned char* axis_conds[3]; // [marked elements][S]
 };
 
 // One sweep axis: the precomputed Thomas coefficients of src/solver/host/diffusion_solver.cpp:72-142
@@ -130,7 +134,9 @@ struct bfvm_solver
 	int* dir_rank = nullptr;
 	float* dir_vals = nullptr;
 	unsigned char* dir_conds = nullptr;
-	unsigned long long* dir_block_mask[3] = { nullptr, nullptr, nullptr };
+	ulonglong2* dir_block_desc[3] = { nullptr, nullptr, nullptr };
+	float* dir_axis_vals[3] = { nullptr, nullptr, nullptr };
+	unsigned char* dir_axis_conds[3] = { nullptr, nullptr, nullptr };
 
 	bfvm::agent_state ag;
 
@@ -138,7 +144,9 @@ struct bfvm_solver
 	int* host_error = nullptr; // pinned mirror
 
 	long long launches = 0;
-	bool use_tma = true; // stage sweeps through shared memory with the TMA where the shape allows
+	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
+	int sweep_ctas_per_sm = 0; // TMA sweep occupancy for lines of <= 320 voxels: 0 auto, 1 or 2
+	int sweep_uniform = 1;	   // specialise the sweeps for lines split into equal blocks of 32
 
 	// graphs for run_steps: [recompute]
 	cudaGraphExec_t step_graph[2] = { nullptr, nullptr };
@@ -157,7 +165,11 @@ struct bfvm_solver
 		d.iconds = dir_conds;
 		d.has_interior = n_interior > 0;
 		for (int a = 0; a < 3; a++)
-			d.block_mask[a] = dir_block_mask[a];
+		{
+			d.block_desc[a] = dir_block_desc[a];
+			d.axis_vals[a] = dir_axis_vals[a];
+			d.axis_conds[a] = dir_axis_conds[a];
+		}
 		return d;
 	}
 };

@@ -53,6 +53,70 @@ __global__ void __launch_bounds__(256) gradient_kernel(const float* __restrict__
 	g[2 * total + i] = gz;
 }
 
+// 3D gradients when S % 4 == 0: a thread owns a float4 of four consecutive substrates of one voxel
+// column (x, y) and walks ZC planes of z, keeping u(z-1), u(z), u(z+1) in registers, so each
+// element costs one streamed 16-byte load of u(z+1) plus the x and y neighbours (L1/L2 hits) and
+// three 16-byte stores.  All four substrates share x, so the border logic is per thread.
+static constexpr int GRAD_ZC = 32;
+
+__device__ __forceinline__ float4 f4sub_mul(float4 a, float4 b, float f)
+{
+	return make_float4(__fmul_rn(__fsub_rn(a.x, b.x), f), __fmul_rn(__fsub_rn(a.y, b.y), f),
+					   __fmul_rn(__fsub_rn(a.z, b.z), f), __fmul_rn(__fsub_rn(a.w, b.w), f));
+}
+
+__global__ void __launch_bounds__(256) gradient3d_vec4_kernel(const float4* __restrict__ u, float4* __restrict__ g,
+															   long long total4, int S4, int X, int Y, int Z, float bx,
+															   float cx, float by, float cy, float bz, float cz)
+{
+	const int XS4 = X * S4;
+	const int q4 = blockIdx.x * blockDim.x + threadIdx.x;
+	if (q4 >= XS4)
+		return;
+	const int y = blockIdx.y;
+	const int z0 = blockIdx.z * GRAD_ZC;
+	const int z1 = min(Z, z0 + GRAD_ZC);
+	const int x = q4 / S4;
+	const long long plane = (long long)Y * XS4;
+	const long long row = (long long)y * XS4 + q4;
+
+	// x neighbours: +-S4 float4s; y neighbours: +-XS4
+	const int xo_hi = x == X - 1 ? 0 : S4, xo_lo = x == 0 ? 0 : S4;
+	const float fx = (x == 0 || x == X - 1) ? bx : cx;
+	const int yo_hi = y == Y - 1 ? 0 : XS4, yo_lo = y == 0 ? 0 : XS4;
+	const float fy = (y == 0 || y == Y - 1) ? by : cy;
+
+	float4 prev = z0 > 0 ? __ldg(&u[(long long)(z0 - 1) * plane + row]) : make_float4(0, 0, 0, 0);
+	float4 cur = __ldg(&u[(long long)z0 * plane + row]);
+	for (int z = z0; z < z1; z++)
+	{
+		const long long i = (long long)z * plane + row;
+		const float4 next = z + 1 < Z ? __ldg(&u[i + plane]) : cur;
+		float4 gx, gy, gz;
+		if (X == 1)
+			gx = make_float4(0, 0, 0, 0);
+		else
+			gx = f4sub_mul(__ldg(&u[i + xo_hi]), __ldg(&u[i - xo_lo]), fx);
+		if (Y == 1)
+			gy = make_float4(0, 0, 0, 0);
+		else
+			gy = f4sub_mul(__ldg(&u[i + yo_hi]), __ldg(&u[i - yo_lo]), fy);
+		if (Z == 1)
+			gz = make_float4(0, 0, 0, 0);
+		else if (z == 0)
+			gz = f4sub_mul(next, cur, bz);
+		else if (z == Z - 1)
+			gz = f4sub_mul(cur, prev, bz);
+		else
+			gz = f4sub_mul(next, prev, cz);
+		__stcs(&g[i], gx);
+		__stcs(&g[total4 + i], gy);
+		__stcs(&g[2 * total4 + i], gz);
+		prev = cur;
+		cur = next;
+	}
+}
+
 int launch_gradient(bfvm_solver* st)
 {
 	const long long total = st->V * st->S;
@@ -64,6 +128,15 @@ int launch_gradient(bfvm_solver* st)
 	}
 	const int threads = 256;
 	const int S = st->S, X = st->grid[0], Y = st->grid[1], Z = st->grid[2];
+	if (st->dims == 3 && S % 4 == 0)
+	{
+		const int XS4 = X * (S / 4);
+		const dim3 blocks((unsigned)((XS4 + threads - 1) / threads), (unsigned)Y, (unsigned)((Z + GRAD_ZC - 1) / GRAD_ZC));
+		gradient3d_vec4_kernel<<<blocks, threads, 0, st->stream>>>(
+			reinterpret_cast<const float4*>(st->dens), reinterpret_cast<float4*>(st->grad), total / 4, S / 4, X, Y, Z, f[0],
+			f[1], f[2], f[3], f[4], f[5]);
+		return check_launch(st, "gradient3d_vec4_kernel");
+	}
 	const dim3 blocks((unsigned)((X * S + threads - 1) / threads), (unsigned)Y, (unsigned)Z);
 	if (st->dims == 1)
 		gradient_kernel<1><<<blocks, threads, 0, st->stream>>>(st->dens, st->grad, total, S, X, Y, Z, f[0], f[1], f[2],

@@ -67,14 +67,18 @@ __device__ __forceinline__ float apply_dirichlet(const dirichlet_dev& d, float v
 // cost is a select plus one bitmap probe.
 struct line_dirichlet
 {
-	bool any;			 // anything to apply on this line
-	bool line_face;		 // a face of another axis covers the line (after own faces in precedence)
-	float line_val;
-	bool own_min, own_max; // sweep-axis faces at element 0 / n-1 (already merged with line faces)
-	float min_val, max_val;
-	long long base_vid, vid_stride;
-	int n;
-	unsigned long long mask; // interior Dirichlet elements of this thread's block
+	// every field has a neutral default: a line with no conditions applies nothing
+	bool any = false;		// anything to apply on this line
+	bool line_face = false; // a face of another axis covers the line (after own faces in precedence)
+	float line_val = 0.f;
+	bool own_min = false, own_max = false; // sweep-axis faces at element 0 / n-1 (merged with line faces)
+	float min_val = 0.f, max_val = 0.f;
+	long long base_vid = 0, vid_stride = 0;
+	int n = 0;
+	unsigned long long mask = 0ull; // interior Dirichlet elements of this thread's block
+	long long row0 = 0;				// row of its first marked element in the axis tables
+	const float* avals = nullptr;
+	const unsigned char* aconds = nullptr;
 
 	// fvals / fconds: the face values and conditions [6][S] staged in shared memory
 	template <int AXIS>
@@ -148,6 +152,9 @@ struct line_dirichlet
 			base_vid = (long long)cx + (long long)X * cy;
 		}
 		mask = 0ull;
+		row0 = 0;
+		avals = nullptr;
+		aconds = nullptr;
 		any = line_face || own_min || own_max;
 	}
 
@@ -157,9 +164,20 @@ struct line_dirichlet
 	{
 		if (d.has_interior)
 		{
-			mask = d.block_mask[AXIS][line * P + j];
+			const ulonglong2 desc = d.block_desc[AXIS][line * P + j];
+			mask = desc.x;
+			row0 = (long long)desc.y;
+			avals = d.axis_vals[AXIS];
+			aconds = d.axis_conds[AXIS];
 			any = any || mask != 0ull;
 		}
+	}
+
+	// interior Dirichlet value of marked element k of this block (substrate s), or v
+	__device__ __forceinline__ float marked(int k, int s, int S, float v) const
+	{
+		const long long row = row0 + __popcll(mask & ((1ull << k) - 1ull));
+		return aconds[row * S + s] ? avals[row * S + s] : v;
 	}
 
 	// the interior Dirichlet value of line element i (substrate s), or v if it has no condition
@@ -243,7 +261,34 @@ __device__ __forceinline__ void dirichlet_block(const line_dirichlet& ld, const 
 #pragma unroll
 		for (int k = 0; k < M; k++)
 			if ((ld.mask >> k) & 1ull)
-				d[k] = ld.interior(dir, p + k, s, S, d[k]);
+				d[k] = ld.marked(k, s, S, d[k]);
+	}
+}
+
+// faces only (the interior marks are applied separately by the TMA kernels)
+template <int M, bool UNI>
+__device__ __forceinline__ void dirichlet_faces(const line_dirichlet& ld, float (&d)[M], int p, int L)
+{
+	if (ld.line_face)
+	{
+#pragma unroll
+		for (int k = 0; k < M; k++)
+			if (UNI || k < L)
+				d[k] = ld.line_val;
+	}
+	if (ld.own_min && p == 0)
+		d[0] = ld.min_val;
+	if (ld.own_max && p + L == ld.n)
+	{
+		if (UNI)
+			d[M - 1] = ld.max_val;
+		else
+		{
+#pragma unroll
+			for (int k = 0; k < M; k++)
+				if (k == L - 1)
+					d[k] = ld.max_val;
+		}
 	}
 }
 
@@ -263,6 +308,7 @@ __device__ __forceinline__ void thomas_block(float (&d)[M], int L, int p, int j,
 		if (UNI || k < L)
 			d[k] = __fsub_rn(d[k], __fmul_rn(__fmul_rn(cs, bp[(p + k - 1) * bstride]), d[k - 1]));
 
+	asm volatile("" ::: "memory"); // keep the next pass's table loads from being hoisted here
 	if (active)
 	{
 		if (UNI)
@@ -295,6 +341,7 @@ __device__ __forceinline__ void thomas_block(float (&d)[M], int L, int p, int j,
 	}
 
 	// backward substitution from a zero carry: t_q = d'_q b'_q, t_i = (d'_i - c t_{i+1}) b'_i
+	asm volatile("" ::: "memory");
 #pragma unroll
 	for (int k = M - 1; k >= 0; k--)
 	{
@@ -308,6 +355,7 @@ __device__ __forceinline__ void thomas_block(float (&d)[M], int L, int p, int j,
 		}
 	}
 
+	asm volatile("" ::: "memory");
 	if (active)
 		carry_t[j * cstride] = d[0];
 	__syncthreads();

@@ -92,6 +92,7 @@ struct tma_tile
 	long long nrows;
 	long long XS;
 	int stage_floats;
+	int stages; // pipeline depth (NST)
 };
 
 // Issue the copies of tile w into `dst`, completing on `bar` (one thread).
@@ -120,6 +121,70 @@ __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMa
 	}
 }
 
+// Where line `lane` of tile w lives: in the shared-memory stage (sbase + i*sstride) and in the
+// field (line + i*gstride), and its Dirichlet conditions.
+struct tile_line
+{
+	bool active;
+	int s, sbase, sstride;
+	float* line;
+	long long gstride;
+	long long rr;			// x sweep: row index y + Y*z
+	long long outer, qq;	// y/z sweeps: plane and column
+
+	__device__ __forceinline__ void locate(const sweep_args& a, const tma_tile& tt, long long w, int lane)
+	{
+		const int S = a.S;
+		if (tt.axis == 0)
+		{
+			const int rl = lane / S;
+			s = lane - rl * S;
+			const long long row = w * tt.R + rl;
+			active = rl < tt.R && row < tt.nrows;
+			rr = active ? row : 0;
+			sbase = (rl < tt.R ? rl : 0) * tt.row_pitch + s; // lanes past the last row read row 0
+			sstride = S;
+			line = a.data + rr * tt.XS + s;
+			gstride = S;
+		}
+		else
+		{
+			outer = w / tt.col_tiles;
+			const long long q = (w % tt.col_tiles) * 32 + lane;
+			active = q < tt.ncols;
+			qq = active ? q : 0;
+			s = (int)(qq % S);
+			sbase = lane;
+			sstride = 32;
+			line = a.data + outer * tt.outer_stride + qq;
+			gstride = tt.line_stride;
+		}
+	}
+
+	__device__ __forceinline__ void dirichlet(const sweep_args& a, const tma_tile& tt, const float* fvals,
+											  const unsigned char* fconds, int j, line_dirichlet& ld) const
+	{
+		const int S = a.S;
+		if (tt.axis == 0)
+		{
+			ld.init<0>(a.dir, fvals, fconds, (int)(rr % a.Y), (int)(rr / a.Y), s, S, a.X, a.Y, a.Z, a.n);
+			ld.load_mask<0>(a.dir, rr, j, a.P);
+		}
+		else if (tt.axis == 1)
+		{
+			const int x = (int)(qq / S);
+			ld.init<1>(a.dir, fvals, fconds, x, (int)outer, s, S, a.X, a.Y, a.Z, a.n);
+			ld.load_mask<1>(a.dir, x + (long long)a.X * outer, j, a.P);
+		}
+		else
+		{
+			const int x = (int)((qq % tt.XS) / S), y = (int)(qq / tt.XS);
+			ld.init<2>(a.dir, fvals, fconds, x, y, s, S, a.X, a.Y, a.Z, a.n);
+			ld.load_mask<2>(a.dir, x + (long long)a.X * y, j, a.P);
+		}
+	}
+};
+
 template <bool UNI, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
@@ -127,11 +192,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
 {
 	constexpr int M = 32;
 	extern __shared__ __align__(128) unsigned char smem_raw[];
-	// stages on a 1024-byte boundary (TMA destinations), then tables, carries and the barriers
-	float* stage[2];
-	stage[0] = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-	stage[1] = stage[0] + tt.stage_floats;
-	float* tab = stage[1] + tt.stage_floats;
+	// NST stages on a 1024-byte boundary (TMA destinations), then tables, carries and barriers
+	const int NST = tt.stages;
+	float* const stages = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+	float* tab = stages + (size_t)NST * tt.stage_floats;
 	const int S = a.S;
 	const float* ctab = tab + a.n * S;
 	const float* gtab = ctab + S;
@@ -148,8 +212,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
 	const bool leader = lane == 0 && j == 0;
 	if (leader)
 	{
-		mbar_init(&bars[0], 1);
-		mbar_init(&bars[1], 1);
+		for (int k = 0; k < NST; k++)
+			mbar_init(&bars[k], 1);
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	stage_faces(a, fvals, fconds);
@@ -158,22 +222,43 @@ __global__ void __launch_bounds__(MAXT, MINB)
 	int p, L;
 	block_range(j, a.base_len, a.extra, p, L);
 
-	long long w = blockIdx.x;
-	if (leader && w < tt.items)
-		issue_tile(a, &map, tt, w, stage[0], &bars[0]);
+	// prologue: the first NST-1 tiles of this CTA
+	if (leader)
+		for (int k = 0; k < NST - 1; k++)
+		{
+			const long long wk = blockIdx.x + (long long)k * gridDim.x;
+			if (wk < tt.items)
+				issue_tile(a, &map, tt, wk, stages + (size_t)k * tt.stage_floats, &bars[k]);
+		}
 
 	bool failed = false;
 	int it = 0;
+	long long w = blockIdx.x;
 	for (; w < tt.items; w += gridDim.x, it++)
 	{
-		const int st = it & 1;
-		const uint32_t parity = (uint32_t)((it >> 1) & 1);
-		if (leader && w + gridDim.x < tt.items)
+		const int st = it % NST;
+		const uint32_t parity = (uint32_t)((it / NST) & 1);
+		if (leader)
 		{
-			// the other stage was released by the __syncthreads that ended the previous tile
-			asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-			issue_tile(a, &map, tt, w + gridDim.x, stage[st ^ 1], &bars[st ^ 1]);
+			// keep NST-1 tiles in flight; that stage was released by the previous tile's final barrier
+			const long long wn = w + (long long)(NST - 1) * gridDim.x;
+			if (wn < tt.items)
+			{
+				const int sn = (it + NST - 1) % NST;
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				issue_tile(a, &map, tt, wn, stages + (size_t)sn * tt.stage_floats, &bars[sn]);
+			}
 		}
+
+		// this thread's line in the tile (its Dirichlet descriptor load overlaps the wait)
+		float* cur = stages + (size_t)st * tt.stage_floats;
+		tile_line tl;
+		tl.locate(a, tt, w, lane);
+		line_dirichlet ld;
+		ld.any = false;
+		if (a.pre_dirichlet && tl.active)
+			tl.dirichlet(a, tt, fvals, fconds, j, ld);
+
 		const bool ok = mbar_wait(&bars[st], parity);
 		if (!__syncthreads_and(ok))
 		{
@@ -181,81 +266,59 @@ __global__ void __launch_bounds__(MAXT, MINB)
 			break;
 		}
 
-		// this thread's line in the tile
-		const float* cur = stage[st];
-		bool active;
-		int s, sbase, sstride;
-		float* line;
-		long long gstride;
-		line_dirichlet ld;
-		ld.any = false;
-		if (tt.axis == 0)
-		{
-			const int rl = lane / S;
-			s = lane - rl * S;
-			const long long row = w * tt.R + rl;
-			active = rl < tt.R && row < tt.nrows;
-			const long long rr = active ? row : 0;
-			sbase = (rl < tt.R ? rl : 0) * tt.row_pitch + s; // lanes past the last row read row 0
-			sstride = S;
-			line = a.data + rr * tt.XS + s;
-			gstride = S;
-			if (a.pre_dirichlet && active)
-			{
-				ld.init<0>(a.dir, fvals, fconds, (int)(rr % a.Y), (int)(rr / a.Y), s, S, a.X, a.Y, a.Z, a.n);
-				ld.load_mask<0>(a.dir, rr, j, a.P);
-			}
-		}
-		else
-		{
-			const long long outer = w / tt.col_tiles;
-			const long long q = (w % tt.col_tiles) * 32 + lane;
-			active = q < tt.ncols;
-			const long long qq = active ? q : 0;
-			s = (int)(qq % S);
-			sbase = lane;
-			sstride = 32;
-			line = a.data + outer * tt.outer_stride + qq;
-			gstride = tt.line_stride;
-			if (a.pre_dirichlet && active)
-			{
-				if (tt.axis == 1)
-				{
-					const int x = (int)(qq / S);
-					ld.init<1>(a.dir, fvals, fconds, x, (int)outer, s, S, a.X, a.Y, a.Z, a.n);
-					ld.load_mask<1>(a.dir, x + (long long)a.X * outer, j, a.P);
-				}
-				else
-				{
-					const int x = (int)((qq % tt.XS) / S), y = (int)(qq / tt.XS);
-					ld.init<2>(a.dir, fvals, fconds, x, y, s, S, a.X, a.Y, a.Z, a.n);
-					ld.load_mask<2>(a.dir, x + (long long)a.X * y, j, a.P);
-				}
-			}
-		}
-
 		float d[M];
-#pragma unroll
-		for (int k = 0; k < M; k++)
-			d[k] = (UNI || k < L) ? cur[sbase + (p + k) * sstride] : 0.f;
-		if (ld.any)
-			dirichlet_block<M, UNI>(ld, a.dir, d, p, L, s, S);
-
-		thomas_block<M, UNI>(d, L, p, j, a.P, tab + s, gtab + s, Gtab + s, S, ctab[s], active, carry_f + lane,
-							 carry_t + lane, 32);
-
-		if (a.post_dirichlet && ld.any)
-			dirichlet_block<M, UNI>(ld, a.dir, d, p, L, s, S);
-		if (active)
 		{
-			float* ptr = line + (long long)p * gstride;
+			// interior Dirichlet voxels of this block are written into the tile before it is read
+			for (unsigned long long m = ld.mask; m; m &= m - 1)
+			{
+				const int k = __ffsll((long long)m) - 1;
+				float* e = cur + tl.sbase + (p + k) * tl.sstride;
+				*e = ld.marked(k, tl.s, S, *e);
+			}
 #pragma unroll
 			for (int k = 0; k < M; k++)
-				if (UNI || k < L)
+				d[k] = (UNI || k < L) ? cur[tl.sbase + (p + k) * tl.sstride] : 0.f;
+			if (ld.any)
+				dirichlet_faces<M, UNI>(ld, d, p, L);
+		}
+		const int s_now = tl.s;
+		const bool active_now = tl.active;
+
+		thomas_block<M, UNI>(d, L, p, j, a.P, tab + s_now, gtab + s_now, Gtab + s_now, S, ctab[s_now], active_now,
+							 carry_f + lane, carry_t + lane, 32);
+
+		{
+			// recompute the line from an opaque copy of the tile index, so nothing of the load
+			// phase stays live across the solve
+			long long w2;
+			asm volatile("mov.b64 %0, %1;" : "=l"(w2) : "l"(w));
+			tile_line tl2;
+			tl2.locate(a, tt, w2, lane);
+			line_dirichlet ld2;
+			ld2.any = false;
+			if (a.post_dirichlet && tl2.active)
+				tl2.dirichlet(a, tt, fvals, fconds, j, ld2);
+			if (ld2.any)
+				dirichlet_faces<M, UNI>(ld2, d, p, L);
+			if (tl2.active)
+			{
+				float* ptr = tl2.line + (long long)p * tl2.gstride;
+#pragma unroll
+				for (int k = 0; k < M; k++)
+					if (UNI || k < L)
+					{
+						*ptr = d[k];
+						ptr += tl2.gstride;
+					}
+				// the closing overwrite of interior voxels, stored over the solved values
+				for (unsigned long long m = ld2.mask; m; m &= m - 1)
 				{
-					*ptr = d[k];
-					ptr += gstride;
+					const int k = __ffsll((long long)m) - 1;
+					const long long row = ld2.row0 + __popcll(ld2.mask & ((1ull << k) - 1ull));
+					if (ld2.aconds[row * S + tl2.s])
+						tl2.line[(long long)(p + k) * tl2.gstride] = ld2.avals[row * S + tl2.s];
 				}
+			}
 		}
 		__syncthreads(); // stage st fully read before it is refilled
 	}
@@ -264,9 +327,12 @@ __global__ void __launch_bounds__(MAXT, MINB)
 	{
 		atomicOr(a.err, DEVERR_TIMEOUT);
 		// let the copies already issued land before the CTA exits (bounded waits)
-		mbar_wait(&bars[it & 1], (uint32_t)((it >> 1) & 1));
-		if (w + gridDim.x < tt.items)
-			mbar_wait(&bars[(it & 1) ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+		for (int k = 0; k < NST - 1; k++)
+		{
+			const long long wk = w + (long long)k * gridDim.x;
+			if (wk < tt.items)
+				mbar_wait(&bars[(it + k) % NST], (uint32_t)(((it + k) / NST) & 1));
+		}
 	}
 }
 
@@ -379,18 +445,24 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		if (r != CUDA_SUCCESS)
 			return BFVM_OK; // fall back to the direct kernels
 	}
-	const size_t smem =
-		1024 + (2 * (size_t)tt.stage_floats + table_floats(a.n, a.P, (int)S, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float)
-		+ 8 + 2 * sizeof(uint64_t);
 	int dev = 0, optin = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-	if (smem > (size_t)optin)
+	// one CTA per SM (128 registers) with as many stages as fit, up to 4; or, on request, two
+	// 320-thread CTAs per SM (96 registers) with two stages each
+	const bool two_per_sm = a.P <= 10 && st->sweep_ctas_per_sm == 2;
+	const size_t fixed = 1024 + (table_floats(a.n, a.P, (int)S, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float) + 8
+						 + 4 * sizeof(uint64_t);
+	const size_t stage_bytes = (size_t)tt.stage_floats * sizeof(float);
+	const size_t budget = two_per_sm ? std::min<size_t>((size_t)optin, 110 * 1024) : (size_t)optin;
+	if (fixed + 2 * stage_bytes > budget)
 		return BFVM_OK;
+	tt.stages = (int)std::min<size_t>(two_per_sm ? 2 : 4, (budget - fixed) / stage_bytes);
+	const size_t smem = fixed + tt.stages * stage_bytes;
 
 	handled = true;
-	const bool uni = a.extra == 0 && a.base_len == 32;
-	if (a.P <= 10)
+	const bool uni = a.extra == 0 && a.base_len == 32 && st->sweep_uniform != 0;
+	if (two_per_sm)
 		return uni ? launch_tma_variant<true, 320, 2>(st, a, map, tt, smem)
 				   : launch_tma_variant<false, 320, 2>(st, a, map, tt, smem);
 	return uni ? launch_tma_variant<true, 512, 1>(st, a, map, tt, smem)

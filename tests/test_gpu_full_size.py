@@ -37,7 +37,8 @@ def test_one_full_step_matches_oracle(big):
     assert e < 1e-5
     du = np.max(np.abs(gd.astype(np.float64) - o.densities()))
     dg = np.max(np.abs(gg.astype(np.float64) - o.gradients()))
-    assert dg <= du / 20 * 1.001 + 1e-12
+    # one-sided differences at the borders divide by h: |dg| <= 2 max|du| / h, plus rounding of g
+    assert dg <= 2 * du / 20 * 1.001 + 2 * np.spacing(np.float32(np.abs(gg).max()))
     assert rel_l2(gi, o.internalized()) < 1e-6
 
 
