@@ -74,12 +74,7 @@ static void free_graphs(bfvm_solver* s)
 
 static void free_dirichlet_interior(bfvm_solver* s)
 {
-	for (int a = 0; a < 3; a++)
-	{
-		device_free(s->dir_block_desc[a]);
-		device_free(s->dir_axis_vals[a]);
-		device_free(s->dir_axis_conds[a]);
-	}
+	device_free(s->dir_rows_vid);
 	device_free(s->dir_bits);
 	device_free(s->dir_rank);
 	device_free(s->dir_vals);
@@ -451,62 +446,16 @@ int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* vo
 	BFVM_CUDA(cudaMemcpy(s->dir_vals, svals.data(), svals.size() * sizeof(float), cudaMemcpyHostToDevice));
 	BFVM_CUDA(cudaMemcpy(s->dir_conds, sconds.data(), sconds.size(), cudaMemcpyHostToDevice));
 
-	// per-axis block descriptors and value tables for the sweeps
-	const long long X = s->grid[0], Y = s->grid[1], Z = s->grid[2];
-	for (int axis = 0; axis < s->dims; axis++)
+	std::vector<long long> vids;
+	vids.reserve(row_of.size());
+	for (auto& kv : row_of)
+		vids.push_back(kv.first);
+	if ((st = device_alloc(&s->dir_rows_vid, vids.size())))
 	{
-		const sweep_plan& pl = s->plan[axis];
-		const long long lines = axis == 0 ? Y * Z : (axis == 1 ? X * Z : X * Y);
-		struct entry
-		{
-			long long line;
-			int i, row;
-		};
-		std::vector<entry> ents;
-		ents.reserve(row_of.size());
-		int r = 0;
-		for (auto& kv : row_of) // rows of svals / sconds are in map order
-		{
-			const long long v = kv.first;
-			const long long x = v % X, y = (v / X) % Y, z = v / (X * Y);
-			const long long line = axis == 0 ? y + Y * z : (axis == 1 ? x + X * z : x + X * y);
-			const int i = (int)(axis == 0 ? x : (axis == 1 ? y : z));
-			ents.push_back({ line, i, r++ });
-		}
-		std::sort(ents.begin(), ents.end(),
-				  [](const entry& a, const entry& b) { return a.line != b.line ? a.line < b.line : a.i < b.i; });
-		std::vector<ulonglong2> desc((size_t)(lines * pl.P));
-		for (auto& d : desc)
-		{
-			d.x = 0ull;
-			d.y = 0ull;
-		}
-		std::vector<float> av(ents.size() * (size_t)S);
-		std::vector<unsigned char> ac(ents.size() * (size_t)S);
-		const int big = pl.extra * (pl.base_len + 1);
-		for (size_t e = 0; e < ents.size(); e++)
-		{
-			const int i = ents[e].i;
-			// block of element i: the first `extra` blocks have base_len + 1 elements
-			const int j = i < big ? i / (pl.base_len + 1) : pl.extra + (i - big) / pl.base_len;
-			const int pj = j * pl.base_len + std::min(j, pl.extra);
-			ulonglong2& d = desc[(size_t)(ents[e].line * pl.P + j)];
-			if (d.x == 0ull)
-				d.y = (unsigned long long)e; // entries of a block are consecutive after the sort
-			d.x |= 1ull << (i - pj);
-			std::memcpy(&av[e * S], &svals[(size_t)ents[e].row * S], S * sizeof(float));
-			std::memcpy(&ac[e * S], &sconds[(size_t)ents[e].row * S], S);
-		}
-		if ((st = device_alloc(&s->dir_block_desc[axis], desc.size())) || (st = device_alloc(&s->dir_axis_vals[axis], av.size()))
-			|| (st = device_alloc(&s->dir_axis_conds[axis], ac.size())))
-		{
-			free_dirichlet_interior(s);
-			return st;
-		}
-		BFVM_CUDA(cudaMemcpy(s->dir_block_desc[axis], desc.data(), desc.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice));
-		BFVM_CUDA(cudaMemcpy(s->dir_axis_vals[axis], av.data(), av.size() * sizeof(float), cudaMemcpyHostToDevice));
-		BFVM_CUDA(cudaMemcpy(s->dir_axis_conds[axis], ac.data(), ac.size(), cudaMemcpyHostToDevice));
+		free_dirichlet_interior(s);
+		return st;
 	}
+	BFVM_CUDA(cudaMemcpy(s->dir_rows_vid, vids.data(), vids.size() * sizeof(long long), cudaMemcpyHostToDevice));
 	s->n_interior = (int)row_of.size();
 	return BFVM_OK;
 }

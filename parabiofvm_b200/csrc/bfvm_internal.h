@@ -48,13 +48,6 @@ struct dirichlet_dev
 	const float* ivals;				  // [N][S]
 	const unsigned char* iconds;	  // [N][S]
 	int has_interior;
-	// Per sweep axis, one descriptor per (line, block): .x has bit k set when element k of block j
-	// of the line is an interior Dirichlet voxel, .y is the row of its first such element in
-	// axis_vals / axis_conds, which list the marked elements in (line, block, element) order
-	// (lines: x sweep y + Y*z, y sweep x + X*z, z sweep x + X*y; descriptor index line * P + j).
-	const ulonglong2* block_desc[3];
-	const float* axis_vals[3];			// [marked elements][S]
-	const unsigned char* axis_conds[3]; // [marked elements][S]
 };
 
 // One sweep axis: the precomputed Thomas coefficients of src/solver/host/diffusion_solver.cpp:72-142
@@ -134,9 +127,7 @@ struct bfvm_solver
 	int* dir_rank = nullptr;
 	float* dir_vals = nullptr;
 	unsigned char* dir_conds = nullptr;
-	ulonglong2* dir_block_desc[3] = { nullptr, nullptr, nullptr };
-	float* dir_axis_vals[3] = { nullptr, nullptr, nullptr };
-	unsigned char* dir_axis_conds[3] = { nullptr, nullptr, nullptr };
+	long long* dir_rows_vid = nullptr; // linear voxel index of each interior row
 
 	bfvm::agent_state ag;
 
@@ -164,12 +155,6 @@ struct bfvm_solver
 		d.ivals = dir_vals;
 		d.iconds = dir_conds;
 		d.has_interior = n_interior > 0;
-		for (int a = 0; a < 3; a++)
-		{
-			d.block_desc[a] = dir_block_desc[a];
-			d.axis_vals[a] = dir_axis_vals[a];
-			d.axis_conds[a] = dir_axis_conds[a];
-		}
 		return d;
 	}
 };
@@ -184,6 +169,7 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 
 // sweep.cu
 int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);
+// dirichlet.cu
 int launch_dirichlet(bfvm_solver* s);
 
 // gradient.cu

@@ -5,7 +5,8 @@
 // lines).  Warp j holds register block j of every line of the tile (blockDim = (32, P)).  Two
 // shared-memory stages alternate: while the CTA solves the tile in one stage, the TMA copies the
 // next tile into the other, so the HBM reads of the next tile overlap the recurrences of this one.
-// Results are written straight from registers with coalesced stores.
+// Results are written straight from registers with coalesced stores.  The Dirichlet overwrites run
+// before and after the sweeps (dirichlet.cu), so this kernel is a pure line solve.
 //
 //   y sweep: 3D tensor map over [Z][Y][XS], boxes of 32 columns x box_h rows
 //   z sweep: 2D tensor map over [Z][Y*XS], boxes of 32 columns x box_h planes
@@ -161,28 +162,6 @@ struct tile_line
 		}
 	}
 
-	__device__ __forceinline__ void dirichlet(const sweep_args& a, const tma_tile& tt, const float* fvals,
-											  const unsigned char* fconds, int j, line_dirichlet& ld) const
-	{
-		const int S = a.S;
-		if (tt.axis == 0)
-		{
-			ld.init<0>(a.dir, fvals, fconds, (int)(rr % a.Y), (int)(rr / a.Y), s, S, a.X, a.Y, a.Z, a.n);
-			ld.load_mask<0>(a.dir, rr, j, a.P);
-		}
-		else if (tt.axis == 1)
-		{
-			const int x = (int)(qq / S);
-			ld.init<1>(a.dir, fvals, fconds, x, (int)outer, s, S, a.X, a.Y, a.Z, a.n);
-			ld.load_mask<1>(a.dir, x + (long long)a.X * outer, j, a.P);
-		}
-		else
-		{
-			const int x = (int)((qq % tt.XS) / S), y = (int)(qq / tt.XS);
-			ld.init<2>(a.dir, fvals, fconds, x, y, s, S, a.X, a.Y, a.Z, a.n);
-			ld.load_mask<2>(a.dir, x + (long long)a.X * y, j, a.P);
-		}
-	}
 };
 
 template <bool UNI, int MAXT, int MINB>
@@ -200,9 +179,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 	const float* ctab = tab + a.n * S;
 	const float* gtab = ctab + S;
 	const float* Gtab = gtab + a.P * S;
-	float* fvals = const_cast<float*>(Gtab) + a.P * S;
-	unsigned char* fconds = reinterpret_cast<unsigned char*>(fvals + 6 * S);
-	float* carry_f = tab + table_floats(a.n, a.P, S, S);
+	float* carry_f = tab + table_floats(a.n, a.P, S);
 	float* carry_t = carry_f + a.P * 32;
 	uint64_t* bars =
 		reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(carry_t + a.P * 32) + 7) & ~uintptr_t(7));
@@ -216,7 +193,6 @@ __global__ void __launch_bounds__(MAXT, MINB)
 			mbar_init(&bars[k], 1);
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
-	stage_faces(a, fvals, fconds);
 	stage_table(a, tab, 0, S); // ends with __syncthreads, which also publishes the barrier init
 
 	int p, L;
@@ -250,14 +226,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
 			}
 		}
 
-		// this thread's line in the tile (its Dirichlet descriptor load overlaps the wait)
-		float* cur = stages + (size_t)st * tt.stage_floats;
+		// this thread's line in the tile
+		const float* cur = stages + (size_t)st * tt.stage_floats;
 		tile_line tl;
 		tl.locate(a, tt, w, lane);
-		line_dirichlet ld;
-		ld.any = false;
-		if (a.pre_dirichlet && tl.active)
-			tl.dirichlet(a, tt, fvals, fconds, j, ld);
 
 		const bool ok = mbar_wait(&bars[st], parity);
 		if (!__syncthreads_and(ok))
@@ -267,20 +239,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
 		}
 
 		float d[M];
-		{
-			// interior Dirichlet voxels of this block are written into the tile before it is read
-			for (unsigned long long m = ld.mask; m; m &= m - 1)
-			{
-				const int k = __ffsll((long long)m) - 1;
-				float* e = cur + tl.sbase + (p + k) * tl.sstride;
-				*e = ld.marked(k, tl.s, S, *e);
-			}
 #pragma unroll
-			for (int k = 0; k < M; k++)
-				d[k] = (UNI || k < L) ? cur[tl.sbase + (p + k) * tl.sstride] : 0.f;
-			if (ld.any)
-				dirichlet_faces<M, UNI>(ld, d, p, L);
-		}
+		for (int k = 0; k < M; k++)
+			d[k] = (UNI || k < L) ? cur[tl.sbase + (p + k) * tl.sstride] : 0.f;
 		const int s_now = tl.s;
 		const bool active_now = tl.active;
 
@@ -294,12 +255,6 @@ __global__ void __launch_bounds__(MAXT, MINB)
 			asm volatile("mov.b64 %0, %1;" : "=l"(w2) : "l"(w));
 			tile_line tl2;
 			tl2.locate(a, tt, w2, lane);
-			line_dirichlet ld2;
-			ld2.any = false;
-			if (a.post_dirichlet && tl2.active)
-				tl2.dirichlet(a, tt, fvals, fconds, j, ld2);
-			if (ld2.any)
-				dirichlet_faces<M, UNI>(ld2, d, p, L);
 			if (tl2.active)
 			{
 				float* ptr = tl2.line + (long long)p * tl2.gstride;
@@ -310,14 +265,6 @@ __global__ void __launch_bounds__(MAXT, MINB)
 						*ptr = d[k];
 						ptr += tl2.gstride;
 					}
-				// the closing overwrite of interior voxels, stored over the solved values
-				for (unsigned long long m = ld2.mask; m; m &= m - 1)
-				{
-					const int k = __ffsll((long long)m) - 1;
-					const long long row = ld2.row0 + __popcll(ld2.mask & ((1ull << k) - 1ull));
-					if (ld2.aconds[row * S + tl2.s])
-						tl2.line[(long long)(p + k) * tl2.gstride] = ld2.avals[row * S + tl2.s];
-				}
 			}
 		}
 		__syncthreads(); // stage st fully read before it is refilled
@@ -451,7 +398,7 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	// one CTA per SM (128 registers) with as many stages as fit, up to 4; or, on request, two
 	// 320-thread CTAs per SM (96 registers) with two stages each
 	const bool two_per_sm = a.P <= 10 && st->sweep_ctas_per_sm == 2;
-	const size_t fixed = 1024 + (table_floats(a.n, a.P, (int)S, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float) + 8
+	const size_t fixed = 1024 + (table_floats(a.n, a.P, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float) + 8
 						 + 4 * sizeof(uint64_t);
 	const size_t stage_bytes = (size_t)tt.stage_floats * sizeof(float);
 	const size_t budget = two_per_sm ? std::min<size_t>((size_t)optin, 110 * 1024) : (size_t)optin;
