@@ -441,7 +441,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plain-320")
     ap.add_argument("--kernel-reps", type=int, default=5)
     ap.add_argument("--option", action="append", default=[],
-                    help="solver tuning option name=value (bfvm_set_option), e.g. sweep_ctas_per_sm=1")
+                    help="solver tuning option name=value (bfvm_set_option), e.g. tma_sweeps=0")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)

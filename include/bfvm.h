@@ -133,9 +133,8 @@ int bfvm_synchronize(bfvm_solver* s);
 
 /*
  * Tuning options (no counterpart in the reference): "tma_sweeps" 0/1 stages sweep tiles through
- * shared memory with the TMA (default 1); "sweep_ctas_per_sm" 0 (auto), 1 or 2 picks the TMA
- * sweep occupancy for lines of up to 320 voxels; "sweep_uniform_blocks" 0/1 allows the kernel
- * variant specialised for lines made of equal 32-voxel blocks.  Results do not depend on them.
+ * shared memory with the TMA (default 1; 0 selects the kernels that read the field directly).
+ * Results agree to rounding either way.
  */
 int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value);
 

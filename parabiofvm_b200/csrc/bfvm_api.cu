@@ -50,6 +50,14 @@ static int upload_plan(bfvm_solver* s, int axis)
 	BFVM_CUDA(cudaMemcpy(p.Gp, Gp.data(), Gp.size() * sizeof(float), cudaMemcpyHostToDevice));
 	BFVM_CUDA(cudaMemcpy(p.bp, bp.data(), nS * sizeof(float), cudaMemcpyHostToDevice));
 	BFVM_CUDA(cudaMemcpy(p.c, c.data(), (size_t)s->S * sizeof(float), cudaMemcpyHostToDevice));
+	if (n >= 2)
+	{
+		std::vector<float> vt;
+		precompute_padded(n, s->S, bp, c, p.vP, p.pad, vt);
+		if ((st = device_alloc(&p.vtab, vt.size())))
+			return st;
+		BFVM_CUDA(cudaMemcpy(p.vtab, vt.data(), vt.size() * sizeof(float), cudaMemcpyHostToDevice));
+	}
 	return BFVM_OK;
 }
 
@@ -59,6 +67,7 @@ static void free_plan(sweep_plan& p)
 	device_free(p.c);
 	device_free(p.gq);
 	device_free(p.Gp);
+	device_free(p.vtab);
 }
 
 static void free_graphs(bfvm_solver* s)
@@ -72,16 +81,6 @@ static void free_graphs(bfvm_solver* s)
 	s->graphs_dirty = true;
 }
 
-static void free_dirichlet_interior(bfvm_solver* s)
-{
-	device_free(s->dir_rows_vid);
-	device_free(s->dir_bits);
-	device_free(s->dir_rank);
-	device_free(s->dir_vals);
-	device_free(s->dir_conds);
-	s->n_interior = 0;
-}
-
 static void destroy_all(bfvm_solver* s)
 {
 	if (s->device >= 0)
@@ -90,9 +89,7 @@ static void destroy_all(bfvm_solver* s)
 	for (auto& p : s->plan)
 		free_plan(p);
 	cell_free(s);
-	free_dirichlet_interior(s);
-	device_free(s->face_vals);
-	device_free(s->face_conds);
+	free_dirichlet(s);
 	device_free(s->dens);
 	device_free(s->grad);
 	device_free(s->dev_error);
@@ -100,16 +97,6 @@ static void destroy_all(bfvm_solver* s)
 		cudaFreeHost(s->host_error);
 	if (s->own_stream)
 		cudaStreamDestroy(s->own_stream);
-}
-
-static int upload_faces(bfvm_solver* s)
-{
-	const size_t n = 6 * (size_t)s->S;
-	BFVM_CUDA(cudaMemcpyAsync(s->face_vals, s->face_vals_h.data(), n * sizeof(float), cudaMemcpyHostToDevice,
-							  s->stream));
-	BFVM_CUDA(cudaMemcpyAsync(s->face_conds, s->face_conds_h.data(), n, cudaMemcpyHostToDevice, s->stream));
-	BFVM_CUDA(cudaStreamSynchronize(s->stream));
-	return BFVM_OK;
 }
 
 // error flags raised by kernels since the last check
@@ -265,7 +252,6 @@ int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_
 		}
 		s->stream = s->own_stream;
 		if ((st = device_alloc(&s->dens, (size_t)s->V * s->S)) || (st = device_alloc(&s->grad, (size_t)s->V * s->S * dims))
-			|| (st = device_alloc(&s->face_vals, 6 * (size_t)s->S)) || (st = device_alloc(&s->face_conds, 6 * (size_t)s->S))
 			|| (st = device_alloc(&s->dev_error, 1)))
 			break;
 		if (cudaMallocHost((void**)&s->host_error, sizeof(int)) != cudaSuccess)
@@ -284,9 +270,6 @@ int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_
 		}
 		for (int d = 0; d < dims && !st; d++)
 			st = upload_plan(s, d);
-		if (st)
-			break;
-		st = upload_faces(s);
 	} while (0);
 
 	if (st)
@@ -363,8 +346,10 @@ int bfvm_set_boundary_dirichlet(bfvm_solver* s, int dim, int is_max, const float
 			s->face_conds_h[(size_t)face * s->S + k] = conditions[k] ? 1 : 0;
 		}
 	}
+	// the step graphs and kernels in flight use the current overwrite list
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
 	free_graphs(s);
-	return upload_faces(s);
+	return rebuild_dirichlet(s);
 }
 
 int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* voxels, const float* values,
@@ -375,12 +360,6 @@ int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* vo
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "count must not be negative");
 	if (count > 0 && (!voxels || !values || !conditions))
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "voxels, values and conditions are required");
-	BFVM_CUDA(cudaStreamSynchronize(s->stream));
-	free_graphs(s);
-	free_dirichlet_interior(s);
-	if (count == 0)
-		return BFVM_OK;
-
 	const int S = s->S;
 	// merge duplicates in list order: a later listed condition overwrites an earlier one
 	std::map<long long, int> row_of;
@@ -414,50 +393,22 @@ int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* vo
 				conds[(size_t)row * S + k] = 1;
 			}
 	}
-	// rows in voxel order, rank bitmap over linear voxel indices
-	const long long words = (s->V + 31) / 32;
-	std::vector<unsigned int> bits((size_t)words, 0u);
-	std::vector<int> rank((size_t)words, 0);
-	std::vector<float> svals(row_of.size() * (size_t)S);
-	std::vector<unsigned char> sconds(row_of.size() * (size_t)S);
-	int r = 0;
+	// rows in voxel order
+	s->int_vids_h.clear();
+	s->int_vals_h.assign(row_of.size() * (size_t)S, 0.f);
+	s->int_conds_h.assign(row_of.size() * (size_t)S, 0);
+	size_t r = 0;
 	for (auto& kv : row_of)
 	{
-		bits[(size_t)(kv.first >> 5)] |= 1u << (kv.first & 31);
-		std::memcpy(&svals[(size_t)r * S], &vals[(size_t)kv.second * S], S * sizeof(float));
-		std::memcpy(&sconds[(size_t)r * S], &conds[(size_t)kv.second * S], S);
+		s->int_vids_h.push_back(kv.first);
+		std::memcpy(&s->int_vals_h[r * S], &vals[(size_t)kv.second * S], S * sizeof(float));
+		std::memcpy(&s->int_conds_h[r * S], &conds[(size_t)kv.second * S], S);
 		r++;
 	}
-	int acc = 0;
-	for (long long w = 0; w < words; w++)
-	{
-		rank[(size_t)w] = acc;
-		acc += __builtin_popcount(bits[(size_t)w]);
-	}
-	int st;
-	if ((st = device_alloc(&s->dir_bits, (size_t)words)) || (st = device_alloc(&s->dir_rank, (size_t)words))
-		|| (st = device_alloc(&s->dir_vals, svals.size())) || (st = device_alloc(&s->dir_conds, sconds.size())))
-	{
-		free_dirichlet_interior(s);
-		return st;
-	}
-	BFVM_CUDA(cudaMemcpy(s->dir_bits, bits.data(), bits.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
-	BFVM_CUDA(cudaMemcpy(s->dir_rank, rank.data(), rank.size() * sizeof(int), cudaMemcpyHostToDevice));
-	BFVM_CUDA(cudaMemcpy(s->dir_vals, svals.data(), svals.size() * sizeof(float), cudaMemcpyHostToDevice));
-	BFVM_CUDA(cudaMemcpy(s->dir_conds, sconds.data(), sconds.size(), cudaMemcpyHostToDevice));
-
-	std::vector<long long> vids;
-	vids.reserve(row_of.size());
-	for (auto& kv : row_of)
-		vids.push_back(kv.first);
-	if ((st = device_alloc(&s->dir_rows_vid, vids.size())))
-	{
-		free_dirichlet_interior(s);
-		return st;
-	}
-	BFVM_CUDA(cudaMemcpy(s->dir_rows_vid, vids.data(), vids.size() * sizeof(long long), cudaMemcpyHostToDevice));
-	s->n_interior = (int)row_of.size();
-	return BFVM_OK;
+	// the step graphs and kernels in flight use the current overwrite list
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	free_graphs(s);
+	return rebuild_dirichlet(s);
 }
 
 int bfvm_store_densities(bfvm_solver* s, const float* host)
@@ -647,14 +598,6 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 	const std::string n(name);
 	if (n == "tma_sweeps")
 		s->use_tma = value != 0;
-	else if (n == "sweep_ctas_per_sm")
-	{
-		if (value < 0 || value > 2)
-			return fail(BFVM_ERR_INVALID_ARGUMENT, "sweep_ctas_per_sm must be 0, 1 or 2");
-		s->sweep_ctas_per_sm = (int)value;
-	}
-	else if (n == "sweep_uniform_blocks")
-		s->sweep_uniform = value != 0;
 	else
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "unknown option " + n);
 	free_graphs(s);

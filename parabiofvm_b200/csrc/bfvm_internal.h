@@ -38,18 +38,6 @@ enum device_error_bits : int
 // that order; interior voxels are found through a rank bitmap over linear voxel indices
 // (v = x + X*(y + Y*z)): bit v of `bits` marks a Dirichlet voxel, and its row in ivals/iconds is
 // rank[v/32] + popcount of the lower bits of its word.
-struct dirichlet_dev
-{
-	const float* face_vals;			  // [6][S]
-	const unsigned char* face_conds;  // [6][S]
-	int face_mask;					  // bit (2*axis + is_max) set when the face exists
-	const unsigned int* bits;		  // [ceil(V/32)]
-	const int* rank;				  // [ceil(V/32)]
-	const float* ivals;				  // [N][S]
-	const unsigned char* iconds;	  // [N][S]
-	int has_interior;
-};
-
 // One sweep axis: the precomputed Thomas coefficients of src/solver/host/diffusion_solver.cpp:72-142
 // (only b' is stored; e = c b' is recomputed) plus the whole-block carry products of the
 // partitioned solve.
@@ -64,6 +52,10 @@ struct sweep_plan
 	float* c = nullptr;		// [S] off-diagonal
 	float* gq = nullptr;	// [P][S] forward carry product of each whole block
 	float* Gp = nullptr;	// [P][S] backward carry product of each whole block
+	// front-padded partition of the staged sweeps (precompute_padded): vP blocks of exactly 32
+	int vP = 1;
+	int pad = 0;
+	float* vtab = nullptr; // padded_table_floats(vP, S) floats
 };
 
 // Radix-sort / scan scratch for the agent binning.
@@ -116,18 +108,17 @@ struct bfvm_solver
 
 	bfvm::sweep_plan plan[3];
 
-	// Dirichlet, host copies (for rebuilds) and device buffers
+	// Dirichlet conditions as set (host), and the resolved overwrite list on the device: every
+	// conditioned element once, with the value the reference's order leaves there
 	std::vector<float> face_vals_h;			 // [6][S]
 	std::vector<unsigned char> face_conds_h; // [6][S]
 	int face_mask = 0;
-	float* face_vals = nullptr;
-	unsigned char* face_conds = nullptr;
-	int n_interior = 0;
-	unsigned int* dir_bits = nullptr;
-	int* dir_rank = nullptr;
-	float* dir_vals = nullptr;
-	unsigned char* dir_conds = nullptr;
-	long long* dir_rows_vid = nullptr; // linear voxel index of each interior row
+	std::vector<long long> int_vids_h;		// interior voxels, ascending linear index
+	std::vector<float> int_vals_h;			// [voxel][S]
+	std::vector<unsigned char> int_conds_h; // [voxel][S]
+	long long* dir_idx = nullptr;			// element index vid * S + s
+	float* dir_val = nullptr;
+	long long dir_count = 0;
 
 	bfvm::agent_state ag;
 
@@ -136,27 +127,11 @@ struct bfvm_solver
 
 	long long launches = 0;
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
-	int sweep_ctas_per_sm = 0; // TMA sweep occupancy for lines of <= 320 voxels: 0 auto, 1 or 2
-	int sweep_uniform = 1;	   // specialise the sweeps for lines split into equal blocks of 32
 
 	// graphs for run_steps: [recompute]
 	cudaGraphExec_t step_graph[2] = { nullptr, nullptr };
 	long long graph_kernels[2] = { 0, 0 }; // kernel nodes per step graph
 	bool graphs_dirty = true;
-
-	bfvm::dirichlet_dev dirichlet() const
-	{
-		bfvm::dirichlet_dev d;
-		d.face_vals = face_vals;
-		d.face_conds = face_conds;
-		d.face_mask = face_mask;
-		d.bits = dir_bits;
-		d.rank = dir_rank;
-		d.ivals = dir_vals;
-		d.iconds = dir_conds;
-		d.has_interior = n_interior > 0;
-		return d;
-	}
 };
 
 namespace bfvm {
@@ -166,11 +141,16 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 					 std::vector<float>& bp, std::vector<float>& eprev, std::vector<float>& g, std::vector<float>& G,
 					 std::vector<float>& c, std::vector<float>& gq, std::vector<float>& Gp, int& P, int& base_len,
 					 int& extra);
+int padded_table_floats(int P, int S);
+void precompute_padded(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int& P, int& pad,
+					   std::vector<float>& tab);
 
 // sweep.cu
 int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);
 // dirichlet.cu
 int launch_dirichlet(bfvm_solver* s);
+int rebuild_dirichlet(bfvm_solver* s);
+void free_dirichlet(bfvm_solver* s);
 
 // gradient.cu
 int launch_gradient(bfvm_solver* s);

@@ -1,129 +1,133 @@
 // Dirichlet overwrite (paraBioFVM src/solver/host/dirichlet_solver.cpp:11-151).
 //
 // The reference writes the boundary faces in the order x-min, x-max, y-min, y-max, z-min, z-max
-// (a later face wins on shared edges and corners) and then the interior Dirichlet voxels.  Here
-// one thread owns one voxel that carries a condition and writes, for each substrate that has one,
-// the value the reference's order leaves there; elements without a condition are not touched.
-// Work items are the voxels of every face that exists followed by the interior Dirichlet voxels,
-// so an overwrite costs the conditioned elements only, not a pass over the field.  A voxel listed
-// by two work items (a face edge, or a face voxel also listed as interior) receives the same value
-// from both.
+// (a later face wins on shared edges and corners) and then the interior Dirichlet voxels.  The
+// conditions change only through the set-up calls, so the host resolves that order once, when
+// they are set: the result is a list of (element index, value) pairs holding every conditioned
+// element once with the value the reference leaves there.  The overwrite is then a scatter of the
+// list, touching only the conditioned elements; it runs four times per step (before each sweep
+// and after the last).
+
+#include <algorithm>
+#include <cstring>
 
 #include "bfvm_internal.h"
 
 namespace bfvm {
 
-struct dirichlet_work
+__global__ void __launch_bounds__(256) dirichlet_scatter_kernel(float* __restrict__ data,
+																const long long* __restrict__ idx,
+																const float* __restrict__ val, long long count)
 {
-	long long face_start[7]; // work item ranges of the six faces (empty when the face is absent)
-	int face_w[6];			 // extent of the faster of the two free axes of each face
-	long long n_items;		 // faces + interior voxels
-};
-
-__device__ __forceinline__ bool interior_value(const dirichlet_dev& d, long long vid, int s, int S, float& v)
-{
-	if (!d.has_interior)
-		return false;
-	const unsigned int w = __ldg(&d.bits[vid >> 5]);
-	const unsigned int b = (unsigned int)(vid & 31);
-	if (!((w >> b) & 1u))
-		return false;
-	const long long row = (long long)__ldg(&d.rank[vid >> 5]) + __popc(w & ((1u << b) - 1u));
-	if (!d.iconds[row * S + s])
-		return false;
-	v = d.ivals[row * S + s];
-	return true;
-}
-
-__global__ void __launch_bounds__(256) dirichlet_scatter_kernel(float* __restrict__ data, const dirichlet_dev dir,
-																const dirichlet_work wk, int S, int X, int Y, int Z,
-																const long long* __restrict__ rows_vid)
-{
-	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= wk.n_items)
-		return;
-	long long vid;
-	if (t < wk.face_start[6])
-	{
-		int f = 0;
-		while (t >= wk.face_start[f + 1])
-			f++;
-		const long long r = t - wk.face_start[f];
-		const int ax = f >> 1;
-		const int fixed = (f & 1) ? (ax == 0 ? X : (ax == 1 ? Y : Z)) - 1 : 0;
-		const int a0 = (int)(r % wk.face_w[f]);
-		const int a1 = (int)(r / wk.face_w[f]);
-		// the two free axes in x, y, z order
-		const int x = ax == 0 ? fixed : a0;
-		const int y = ax == 1 ? fixed : (ax == 0 ? a0 : a1);
-		const int z = ax == 2 ? fixed : a1;
-		vid = (long long)x + (long long)X * ((long long)y + (long long)Y * z);
-		for (int s = 0; s < S; s++)
-		{
-			bool hit = false;
-			float v = 0.f;
-			// faces in the reference's order; a later one overwrites
-#pragma unroll
-			for (int g = 0; g < 6; g++)
-			{
-				if (!((dir.face_mask >> g) & 1))
-					continue;
-				const int gax = g >> 1;
-				const int cg = gax == 0 ? x : (gax == 1 ? y : z);
-				const int eg = gax == 0 ? X : (gax == 1 ? Y : Z);
-				const bool on = (g & 1) ? cg == eg - 1 : cg == 0;
-				if (on && dir.face_conds[g * S + s])
-				{
-					v = dir.face_vals[g * S + s];
-					hit = true;
-				}
-			}
-			float iv;
-			if (interior_value(dir, vid, s, S, iv))
-			{
-				v = iv;
-				hit = true;
-			}
-			if (hit)
-				data[vid * S + s] = v;
-		}
-		return;
-	}
-	// interior voxel: written last by the reference, so its conditions are final
-	const long long row = t - wk.face_start[6];
-	vid = rows_vid[row];
-	for (int s = 0; s < S; s++)
-		if (dir.iconds[row * S + s])
-			data[vid * S + s] = dir.ivals[row * S + s];
+	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x)
+		data[__ldg(&idx[t])] = __ldg(&val[t]);
 }
 
 int launch_dirichlet(bfvm_solver* st)
 {
-	const dirichlet_dev d = st->dirichlet();
-	if (!d.face_mask && !d.has_interior)
-		return BFVM_OK;
-	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2];
-	dirichlet_work wk;
-	long long acc = 0;
-	for (int f = 0; f < 6; f++)
-	{
-		wk.face_start[f] = acc;
-		const int ax = f >> 1;
-		// free axes in x, y, z order: x face -> (y, z); y face -> (x, z); z face -> (x, y)
-		const long long w0 = ax == 0 ? Y : X;
-		const long long w1 = ax == 2 ? Y : Z;
-		wk.face_w[f] = (int)w0;
-		if ((d.face_mask >> f) & 1)
-			acc += w0 * w1;
-	}
-	wk.face_start[6] = acc;
-	wk.n_items = acc + (d.has_interior ? st->n_interior : 0);
-	if (wk.n_items == 0)
+	if (st->dir_count == 0)
 		return BFVM_OK;
 	const int threads = 256;
-	dirichlet_scatter_kernel<<<(unsigned)((wk.n_items + threads - 1) / threads), threads, 0, st->stream>>>(
-		st->dens, d, wk, st->S, (int)X, (int)Y, (int)Z, st->dir_rows_vid);
+	const long long blocks = std::min<long long>((st->dir_count + threads - 1) / threads, 148LL * 16);
+	dirichlet_scatter_kernel<<<(unsigned)blocks, threads, 0, st->stream>>>(st->dens, st->dir_idx, st->dir_val,
+																			st->dir_count);
 	return check_launch(st, "dirichlet_scatter_kernel");
+}
+
+void free_dirichlet(bfvm_solver* s)
+{
+	device_free(s->dir_idx);
+	device_free(s->dir_val);
+	s->dir_count = 0;
+}
+
+// Resolve the faces and interior voxels into the overwrite list and upload it.
+int rebuild_dirichlet(bfvm_solver* s)
+{
+	const int S = s->S;
+	const long long X = s->grid[0], Y = s->grid[1], Z = s->grid[2];
+	const long long ext[3] = { X, Y, Z };
+
+	// voxels on any face that has conditions, each once, ascending
+	std::vector<long long> face_vox;
+	for (int f = 0; f < 6; f++)
+	{
+		if (!((s->face_mask >> f) & 1))
+			continue;
+		const int ax = f >> 1;
+		const int a1 = ax == 0 ? 1 : 0, a2 = ax == 2 ? 1 : 2; // the free axes, faster first
+		long long c[3];
+		c[ax] = (f & 1) ? ext[ax] - 1 : 0;
+		for (c[a2] = 0; c[a2] < ext[a2]; c[a2]++)
+			for (c[a1] = 0; c[a1] < ext[a1]; c[a1]++)
+				face_vox.push_back(c[0] + X * (c[1] + Y * c[2]));
+	}
+	std::sort(face_vox.begin(), face_vox.end());
+	face_vox.erase(std::unique(face_vox.begin(), face_vox.end()), face_vox.end());
+
+	std::vector<long long> idx;
+	std::vector<float> val;
+	idx.reserve(face_vox.size() * S + s->int_vids_h.size() * S);
+	val.reserve(idx.capacity());
+	const auto& iv = s->int_vids_h;
+	for (long long vid : face_vox)
+	{
+		const long long c[3] = { vid % X, (vid / X) % Y, vid / (X * Y) };
+		const auto it = std::lower_bound(iv.begin(), iv.end(), vid);
+		const long long row = (it != iv.end() && *it == vid) ? (long long)(it - iv.begin()) : -1;
+		for (int k = 0; k < S; k++)
+		{
+			bool hit = false;
+			float v = 0.f;
+			for (int f = 0; f < 6; f++) // the reference's face order; a later face overwrites
+			{
+				if (!((s->face_mask >> f) & 1))
+					continue;
+				const int ax = f >> 1;
+				const bool on = (f & 1) ? c[ax] == ext[ax] - 1 : c[ax] == 0;
+				if (on && s->face_conds_h[(size_t)f * S + k])
+				{
+					v = s->face_vals_h[(size_t)f * S + k];
+					hit = true;
+				}
+			}
+			if (row >= 0 && s->int_conds_h[(size_t)row * S + k]) // interior voxels come last
+			{
+				v = s->int_vals_h[(size_t)row * S + k];
+				hit = true;
+			}
+			if (hit)
+			{
+				idx.push_back(vid * S + k);
+				val.push_back(v);
+			}
+		}
+	}
+	for (size_t r = 0; r < iv.size(); r++)
+	{
+		if (std::binary_search(face_vox.begin(), face_vox.end(), iv[r]))
+			continue; // resolved with the faces
+		for (int k = 0; k < S; k++)
+			if (s->int_conds_h[r * S + k])
+			{
+				idx.push_back(iv[r] * S + k);
+				val.push_back(s->int_vals_h[r * S + k]);
+			}
+	}
+
+	free_dirichlet(s);
+	if (idx.empty())
+		return BFVM_OK;
+	int st;
+	if ((st = device_alloc(&s->dir_idx, idx.size())) || (st = device_alloc(&s->dir_val, val.size())))
+	{
+		free_dirichlet(s);
+		return st;
+	}
+	BFVM_CUDA(cudaMemcpy(s->dir_idx, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice));
+	BFVM_CUDA(cudaMemcpy(s->dir_val, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice));
+	s->dir_count = (long long)idx.size();
+	return BFVM_OK;
 }
 
 } // namespace bfvm

@@ -106,4 +106,82 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 	}
 }
 
+// Tables of the front-padded partition used by the staged sweeps (sweep_tma.cu).  The line is
+// extended at its front by pad = 32 P - n virtual elements with b' = 0, so every one of the P
+// blocks holds exactly 32 elements.  A virtual element has e = c * 0 = 0 and so couples nothing
+// into the first real element: a line that fits one block still runs the reference's recurrences
+// bit for bit, and longer lines need no per-element predicates.
+//
+// Each block first runs the forward and backward recurrences from zero carries (f, then t).  The
+// backward substitution is linear, so the effect of the left carry C = d'_{p-1} on the block is
+// the backward substitution tg of g, and the exact solution is
+//   x_i = t_i + C tg_i + X G_i,    X = x_{q+1}.
+// Layout, one float buffer that the kernels copy to shared memory as is (virtual index v < 32 P):
+//   b' [32P][S] | (tg, G) pairs [32P][S][2] | c [S] | gq [P][S] | tgp [P][S] | Gp [P][S]
+// with gq = g at each block end, tgp = tg and Gp = G at each block start.  g, tg and G are
+// evaluated in double from the float b' and e = c b' and rounded once.
+int padded_table_floats(int P, int S) { return 3 * 32 * P * S + S + 3 * P * S; }
+
+void precompute_padded(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int& P, int& pad,
+					   std::vector<float>& tab)
+{
+	P = (n + 31) / 32;
+	pad = 32 * P - n;
+	const int N = 32 * P;
+	tab.assign((size_t)padded_table_floats(P, S), 0.f);
+	float* vbp = tab.data();
+	float* tgG = vbp + (size_t)N * S;
+	float* ct = tgG + (size_t)2 * N * S;
+	float* gq = ct + S;
+	float* tgp = gq + (size_t)P * S;
+	float* Gp = tgp + (size_t)P * S;
+	for (int v = pad; v < N; v++)
+		for (int s = 0; s < S; s++)
+			vbp[(size_t)v * S + s] = bp[(size_t)(v - pad) * S + s];
+	for (int s = 0; s < S; s++)
+		ct[s] = c[s];
+	if (P == 1)
+		return; // a single block uses no carries
+	double gd[32];
+	for (int j = 0; j < P; j++)
+	{
+		const int p = 32 * j, q = p + 31;
+		for (int s = 0; s < S; s++)
+		{
+			const double cs = (double)c[s];
+			if (j < P - 1)
+			{
+				// response to the right carry: G_v = prod_{m=v}^{q} (-c b'_m)
+				double acc = 1.0;
+				for (int v = q; v >= p; v--)
+				{
+					acc *= -cs * (double)vbp[(size_t)v * S + s];
+					tgG[((size_t)v * S + s) * 2 + 1] = (float)acc;
+				}
+				Gp[(size_t)j * S + s] = (float)acc;
+			}
+			if (j > 0)
+			{
+				// forward response g_v = prod_{m=p-1}^{v-1} (-e_m), e_m = c b'_m the float product
+				double acc = 1.0;
+				for (int v = p; v <= q; v++)
+				{
+					acc *= -(double)(c[s] * vbp[(size_t)(v - 1) * S + s]);
+					gd[v - p] = acc;
+				}
+				gq[(size_t)j * S + s] = (float)acc;
+				// tg: the backward substitution of g within the block
+				double t = 0.0;
+				for (int v = q; v >= p; v--)
+				{
+					const double b = (double)vbp[(size_t)v * S + s];
+					t = (v == q) ? gd[v - p] * b : (gd[v - p] - cs * t) * b;
+					tgG[((size_t)v * S + s) * 2] = (float)t;
+				}
+				tgp[(size_t)j * S + s] = (float)t;
+			}
+		}
+	}
+}
+
 } // namespace bfvm

@@ -200,6 +200,9 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 	a.P = pl.P;
 	a.base_len = pl.base_len;
 	a.extra = pl.extra;
+	a.vtab = pl.vtab;
+	a.vP = pl.vP;
+	a.pad = pl.pad;
 	a.S = st->S;
 	a.X = st->grid[0];
 	a.Y = st->grid[1];

@@ -17,6 +17,8 @@ struct sweep_args
 	const float* gq; // [P][S] whole-block forward carry products
 	const float* Gp; // [P][S] whole-block backward carry products
 	int n, P, base_len, extra, S;
+	const float* vtab; // front-padded tables of the staged sweeps (precompute_padded)
+	int vP, pad;
 	int X, Y, Z;
 	int* err; // device error flags (DEVERR_*)
 };

@@ -2,11 +2,20 @@
 //
 // A persistent CTA owns a tile of 32 lines at a time: 32 adjacent columns of the x*s plane (y
 // sweep) or of the y*x*s plane (z sweep), or R = 32/S whole rows (x sweep, R rows x S substrate
-// lines).  Warp j holds register block j of every line of the tile (blockDim = (32, P)).  Two
-// shared-memory stages alternate: while the CTA solves the tile in one stage, the TMA copies the
-// next tile into the other, so the HBM reads of the next tile overlap the recurrences of this one.
-// Results are written straight from registers with coalesced stores.  The Dirichlet overwrites run
-// before and after the sweeps (dirichlet.cu), so this kernel is a pure line solve.
+// lines).  Up to four shared-memory stages rotate: while the CTA solves the tile in one stage,
+// the TMA copies the next tiles into the others, so the HBM reads overlap the recurrences.
+// Results are written straight from registers with coalesced stores.  The Dirichlet overwrites
+// run before and after the sweeps (dirichlet.cu), so this kernel is a pure line solve.
+//
+// Lines use the front-padded partition of precompute.cpp: P blocks of exactly 32 elements, the
+// first `pad` of them virtual (b' = 0, read as zeros from a front of the stage that the copies
+// never write).  Warp j holds block j of every line of the tile (blockDim = (32, P)) and
+//   1. runs the forward and the backward recurrence on its registers from zero carries,
+//   2. barrier; folds the forward carries of the blocks to its left into C and publishes its
+//      first element corrected by C,
+//   3. barrier; folds those first elements of the blocks to its right into X and applies
+//      x = t + C tg + X G with the precomputed responses tg and G.
+// With P == 1 steps 2 and 3 vanish and the arithmetic is the reference's Thomas solve.
 //
 //   y sweep: 3D tensor map over [Z][Y][XS], boxes of 32 columns x box_h rows
 //   z sweep: 2D tensor map over [Z][Y*XS], boxes of 32 columns x box_h planes
@@ -90,13 +99,19 @@ struct tma_tile
 	long long outer_stride, line_stride;
 	int box_h, nbox;	 // TMA boxes along the line (y, z)
 	int R, row_pitch;	 // rows per tile and padded row length in floats (x)
+	int front;			 // x: floats before each staged row (holds its virtual front, 16-byte multiple)
 	long long nrows;
 	long long XS;
 	int stage_floats;
-	int stages; // pipeline depth (NST)
+	int groups; // warp groups per CTA, each solving its own tiles
+	int stages; // pipeline depth of each group
+	// zero-filled virtual fronts of a stage: `front_count` runs of `front_floats`, `front_pitch` apart
+	int front_floats, front_count, front_pitch;
 };
 
-// Issue the copies of tile w into `dst`, completing on `bar` (one thread).
+// Issue the copies of tile w into `dst`, completing on `bar` (one thread).  The line elements land
+// after the virtual front: row rl of an x tile at rl * row_pitch + front, and the columns of a y/z
+// tile from stage row `pad` on.
 __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMap* map, const tma_tile& tt, long long w,
 										   float* dst, uint64_t* bar)
 {
@@ -107,31 +122,30 @@ __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMa
 		const uint32_t row_bytes = (uint32_t)(tt.XS * sizeof(float));
 		mbar_expect_tx(bar, row_bytes * rows);
 		for (int r = 0; r < rows; r++)
-			bulk_load(dst + r * tt.row_pitch, a.data + (row0 + r) * tt.XS, row_bytes, bar);
+			bulk_load(dst + r * tt.row_pitch + tt.front, a.data + (row0 + r) * tt.XS, row_bytes, bar);
 		return;
 	}
 	const long long outer = w / tt.col_tiles;
 	const int c0 = (int)((w % tt.col_tiles) * 32);
 	mbar_expect_tx(bar, (uint32_t)(tt.nbox * tt.box_h * 32 * sizeof(float)));
+	float* base = dst + a.pad * 32;
 	for (int b = 0; b < tt.nbox; b++)
 	{
 		if (tt.axis == 1)
-			tma_load_3d(dst + b * tt.box_h * 32, map, c0, b * tt.box_h, (int)outer, bar);
+			tma_load_3d(base + b * tt.box_h * 32, map, c0, b * tt.box_h, (int)outer, bar);
 		else
-			tma_load_2d(dst + b * tt.box_h * 32, map, c0, b * tt.box_h, bar);
+			tma_load_2d(base + b * tt.box_h * 32, map, c0, b * tt.box_h, bar);
 	}
 }
 
-// Where line `lane` of tile w lives: in the shared-memory stage (sbase + i*sstride) and in the
-// field (line + i*gstride), and its Dirichlet conditions.
+// Where line `lane` of tile w lives: virtual element v at stage[sbase + v * sstride], real element
+// i = v - pad at line[i * gstride] in the field.
 struct tile_line
 {
 	bool active;
 	int s, sbase, sstride;
 	float* line;
 	long long gstride;
-	long long rr;			// x sweep: row index y + Y*z
-	long long outer, qq;	// y/z sweeps: plane and column
 
 	__device__ __forceinline__ void locate(const sweep_args& a, const tma_tile& tt, long long w, int lane)
 	{
@@ -142,18 +156,19 @@ struct tile_line
 			s = lane - rl * S;
 			const long long row = w * tt.R + rl;
 			active = rl < tt.R && row < tt.nrows;
-			rr = active ? row : 0;
-			sbase = (rl < tt.R ? rl : 0) * tt.row_pitch + s; // lanes past the last row read row 0
+			const long long rr = active ? row : 0;
+			// lanes past the last row of the tile read row 0
+			sbase = (rl < tt.R ? rl : 0) * tt.row_pitch + tt.front - a.pad * S + s;
 			sstride = S;
 			line = a.data + rr * tt.XS + s;
 			gstride = S;
 		}
 		else
 		{
-			outer = w / tt.col_tiles;
+			const long long outer = w / tt.col_tiles;
 			const long long q = (w % tt.col_tiles) * 32 + lane;
 			active = q < tt.ncols;
-			qq = active ? q : 0;
+			const long long qq = active ? q : 0;
 			s = (int)(qq % S);
 			sbase = lane;
 			sstride = 32;
@@ -161,63 +176,134 @@ struct tile_line
 			gstride = tt.line_stride;
 		}
 	}
-
 };
 
-template <bool UNI, int MAXT, int MINB>
-__global__ void __launch_bounds__(MAXT, MINB)
+// Shared-memory tables of the padded partition: the per-element tables transposed to [S][NP],
+// NP = 32P + 1, so that a thread reaches its substrate's column with immediate offsets and the
+// substrates of a warp fall into distinct banks, and c.  The per-block tables (gq, tgp, Gp; a few
+// hundred floats read only by the carry folds) stay in global memory and are served by L1.
+__host__ __device__ __forceinline__ int staged_table_floats(int P, int S)
+{
+	const int NP = 32 * P + 1;
+	return 3 * S * NP + S;
+}
+
+// Barriers of one warp group (ids 1 + group; id 0 is the CTA-wide __syncthreads).
+__device__ __forceinline__ void group_sync(int id, int nthreads)
+{
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ bool group_sync_and(int id, int nthreads, bool pred)
+{
+	uint32_t r;
+	asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+				 "selp.u32 %0, 1, 0, q;\n}"
+				 : "=r"(r)
+				 : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+				 : "memory");
+	return r != 0;
+}
+
+// ROWS: x sweep (tiles of whole rows, runtime element stride S in the stage); otherwise y/z
+// sweep (tiles of 32 columns, element stride 32).  CTA = (32, P, G) threads: G warp groups share
+// the coefficient tables; group g solves its own tiles with its own stages and barriers, and warp
+// j of a group holds block j (virtual elements 32j .. 32j+31) of the 32 lines of its tile.
+template <bool ROWS>
+__global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt)
 {
 	constexpr int M = 32;
 	extern __shared__ __align__(128) unsigned char smem_raw[];
-	// NST stages on a 1024-byte boundary (TMA destinations), then tables, carries and barriers
+	// G * NST stages on a 128-byte boundary (TMA destinations), then tables, carries, barriers
 	const int NST = tt.stages;
-	float* const stages = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-	float* tab = stages + (size_t)NST * tt.stage_floats;
+	const int G = tt.groups;
+	float* const stages0 = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
 	const int S = a.S;
-	const float* ctab = tab + a.n * S;
-	const float* gtab = ctab + S;
-	const float* Gtab = gtab + a.P * S;
-	float* carry_f = tab + table_floats(a.n, a.P, S);
-	float* carry_t = carry_f + a.P * 32;
-	uint64_t* bars =
-		reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(carry_t + a.P * 32) + 7) & ~uintptr_t(7));
+	const int P = a.vP;
+	const int N = 32 * P;
+	const int NP = N + 1;
+	float* tab = stages0 + (size_t)G * NST * tt.stage_floats;
+	float2* tgtab = reinterpret_cast<float2*>(tab); // [S][NP] (tg, G)
+	float* btab = tab + 2 * S * NP;					// [S][NP] b'
+	float* ctab = btab + S * NP;					// [S]
+	const float* gqtab = a.vtab + (size_t)3 * N * S + S; // [P][S], global
+	const float* tgptab = gqtab + P * S;				 // [P][S], global
+	const float* Gptab = tgptab + P * S;				 // [P][S], global
+	float* carries = tab + staged_table_floats(P, S); // [G][2][P][32]
+	uint64_t* bars0 = reinterpret_cast<uint64_t*>(
+		(reinterpret_cast<uintptr_t>(carries + (size_t)G * 2 * P * 32) + 7) & ~uintptr_t(7)); // [G][NST]
 
 	const int lane = threadIdx.x;
 	const int j = threadIdx.y;
-	const bool leader = lane == 0 && j == 0;
-	if (leader)
+	const int g = threadIdx.z;
+	const int tid = lane + 32 * (j + P * g);
+	const int nthr = 32 * P * G;
+	const int gthr = 32 * P; // threads of a group
+	const int bar_id = 1 + g;
+	const bool leader = lane == 0 && j == 0; // of the group
+	float* const stages = stages0 + (size_t)g * NST * tt.stage_floats;
+	uint64_t* const bars = bars0 + g * NST;
+	float* const carry_f = carries + (size_t)g * 2 * P * 32;
+	float* const carry_t = carry_f + P * 32;
+
+	if (tid == 0)
 	{
-		for (int k = 0; k < NST; k++)
-			mbar_init(&bars[k], 1);
+		for (int k = 0; k < G * NST; k++)
+			mbar_init(&bars0[k], 1);
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
-	stage_table(a, tab, 0, S); // ends with __syncthreads, which also publishes the barrier init
+	{
+		// tables: global [v][S] -> shared [S][NP]
+		const float* gb = a.vtab;
+		const float2* gt = reinterpret_cast<const float2*>(a.vtab + (size_t)N * S);
+		for (int t = tid; t < N * S; t += nthr)
+		{
+			const int v = t / S, s = t - v * S;
+			btab[s * NP + v] = gb[t];
+			tgtab[s * NP + v] = gt[t];
+		}
+		const float* gr = a.vtab + (size_t)3 * N * S;
+		for (int t = tid; t < S; t += nthr)
+			ctab[t] = gr[t];
+		// the virtual fronts read as zeros; the copies never write them
+		for (int k = 0; k < G * NST; k++)
+			for (int r = 0; r < tt.front_count; r++)
+				for (int t = tid; t < tt.front_floats; t += nthr)
+					stages0[(size_t)k * tt.stage_floats + r * tt.front_pitch + t] = 0.f;
+	}
+	__syncthreads(); // also publishes the barrier init
 
-	int p, L;
-	block_range(j, a.base_len, a.extra, p, L);
+	// tiles of this group: w0, w0 + stride, ...
+	const long long w0 = (long long)blockIdx.x * G + g;
+	const long long wstride = (long long)gridDim.x * G;
 
-	// prologue: the first NST-1 tiles of this CTA
+	// prologue: the first NST-1 tiles of this group
 	if (leader)
+	{
+		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 		for (int k = 0; k < NST - 1; k++)
 		{
-			const long long wk = blockIdx.x + (long long)k * gridDim.x;
+			const long long wk = w0 + (long long)k * wstride;
 			if (wk < tt.items)
 				issue_tile(a, &map, tt, wk, stages + (size_t)k * tt.stage_floats, &bars[k]);
 		}
+	}
 
+	const int p = 32 * j;
 	bool failed = false;
 	int it = 0;
-	long long w = blockIdx.x;
-	for (; w < tt.items; w += gridDim.x, it++)
+	long long w = w0;
+	for (; w < tt.items; w += wstride, it++)
 	{
 		const int st = it % NST;
 		const uint32_t parity = (uint32_t)((it / NST) & 1);
 		if (leader)
 		{
-			// keep NST-1 tiles in flight; that stage was released by the previous tile's final barrier
-			const long long wn = w + (long long)(NST - 1) * gridDim.x;
+			// keep NST-1 tiles in flight.  The stage refilled here held the group's previous tile,
+			// whose elements every thread of the group loaded before that tile's first barrier.
+			const long long wn = w + (long long)(NST - 1) * wstride;
 			if (wn < tt.items)
 			{
 				const int sn = (it + NST - 1) % NST;
@@ -226,27 +312,73 @@ __global__ void __launch_bounds__(MAXT, MINB)
 			}
 		}
 
-		// this thread's line in the tile
 		const float* cur = stages + (size_t)st * tt.stage_floats;
-		tile_line tl;
-		tl.locate(a, tt, w, lane);
-
+		int s, sbase, sstride;
+		{
+			tile_line tl;
+			tl.locate(a, tt, w, lane);
+			s = tl.s;
+			sbase = tl.sbase;
+			sstride = ROWS ? tl.sstride : 32;
+		}
 		const bool ok = mbar_wait(&bars[st], parity);
-		if (!__syncthreads_and(ok))
+
+		const float cs = ctab[s];
+		const float* bcol = btab + s * NP + p; // b' of this block: bcol[k]
+		float d[M];
+		{
+			const float* src = cur + sbase + p * sstride;
+#pragma unroll
+			for (int k = 0; k < M; k++)
+				d[k] = src[k * sstride];
+		}
+		// forward elimination from a zero carry: f_v = d_v - e_{v-1} f_{v-1}, with e = c b' the
+		// float product the reference stores
+#pragma unroll
+		for (int k = 1; k < M; k++)
+			d[k] = __fsub_rn(d[k], __fmul_rn(__fmul_rn(cs, bcol[k - 1]), d[k - 1]));
+		carry_f[j * 32 + lane] = d[M - 1];
+		// backward substitution from a zero carry: t_q = f_q b'_q, t_v = (f_v - c t_{v+1}) b'_v
+		d[M - 1] = __fmul_rn(d[M - 1], bcol[M - 1]);
+#pragma unroll
+		for (int k = M - 2; k >= 0; k--)
+			d[k] = __fmul_rn(__fsub_rn(d[k], __fmul_rn(cs, d[k + 1])), bcol[k]);
+
+		if (!group_sync_and(bar_id, gthr, ok))
 		{
 			failed = true;
 			break;
 		}
 
-		float d[M];
+		if (P > 1)
+		{
+			// left carry C = d'_{p-1}: fold the blocks to the left, C_k = f^k_q + gq_k C_{k-1}
+			float C = 0.f;
+			if (j > 0)
+			{
+				C = carry_f[lane];
+				for (int k = 1; k < j; k++)
+					C = fmaf(__ldg(&gqtab[k * S + s]), C, carry_f[k * 32 + lane]);
+			}
+			// this block's first solution element without the right carry
+			carry_t[j * 32 + lane] = fmaf(C, __ldg(&tgptab[j * S + s]), d[0]);
+			group_sync(bar_id, gthr);
+			// right carry X = x_{q+1}: fold the blocks to the right, X_k = x^k_p + Gp_k X_{k+1}
+			float Xc = 0.f;
+			if (j < P - 1)
+			{
+				Xc = carry_t[(P - 1) * 32 + lane];
+				for (int k = P - 2; k > j; k--)
+					Xc = fmaf(__ldg(&Gptab[k * S + s]), Xc, carry_t[k * 32 + lane]);
+			}
+			const float2* tcol = tgtab + s * NP + p;
 #pragma unroll
-		for (int k = 0; k < M; k++)
-			d[k] = (UNI || k < L) ? cur[tl.sbase + (p + k) * tl.sstride] : 0.f;
-		const int s_now = tl.s;
-		const bool active_now = tl.active;
-
-		thomas_block<M, UNI>(d, L, p, j, a.P, tab + s_now, gtab + s_now, Gtab + s_now, S, ctab[s_now], active_now,
-							 carry_f + lane, carry_t + lane, 32);
+			for (int k = 0; k < M; k++)
+			{
+				const float2 r = tcol[k];
+				d[k] = fmaf(Xc, r.y, fmaf(C, r.x, d[k]));
+			}
+		}
 
 		{
 			// recompute the line from an opaque copy of the tile index, so nothing of the load
@@ -257,26 +389,40 @@ __global__ void __launch_bounds__(MAXT, MINB)
 			tl2.locate(a, tt, w2, lane);
 			if (tl2.active)
 			{
-				float* ptr = tl2.line + (long long)p * tl2.gstride;
+				if (j > 0 || a.pad == 0)
+				{
+					float* ptr = tl2.line + (long long)(p - a.pad) * tl2.gstride;
 #pragma unroll
-				for (int k = 0; k < M; k++)
-					if (UNI || k < L)
+					for (int k = 0; k < M; k++)
 					{
 						*ptr = d[k];
 						ptr += tl2.gstride;
 					}
+				}
+				else
+				{
+					// block 0 of a padded line: the first `pad` elements are virtual
+					float* ptr = tl2.line;
+#pragma unroll
+					for (int k = 0; k < M; k++)
+						if (k >= a.pad)
+						{
+							*ptr = d[k];
+							ptr += tl2.gstride;
+						}
+				}
 			}
 		}
-		__syncthreads(); // stage st fully read before it is refilled
 	}
 
 	if (failed && leader)
 	{
 		atomicOr(a.err, DEVERR_TIMEOUT);
-		// let the copies already issued land before the CTA exits (bounded waits)
-		for (int k = 0; k < NST - 1; k++)
+		// let the group's copies already issued (tiles w .. w + (NST-1) * stride) land before the
+		// CTA exits (bounded waits)
+		for (int k = 0; k < NST; k++)
 		{
-			const long long wk = w + (long long)k * gridDim.x;
+			const long long wk = w + (long long)k * wstride;
 			if (wk < tt.items)
 				mbar_wait(&bars[(it + k) % NST], (uint32_t)(((it + k) / NST) & 1));
 		}
@@ -306,17 +452,17 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 static constexpr int TMA_MAX_P = 16;
 
-template <bool UNI, int MAXT, int MINB>
+template <bool ROWS>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem)
 {
-	auto kernel = sweep_tma_kernel<UNI, MAXT, MINB>;
+	auto kernel = sweep_tma_kernel<ROWS>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
-	const int threads = 32 * a.P;
-	const int grid = persistent_grid(kernel, threads, smem, tt.items, st->device);
-	kernel<<<grid, dim3(32, a.P), smem, st->stream>>>(a, map, tt);
+	const int threads = 32 * a.vP * tt.groups;
+	const int grid = persistent_grid(kernel, threads, smem, (tt.items + tt.groups - 1) / tt.groups, st->device);
+	kernel<<<grid, dim3(32, a.vP, tt.groups), smem, st->stream>>>(a, map, tt);
 	return check_launch(st, tt.axis == 0 ? "sweep_tma<x>" : (tt.axis == 1 ? "sweep_tma<y>" : "sweep_tma<z>"));
 }
 
@@ -325,10 +471,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	handled = false;
 	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2], S = st->S;
 	const long long XS = X * S;
-	const sweep_plan& pl = st->plan[axis];
 	// shapes the TMA path covers: 16-byte row strides, at most 16 blocks of 32 per line, and for
 	// the x sweep whole rows of at most 32 substrate lines per tile
-	if (pl.M != 32 || a.P > TMA_MAX_P || XS % 4 != 0 || (axis == 0 && S > 32) || a.n < 2)
+	if (!a.vtab || a.vP > TMA_MAX_P || XS % 4 != 0 || (axis == 0 && S > 32) || a.n < 2)
 		return BFVM_OK;
 	auto encode = encode_fn();
 	if (!encode)
@@ -345,11 +490,16 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.R = (int)(32 / S);
 		tt.nrows = Y * Z;
 		tt.items = (tt.nrows + tt.R - 1) / tt.R;
-		// pad rows so that lane (r, s) = r*pitch + s spreads over the banks, keeping 16-byte rows
-		int pad = (int)(((S % 32) - (XS % 32) + 64) % 32);
-		pad = (pad + 3) / 4 * 4;
-		tt.row_pitch = (int)XS + pad;
+		// each staged row: the virtual front rounded up to 16 bytes, the row, and padding so that
+		// lane (r, s) -> r * pitch + s spreads over the banks
+		tt.front = (int)((a.pad * S + 3) / 4 * 4);
+		int bank = (int)(((S - tt.front - XS) % 32 + 64) % 32);
+		bank = (bank + 3) / 4 * 4;
+		tt.row_pitch = tt.front + (int)XS + bank;
 		tt.stage_floats = (tt.R * tt.row_pitch + 31) / 32 * 32;
+		tt.front_floats = tt.front;
+		tt.front_count = tt.R;
+		tt.front_pitch = tt.row_pitch;
 	}
 	else
 	{
@@ -361,7 +511,12 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.items = (axis == 1 ? Z : 1) * tt.col_tiles;
 		tt.outer_stride = axis == 1 ? Y * XS : 0;
 		tt.line_stride = axis == 1 ? XS : Y * XS;
-		tt.stage_floats = tt.nbox * tt.box_h * 32;
+		// stage rows: the virtual front, then the boxes (the last may run past the line end and is
+		// zero-filled by the copy)
+		tt.stage_floats = (a.pad + tt.nbox * tt.box_h) * 32;
+		tt.front_floats = a.pad * 32;
+		tt.front_count = 1;
+		tt.front_pitch = 0;
 		cuuint64_t dims[3], strides[2];
 		cuuint32_t box[3], estr[3] = { 1, 1, 1 };
 		cuuint32_t rank;
@@ -395,25 +550,24 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	int dev = 0, optin = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-	// one CTA per SM (128 registers) with as many stages as fit, up to 4; or, on request, two
-	// 320-thread CTAs per SM (96 registers) with two stages each
-	const bool two_per_sm = a.P <= 10 && st->sweep_ctas_per_sm == 2;
-	const size_t fixed = 1024 + (table_floats(a.n, a.P, (int)S) + 2 * (size_t)a.P * 32) * sizeof(float) + 8
-						 + 4 * sizeof(uint64_t);
+	// warp groups per CTA: up to 640 threads (20 warps per SM), fewer when their stages (at least
+	// two each) do not fit; each group then takes as many stages as fit, up to 4
 	const size_t stage_bytes = (size_t)tt.stage_floats * sizeof(float);
-	const size_t budget = two_per_sm ? std::min<size_t>((size_t)optin, 110 * 1024) : (size_t)optin;
-	if (fixed + 2 * stage_bytes > budget)
+	auto fixed_bytes = [&](int G) {
+		return 128 + (staged_table_floats(a.vP, (int)S) + (size_t)G * 2 * a.vP * 32) * sizeof(float) + 8
+			   + (size_t)G * 4 * sizeof(uint64_t);
+	};
+	int G = std::max(1, std::min(4, 20 / a.vP));
+	while (G > 1 && fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)
+		G--;
+	if (fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)
 		return BFVM_OK;
-	tt.stages = (int)std::min<size_t>(two_per_sm ? 2 : 4, (budget - fixed) / stage_bytes);
-	const size_t smem = fixed + tt.stages * stage_bytes;
+	tt.groups = G;
+	tt.stages = (int)std::min<size_t>(4, ((size_t)optin - fixed_bytes(G)) / ((size_t)G * stage_bytes));
+	const size_t smem = fixed_bytes(G) + (size_t)G * tt.stages * stage_bytes;
 
 	handled = true;
-	const bool uni = a.extra == 0 && a.base_len == 32 && st->sweep_uniform != 0;
-	if (two_per_sm)
-		return uni ? launch_tma_variant<true, 320, 2>(st, a, map, tt, smem)
-				   : launch_tma_variant<false, 320, 2>(st, a, map, tt, smem);
-	return uni ? launch_tma_variant<true, 512, 1>(st, a, map, tt, smem)
-			   : launch_tma_variant<false, 512, 1>(st, a, map, tt, smem);
+	return axis == 0 ? launch_tma_variant<true>(st, a, map, tt, smem) : launch_tma_variant<false>(st, a, map, tt, smem);
 }
 
 } // namespace bfvm

@@ -72,7 +72,11 @@ def test_uniform_field_decays_exactly():
     d = g.load_densities().reshape(-1, S).astype(np.float64)
     g.close()
     expected = np.linspace(0.5, 2.0, S, dtype=np.float32).astype(np.float64) / (1 + 0.01 * decay / 3) ** 3
-    assert np.max(np.abs(d - expected) / expected) < 2e-6
+    # Bound: with float32 coefficients the exact solution of one uniform 320-voxel line already
+    # differs from the analytic decay by up to 5.3e-7 (the rounding of b' for the most strongly
+    # coupled substrate, D = 1e5), and a float32 solve adds about 2e-7 of its own (the sequential
+    # Thomas recurrence and the blocked solve alike); three sweeps give at most ~2.2e-6.
+    assert np.max(np.abs(d - expected) / expected) < 3e-6
 
 
 def test_linearity(big):
