@@ -146,6 +146,42 @@ int bfvm_device_gradients(bfvm_solver* s, float** ptr, int64_t* count);
  * every kernel node). */
 int bfvm_launch_count(const bfvm_solver* s, int64_t* launches);
 
+/*
+ * Secretion and uptake with recompute, for callers that cannot allocate GPU memory: code that runs
+ * under a memory budget planned ahead of time, inside a host framework that owns every device
+ * allocation, or while another library's stream capture forbids cudaMalloc.  No counterpart in the
+ * reference; it does what bfvm_secretion_solve(s, 1) does for a solver holding the same field and
+ * agents, on buffers the caller owns, and allocates nothing: no cudaMalloc, no cudaFree, no
+ * allocating library routine.
+ *
+ * Every pointer except `error_flags` and `internalized_substrates` is required (the agent arrays
+ * when agent_count > 0) and is device memory of the current device: densities [voxels][substrates]
+ * (updated in place), the four rate arrays [agent_count][substrates], internalized_substrates
+ * (updated in place, or NULL when internalized substrates are not tracked), volumes
+ * [agent_count], positions [agent_count][dims].  The mesh is given as in bfvm_create by its
+ * minimum corner and voxel shape, plus grid_shape (1 along unused axes).  Work is enqueued on
+ * `stream` (a cudaStream_t; NULL is the legacy default stream) and the call returns without
+ * waiting.  An agent outside the mesh is skipped and sets bit 1 of *error_flags (device int) when
+ * error_flags is not NULL.
+ *
+ * Its scratch memory is one static device array of BFVM_NOALLOC_SCRATCH_BYTES (about 8 MB), held
+ * by every GPU that loads the library until the process exits; the call rejects more than
+ * BFVM_NOALLOC_MAX_AGENTS agents or more than BFVM_NOALLOC_MAX_AGENT_SUBSTRATES agent x substrate
+ * pairs with BFVM_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
+ * the array, so calls that overlap on the GPU (other streams, other host threads) race: order
+ * them on one stream.
+ */
+#define BFVM_NOALLOC_MAX_AGENTS 65536
+#define BFVM_NOALLOC_MAX_AGENT_SUBSTRATES 262144
+#define BFVM_NOALLOC_SCRATCH_BYTES 8143872
+int bfvm_secretion_solve_noalloc(float* densities, int dims, const int32_t bounding_box_mins[3],
+                                 const int32_t voxel_shape[3], const int32_t grid_shape[3], int32_t substrates,
+                                 float time_step, int32_t agent_count, const float* secretion_rates,
+                                 const float* saturation_densities, const float* uptake_rates,
+                                 const float* net_export_rates, float* internalized_substrates, const float* volumes,
+                                 const float* positions, int32_t* error_flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,8 @@ SIGNATURES = {
     "bfvm_device_densities": (c_int, [c_void_p, P(P(c_float)), P(c_int64)]),
     "bfvm_device_gradients": (c_int, [c_void_p, P(P(c_float)), P(c_int64)]),
     "bfvm_launch_count": (c_int, [c_void_p, P(c_int64)]),
+    "bfvm_secretion_solve_noalloc": (c_int, [c_void_p, c_int, P(c_int32), P(c_int32), P(c_int32), c_int32, c_float,
+                                             c_int32] + [c_void_p] * 8 + [c_void_p]),
 }
 
 

@@ -1,0 +1,61 @@
+// Kernels of the agent binning and secretion pipeline (cell.cu) and of the exclusive scan
+// (scan.cu), declared for the launchers in other files.
+#pragma once
+
+#include "bfvm_internal.h"
+
+namespace bfvm {
+
+// radix sort of the agents' voxel keys: 256-thread CTAs, each ranking 16 rounds of 256 keys
+static constexpr int SORT_THREADS = 256;
+static constexpr int SORT_ROUNDS = 16;
+static constexpr int SORT_TILE = SORT_THREADS * SORT_ROUNDS;
+
+// exclusive scan: 1024-thread CTAs, 4 elements per thread
+static constexpr int SCAN_THREADS = 1024;
+static constexpr int SCAN_ITEMS = 4;
+static constexpr long long SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__global__ void agent_keys_kernel(const float* __restrict__ pos, int A, int dims, int3 bmin, int3 vox, int3 grid,
+								  unsigned int* __restrict__ keys, int* __restrict__ vals, unsigned int invalid_key,
+								  int* err);
+__global__ void __launch_bounds__(SORT_THREADS) radix_hist_kernel(const unsigned int* __restrict__ keys, int n, int shift, int* __restrict__ hist,
+								  int tiles);
+__global__ void __launch_bounds__(SORT_THREADS) radix_scatter_kernel(const unsigned int* __restrict__ keys_in, const int* __restrict__ vals_in,
+									 unsigned int* __restrict__ keys_out, int* __restrict__ vals_out, int n, int shift,
+									 const int* __restrict__ offsets, int tiles);
+__global__ void seg_flags_kernel(const unsigned int* __restrict__ keys, int n, unsigned int invalid_key,
+								 int* __restrict__ flags);
+__global__ void seg_finish_kernel(const unsigned int* __restrict__ keys, const int* __restrict__ flags,
+								  const int* __restrict__ seg_id, int n, unsigned int invalid_key,
+								  int* __restrict__ seg_start, int* __restrict__ counts);
+__global__ void intermediates_kernel(long long total, int S, const float* __restrict__ sec,
+									 const float* __restrict__ sat, const float* __restrict__ upt,
+									 const float* __restrict__ nex, const float* __restrict__ vol, float voxel_volume,
+									 float dt, float* __restrict__ num, float* __restrict__ den, float* __restrict__ fac);
+__global__ void reduce_kernel(long long total, int S, const int* __restrict__ counts,
+							  const int* __restrict__ seg_start, const int* __restrict__ order,
+							  const float* __restrict__ num, const float* __restrict__ den,
+							  const float* __restrict__ fac, float* __restrict__ red_num, float* __restrict__ red_den,
+							  float* __restrict__ red_fac);
+__global__ void secrete_kernel(long long total, int S, float* __restrict__ dens, const int* __restrict__ counts,
+							   const int* __restrict__ seg_start, const int* __restrict__ order,
+							   const unsigned int* __restrict__ keys, const float* __restrict__ num,
+							   const float* __restrict__ den, const float* __restrict__ fac,
+							   const float* __restrict__ red_num, const float* __restrict__ red_den,
+							   const float* __restrict__ red_fac, float* __restrict__ intern, int internalized,
+							   float voxel_volume);
+
+__global__ void __launch_bounds__(SCAN_THREADS) scan_tile_kernel(const int* in, int* out, long long n, int* tile_sums);
+__global__ void scan_add_kernel(int* out, long long n, const int* tile_offsets);
+
+// number of 8-bit radix passes for keys in [0, V] (V marks agents outside the mesh)
+inline int sort_passes(long long V)
+{
+	int bits = 1;
+	while (bits < 32 && ((1ull << bits) <= (unsigned long long)V))
+		bits++;
+	return (bits + 7) / 8;
+}
+
+} // namespace bfvm

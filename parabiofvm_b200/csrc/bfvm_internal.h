@@ -34,10 +34,6 @@ enum device_error_bits : int
 };
 
 // ------------------------------------------------------------------------------------------------
-// Dirichlet conditions as seen by the kernels.  Faces are indexed 2*axis + is_max and applied in
-// that order; interior voxels are found through a rank bitmap over linear voxel indices
-// (v = x + X*(y + Y*z)): bit v of `bits` marks a Dirichlet voxel, and its row in ivals/iconds is
-// rank[v/32] + popcount of the lower bits of its word.
 // One sweep axis: the precomputed Thomas coefficients of src/solver/host/diffusion_solver.cpp:72-142
 // (only b' is stored; e = c b' is recomputed) plus the whole-block carry products of the
 // partitioned solve.

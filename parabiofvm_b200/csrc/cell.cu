@@ -20,13 +20,9 @@
 
 #include <algorithm>
 
-#include "bfvm_internal.h"
+#include "agent_kernels.cuh"
 
 namespace bfvm {
-
-static constexpr int SORT_THREADS = 256;
-static constexpr int SORT_ROUNDS = 16;
-static constexpr int SORT_TILE = SORT_THREADS * SORT_ROUNDS;
 
 // ---------------------------------------------------------------------------------------------
 // voxel keys
@@ -294,15 +290,6 @@ __global__ void release_kernel(int index, int S, int dims, const float* __restri
 
 // ---------------------------------------------------------------------------------------------
 // host side
-
-static int sort_passes(long long V)
-{
-	// keys are in [0, V] (V marks agents outside the mesh)
-	int bits = 1;
-	while (bits < 32 && ((1ull << bits) <= (unsigned long long)V))
-		bits++;
-	return (bits + 7) / 8;
-}
 
 void cell_free(bfvm_solver* s)
 {

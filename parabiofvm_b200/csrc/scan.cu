@@ -2,13 +2,9 @@
 // total, the totals are scanned recursively, and a second pass adds the scanned totals back.
 // All buffers are allocated when the plan is built, so a scan can be captured in a CUDA graph.
 
-#include "bfvm_internal.h"
+#include "agent_kernels.cuh"
 
 namespace bfvm {
-
-static constexpr int SCAN_THREADS = 1024;
-static constexpr int SCAN_ITEMS = 4;
-static constexpr long long SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
 __global__ void __launch_bounds__(SCAN_THREADS) scan_tile_kernel(const int* in, int* out, long long n, int* tile_sums)
 {
