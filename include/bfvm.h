@@ -102,6 +102,13 @@ int bfvm_load_gradients(bfvm_solver* s, float* host_gradients);
 int bfvm_store_agents(bfvm_solver* s, int32_t count, const float* secretion_rates, const float* saturation_densities,
 					  const float* uptake_rates, const float* net_export_rates, const float* internalized_substrates,
 					  const float* fraction_released_at_death, const float* volumes, const float* positions);
+/*
+ * Positions alone ([count][dims]) of the stored agents, count equal to the stored count: the
+ * per-step input of a model whose agents move.  No counterpart in the reference, whose
+ * store_data_to_solver copies every agent array (src/solver/device/CUDA/cell_solver.cpp:172-178).
+ * As with bfvm_store_agents, new positions enter the voxel binning at the next recompute.
+ */
+int bfvm_store_agent_positions(bfvm_solver* s, int32_t count, const float* positions);
 int bfvm_load_internalized(bfvm_solver* s, float* host_internalized);
 
 /* One LOD diffusion-decay step with the Dirichlet overwrites between sweeps

@@ -123,6 +123,13 @@ class Solver:
                                           _fp(vol), _fp(pos)))
         self.agents_count = n
 
+    def store_agent_positions(self, positions):
+        """Positions alone of the stored agents (the per-step input of moving agents); they enter
+        the voxel binning at the next recompute."""
+        pos = _f32(positions, self.agents_count * self.dims)
+        self._positions_keep = pos
+        check(self._lib.bfvm_store_agent_positions(self._h, self.agents_count, _fp(pos)))
+
     def load_internalized(self, out=None):
         out = np.empty(self.agents_count * self.S, np.float32) if out is None else out
         check(self._lib.bfvm_load_internalized(self._h, _fp(out)))

@@ -37,6 +37,7 @@ SIGNATURES = {
     "bfvm_load_densities": (c_int, [c_void_p, P(c_float)]),
     "bfvm_load_gradients": (c_int, [c_void_p, P(c_float)]),
     "bfvm_store_agents": (c_int, [c_void_p, c_int32] + [P(c_float)] * 8),
+    "bfvm_store_agent_positions": (c_int, [c_void_p, c_int32, P(c_float)]),
     "bfvm_load_internalized": (c_int, [c_void_p, P(c_float)]),
     "bfvm_diffusion_solve": (c_int, [c_void_p]),
     "bfvm_diffusion_sweep": (c_int, [c_void_p, c_int]),

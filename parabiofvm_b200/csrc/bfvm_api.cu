@@ -484,6 +484,21 @@ int bfvm_store_agents(bfvm_solver* s, int32_t count, const float* secretion_rate
 	return BFVM_OK;
 }
 
+int bfvm_store_agent_positions(bfvm_solver* s, int32_t count, const float* positions)
+{
+	CHECK_SOLVER(s);
+	if (count != s->ag.count)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "count " + std::to_string(count) + " differs from the "
+												   + std::to_string(s->ag.count) + " stored agents");
+	if (count == 0)
+		return BFVM_OK;
+	if (!positions)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null positions");
+	BFVM_CUDA(cudaMemcpyAsync(s->ag.pos, positions, (size_t)count * s->dims * sizeof(float), cudaMemcpyHostToDevice,
+							  s->stream));
+	return BFVM_OK;
+}
+
 int bfvm_load_internalized(bfvm_solver* s, float* host)
 {
 	CHECK_SOLVER(s);

@@ -97,3 +97,44 @@ def test_agent_count_change_rebins():
     o.secretion(True)
     g.secretion(False)  # a new agent count forces the binning to be rebuilt
     np.testing.assert_array_equal(g.densities(), o.densities())
+
+
+def test_positions_alone_enter_binning_at_recompute():
+    """bfvm_store_agent_positions: the new positions take effect at the next recompute, exactly as
+    a full bfvm_store_agents of the same arrays with the moved positions would."""
+    from parabiofvm_b200.workloads import make_solver
+
+    scn = synthetic(24, 3, 800, seed=11, clustered=True, sigma=60.0)
+    a = scn.agents
+    moved = np.ascontiguousarray(a.positions[::-1], np.float32)
+
+    g = make_solver(scn)
+    g.secretion(True)
+    g.store_agent_positions(moved)
+    g.secretion(False)  # still binned by the old positions
+    g.secretion(True)
+    got = g.load_densities(), g.load_internalized()
+    g.close()
+
+    h = make_solver(scn)
+    h.secretion(True)
+    h.store_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates,
+                   h.load_internalized(), a.fraction_released, a.volumes, moved)
+    h.secretion(False)
+    h.secretion(True)
+    want = h.load_densities(), h.load_internalized()
+    h.close()
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+
+
+def test_positions_alone_reject_a_count_change():
+    from parabiofvm_b200._abi import check
+    from parabiofvm_b200.workloads import make_solver
+
+    scn = synthetic(12, 2, 50, seed=3)
+    g = make_solver(scn)
+    with pytest.raises(BfvmError) as e:
+        check(g._lib.bfvm_store_agent_positions(g._h, 49, None))
+    assert e.value.status == 1
+    g.close()
