@@ -1,4 +1,5 @@
-"""Build the CUDA library ``parabiofvm_b200/_lib/libbfvm_cuda.so`` in-tree with nvcc for sm_100a.
+"""Build the CUDA library ``parabiofvm_b200/_lib/libbfvm_cuda.so`` in-tree with nvcc for sm_100a,
+and the C++20 host API over it, ``parabiofvm_b200/_lib/libbiofvm_b200.so`` (``host/``).
 
 Each translation unit is compiled to an object in ``parabiofvm_b200/_build`` (in parallel, only when
 its sources changed) and linked into one shared library that exports the C ABI of
@@ -20,6 +21,9 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libbfvm_cuda.so")
+HOST = os.path.join(PKG, "host")
+HOST_LIB = os.path.join(LIBDIR, "libbiofvm_b200.so")
+HOST_INCLUDE = os.path.join(HOST, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off",
@@ -73,7 +77,30 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_host()
     return LIB
+
+
+def _cxx():
+    for cand in (os.environ.get("HOST_CXX"), "g++", shutil.which("g++")):
+        if cand and shutil.which(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def build_host() -> str:
+    """The C++20 host API (include/BioFVM/*.h) as one shared library linked to the CUDA library."""
+    srcs = sorted(os.path.join(HOST, "src", f) for f in os.listdir(os.path.join(HOST, "src")) if f.endswith(".cpp"))
+    deps = srcs + [os.path.join(HOST_INCLUDE, "BioFVM", f) for f in os.listdir(os.path.join(HOST_INCLUDE, "BioFVM"))]
+    deps += [LIB, os.path.join(ROOT, "include", "bfvm.h")]
+    if os.path.exists(HOST_LIB) and os.path.getmtime(HOST_LIB) >= max(os.path.getmtime(p) for p in deps):
+        return HOST_LIB
+    cmd = [_cxx(), "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", "-I" + HOST_INCLUDE,
+           "-o", HOST_LIB, *srcs, "-L" + LIBDIR, "-lbfvm_cuda", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host library build failed:\n{r.stdout}\n{r.stderr}")
+    return HOST_LIB
 
 
 if __name__ == "__main__":
