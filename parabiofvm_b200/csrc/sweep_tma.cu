@@ -2,8 +2,9 @@
 //
 // A persistent CTA owns a tile of 32 lines at a time: 32 adjacent columns of the x*s plane (y
 // sweep) or of the y*x*s plane (z sweep), or R = 32/S whole rows (x sweep, R rows x S substrate
-// lines).  Up to four shared-memory stages rotate: while the CTA solves the tile in one stage,
-// the TMA copies the next tiles into the others, so the HBM reads overlap the recurrences.
+// lines).  Each warp group keeps up to four tiles in flight, one per shared-memory stage: a stage is
+// refilled with the tile NST ahead as soon as the group holds its current tile in registers, so
+// the HBM reads overlap the whole solve.
 // Results are written straight from registers with coalesced stores.  The Dirichlet overwrites
 // run before and after the sweeps (dirichlet.cu), so this kernel is a pure line solve.
 //
@@ -188,6 +189,16 @@ __host__ __device__ __forceinline__ int staged_table_floats(int P, int S)
 	return 3 * S * NP + S;
 }
 
+// Copy tile wn (if it exists) into a stage whose previous contents every thread has read.
+__device__ __forceinline__ void refill(const sweep_args& a, const CUtensorMap& map, const tma_tile& tt, long long wn,
+									   float* stage, uint64_t* bar)
+{
+	if (wn >= tt.items)
+		return;
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+	issue_tile(a, &map, tt, wn, stage, bar);
+}
+
 // Barriers of one warp group (ids 1 + group; id 0 is the CTA-wide __syncthreads).
 __device__ __forceinline__ void group_sync(int id, int nthreads)
 {
@@ -279,11 +290,11 @@ __global__ void __launch_bounds__(640, 1)
 	const long long w0 = (long long)blockIdx.x * G + g;
 	const long long wstride = (long long)gridDim.x * G;
 
-	// prologue: the first NST-1 tiles of this group
+	// prologue: the first NST tiles of this group, one per stage
 	if (leader)
 	{
 		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-		for (int k = 0; k < NST - 1; k++)
+		for (int k = 0; k < NST; k++)
 		{
 			const long long wk = w0 + (long long)k * wstride;
 			if (wk < tt.items)
@@ -299,18 +310,6 @@ __global__ void __launch_bounds__(640, 1)
 	{
 		const int st = it % NST;
 		const uint32_t parity = (uint32_t)((it / NST) & 1);
-		if (leader)
-		{
-			// keep NST-1 tiles in flight.  The stage refilled here held the group's previous tile,
-			// whose elements every thread of the group loaded before that tile's first barrier.
-			const long long wn = w + (long long)(NST - 1) * wstride;
-			if (wn < tt.items)
-			{
-				const int sn = (it + NST - 1) % NST;
-				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-				issue_tile(a, &map, tt, wn, stages + (size_t)sn * tt.stage_floats, &bars[sn]);
-			}
-		}
 
 		const float* cur = stages + (size_t)st * tt.stage_floats;
 		int s, sbase, sstride;
@@ -349,6 +348,11 @@ __global__ void __launch_bounds__(640, 1)
 			failed = true;
 			break;
 		}
+		// every thread of the group holds its elements of this tile in registers now (they were
+		// consumed by the recurrences before the barrier): refill the stage with the tile NST
+		// ahead, so NST tiles stay in flight through the rest of this tile's solve
+		if (leader)
+			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st]);
 
 		if (P > 1)
 		{
