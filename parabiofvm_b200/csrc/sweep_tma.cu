@@ -220,7 +220,18 @@ __device__ __forceinline__ bool group_sync_and(int id, int nthreads, bool pred)
 // sweep (tiles of 32 columns, element stride 32).  CTA = (32, P, G) threads: G warp groups share
 // the coefficient tables; group g solves its own tiles with its own stages and barriers, and warp
 // j of a group holds block j (virtual elements 32j .. 32j+31) of the 32 lines of its tile.
-template <bool ROWS>
+// Global store of one solved element.  NOALLOC: without allocating the line in L1 (faster for the
+// x and y sweeps; the z sweep, whose rows lie a whole plane apart, is faster with plain stores).
+template <bool NOALLOC>
+__device__ __forceinline__ void store_element(float* p, float v)
+{
+	if (NOALLOC)
+		asm volatile("st.global.L1::no_allocate.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+	else
+		*p = v;
+}
+
+template <bool ROWS, bool NOALLOC>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt)
@@ -399,7 +410,7 @@ __global__ void __launch_bounds__(640, 1)
 #pragma unroll
 					for (int k = 0; k < M; k++)
 					{
-						*ptr = d[k];
+						store_element<NOALLOC>(ptr, d[k]);
 						ptr += tl2.gstride;
 					}
 				}
@@ -411,7 +422,7 @@ __global__ void __launch_bounds__(640, 1)
 					for (int k = 0; k < M; k++)
 						if (k >= a.pad)
 						{
-							*ptr = d[k];
+							store_element<NOALLOC>(ptr, d[k]);
 							ptr += tl2.gstride;
 						}
 				}
@@ -456,11 +467,11 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 static constexpr int TMA_MAX_P = 16;
 
-template <bool ROWS>
+template <bool ROWS, bool NOALLOC>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem)
 {
-	auto kernel = sweep_tma_kernel<ROWS>;
+	auto kernel = sweep_tma_kernel<ROWS, NOALLOC>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
@@ -571,7 +582,10 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	const size_t smem = fixed_bytes(G) + (size_t)G * tt.stages * stage_bytes;
 
 	handled = true;
-	return axis == 0 ? launch_tma_variant<true>(st, a, map, tt, smem) : launch_tma_variant<false>(st, a, map, tt, smem);
+	if (axis == 0)
+		return launch_tma_variant<true, true>(st, a, map, tt, smem);
+	return axis == 1 ? launch_tma_variant<false, true>(st, a, map, tt, smem)
+					 : launch_tma_variant<false, false>(st, a, map, tt, smem);
 }
 
 } // namespace bfvm
