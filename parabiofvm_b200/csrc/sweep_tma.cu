@@ -565,14 +565,15 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	int dev = 0, optin = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-	// warp groups per CTA: up to 640 threads (20 warps per SM), fewer when their stages (at least
-	// two each) do not fit; each group then takes as many stages as fit, up to 4
+	// warp groups per CTA: up to 640 threads (20 warps per SM) in at most 8 groups (named barriers
+	// 1..8), fewer when their stages (at least two each) do not fit; each group then takes as many
+	// stages as fit, up to 4
 	const size_t stage_bytes = (size_t)tt.stage_floats * sizeof(float);
 	auto fixed_bytes = [&](int G) {
 		return 128 + (staged_table_floats(a.vP, (int)S) + (size_t)G * 2 * a.vP * 32) * sizeof(float) + 8
 			   + (size_t)G * 4 * sizeof(uint64_t);
 	};
-	int G = std::max(1, std::min(4, 20 / a.vP));
+	int G = std::max(1, std::min(8, 20 / a.vP));
 	while (G > 1 && fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)
 		G--;
 	if (fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)
