@@ -261,6 +261,23 @@ def run_reference(args):
     return 0
 
 
+def reduce_max_over_ranks(x, world, device):
+    """The largest of every rank's ``x`` (the job's time is its slowest replica's)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, steps, ms):
+    """Units every rank processed over the slowest rank's time: replicas do equal work."""
+    return world * units_per_rank * steps / (ms / 1e3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -294,11 +311,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(x, world, "cuda")
 
     def run_steps(n, first):
         if not args.eager:
@@ -329,7 +342,7 @@ def run_ours(args):
     clocks = sampler.stop()
     launches = s.launch_count - launches0
     ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * VS * args.steps / (ms / 1e3)
+    value = whole_job_rate(world, VS, args.steps, ms)
 
     # ---- per-kernel timing on the same stream (the roofline numerator)
     kernels = {}
@@ -429,7 +442,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-        e2e = {"value": world * VS * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+        e2e = {"value": whole_job_rate(world, VS, args.steps, e2e_ms), "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
                "ms_total": e2e_ms,
                "what": "through the C ABI from pinned host memory: field and agents stored before the steps, "
