@@ -149,6 +149,18 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value);
 int bfvm_device_densities(bfvm_solver* s, float** ptr, int64_t* count);
 int bfvm_device_gradients(bfvm_solver* s, float** ptr, int64_t* count);
 
+/*
+ * Bulk supply and uptake (bulk_solver::initialize / solve, src/solver/host/bulk_solver.cpp:8-98):
+ * D = (D + dt*S*T) / (1 + dt*(U+S)) for every voxel and substrate.  The reference calls three
+ * callbacks per voxel; here their values are tabulated: per_voxel != 0 takes [voxels][substrates]
+ * arrays, per_voxel == 0 one [substrates] row for every voxel.  supply_rates == NULL removes the
+ * tables.  bfvm_bulk_solve applies one step (BFVM_ERR_STATE before any rates are set); it is not
+ * part of bfvm_run_steps, as the reference's driver does not call it either.
+ */
+int bfvm_set_bulk_rates(bfvm_solver* s, int per_voxel, const float* supply_rates, const float* uptake_rates,
+                        const float* supply_target_densities);
+int bfvm_bulk_solve(bfvm_solver* s);
+
 /* Number of this library's kernel launches issued so far on this solver (graph replays count
  * every kernel node). */
 int bfvm_launch_count(const bfvm_solver* s, int64_t* launches);

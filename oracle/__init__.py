@@ -60,6 +60,7 @@ def _load():
             "release": (None, [vp, ctypes.c_int]),
             "run_steps": (None, [vp, ctypes.c_int, ctypes.c_int]),
             "is_conflict": (ctypes.c_int, [vp]),
+            "bulk": (None, [vp, tp, tp, tp, ctypes.c_int]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, f"oracle_{suf}_{name}")
@@ -197,6 +198,14 @@ class Oracle:
 
     def run_steps(self, steps, first_step=0):
         self._fn("run_steps")(self._h, int(steps), int(first_step))
+
+    def bulk(self, supply_rates, uptake_rates, supply_target_densities, per_voxel):
+        """Bulk supply/uptake with tabulated rates: [voxel][s] when per_voxel, else [s]."""
+        n = self.voxel_count * self.S if per_voxel else self.S
+        arrs = [np.ascontiguousarray(a, dtype=self.dtype).reshape(-1) for a in
+                (supply_rates, uptake_rates, supply_target_densities)]
+        assert all(a.size == n for a in arrs)
+        self._fn("bulk")(self._h, *[_ptr(a, self._ct) for a in arrs], int(bool(per_voxel)))
 
     @property
     def is_conflict(self):

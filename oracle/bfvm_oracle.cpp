@@ -650,6 +650,28 @@ void set_agents(oracle_state<real_t>& m, int count, const real_t* sec, const rea
 	m.positions.assign(pos, pos + (std::size_t)count * m.dims);
 }
 
+// Bulk supply and uptake (src/solver/host/bulk_solver.cpp:20-33, solve_single), for every voxel:
+//   D = (D + dt * S * T) / (1 + dt * (U + S))
+// with the rates the reference's three callbacks return for the voxel, given here as tables:
+// [voxel][s] when per_voxel, else one [s] row for every voxel.
+template <typename real_t>
+void bulk_solve(oracle_state<real_t>& m, const real_t* supply, const real_t* uptake, const real_t* target, int per_voxel)
+{
+	const std::size_t V = m.voxel_count();
+	const int S = m.S;
+	const real_t dt = m.dt;
+#pragma omp for
+	for (std::size_t v = 0; v < V; v++)
+	{
+		const std::size_t row = per_voxel ? v * S : 0;
+		for (int s = 0; s < S; s++)
+		{
+			real_t& d = m.dens[v * S + s];
+			d = (d + dt * supply[row + s] * target[row + s]) / (1 + dt * (uptake[row + s] + supply[row + s]));
+		}
+	}
+}
+
 template <typename real_t>
 void run_steps(oracle_state<real_t>& m, int steps, int first_step)
 {
@@ -772,7 +794,12 @@ void run_steps(oracle_state<real_t>& m, int steps, int first_step)
 	{                                                                                                                  \
 		run_steps(*static_cast<oracle_state<T>*>(h), steps, first_step);                                               \
 	}                                                                                                                  \
-	extern "C" int oracle_##SUFFIX##_is_conflict(void* h) { return static_cast<oracle_state<T>*>(h)->is_conflict; }
+	extern "C" int oracle_##SUFFIX##_is_conflict(void* h) { return static_cast<oracle_state<T>*>(h)->is_conflict; } \
+	extern "C" void oracle_##SUFFIX##_bulk(void* h, const T* supply, const T* uptake, const T* target, int per_voxel) \
+	{                                                                                                                  \
+		auto& m = *static_cast<oracle_state<T>*>(h);                                                                   \
+		_Pragma("omp parallel") bulk_solve(m, supply, uptake, target, per_voxel);                                      \
+	}
 
 ORACLE_EXPORTS(f32, float)
 ORACLE_EXPORTS(f64, double)

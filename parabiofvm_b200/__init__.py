@@ -151,6 +151,18 @@ class Solver:
     def secretion(self, recompute):
         check(self._lib.bfvm_secretion_solve(self._h, int(bool(recompute))))
 
+    def set_bulk_rates(self, supply_rates, uptake_rates, supply_target_densities, per_voxel):
+        """Tabulated bulk supply/uptake rates: [voxel][s] when per_voxel, else one [s] row."""
+        if supply_rates is None:
+            check(self._lib.bfvm_set_bulk_rates(self._h, 0, None, None, None))
+            return
+        n = self.voxel_count * self.S if per_voxel else self.S
+        arrs = [_f32(a, n) for a in (supply_rates, uptake_rates, supply_target_densities)]
+        check(self._lib.bfvm_set_bulk_rates(self._h, int(bool(per_voxel)), *[_fp(a) for a in arrs]))
+
+    def bulk(self):
+        check(self._lib.bfvm_bulk_solve(self._h))
+
     def release(self, index):
         check(self._lib.bfvm_release_internalized(self._h, int(index)))
 

@@ -45,6 +45,8 @@ SIGNATURES = {
     "bfvm_gradient_solve": (c_int, [c_void_p]),
     "bfvm_secretion_solve": (c_int, [c_void_p, c_int]),
     "bfvm_release_internalized": (c_int, [c_void_p, c_int32]),
+    "bfvm_set_bulk_rates": (c_int, [c_void_p, c_int, P(c_float), P(c_float), P(c_float)]),
+    "bfvm_bulk_solve": (c_int, [c_void_p]),
     "bfvm_run_steps": (c_int, [c_void_p, c_int32, c_int32]),
     "bfvm_synchronize": (c_int, [c_void_p]),
     "bfvm_set_option": (c_int, [c_void_p, ctypes.c_char_p, c_int64]),

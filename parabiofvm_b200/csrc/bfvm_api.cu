@@ -90,6 +90,7 @@ static void destroy_all(bfvm_solver* s)
 		free_plan(p);
 	cell_free(s);
 	free_dirichlet(s);
+	free_bulk(s);
 	device_free(s->dens);
 	device_free(s->grad);
 	device_free(s->dev_error);
@@ -541,6 +542,22 @@ int bfvm_secretion_solve(bfvm_solver* s, int recompute)
 {
 	CHECK_SOLVER(s);
 	return launch_secretion(s, recompute != 0);
+}
+
+int bfvm_set_bulk_rates(bfvm_solver* s, int per_voxel, const float* supply_rates, const float* uptake_rates,
+						const float* supply_target_densities)
+{
+	CHECK_SOLVER(s);
+	if (supply_rates && (!uptake_rates || !supply_target_densities))
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "uptake rates and supply target densities must accompany supply rates");
+	free_graphs(s);
+	return set_bulk_rates(s, per_voxel ? 1 : 0, supply_rates, uptake_rates, supply_target_densities);
+}
+
+int bfvm_bulk_solve(bfvm_solver* s)
+{
+	CHECK_SOLVER(s);
+	return launch_bulk(s);
 }
 
 int bfvm_release_internalized(bfvm_solver* s, int32_t index)

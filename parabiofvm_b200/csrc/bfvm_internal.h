@@ -118,6 +118,11 @@ struct bfvm_solver
 
 	bfvm::agent_state ag;
 
+	// bulk supply/uptake: prepared terms, [bulk_rows][S] (bulk_rows 1: one row for every voxel)
+	float* bulk_add = nullptr;
+	float* bulk_den = nullptr;
+	long long bulk_rows = 0;
+
 	int* dev_error = nullptr; // device error flags
 	int* host_error = nullptr; // pinned mirror
 
@@ -150,6 +155,11 @@ void free_dirichlet(bfvm_solver* s);
 
 // gradient.cu
 int launch_gradient(bfvm_solver* s);
+
+// bulk.cu
+int set_bulk_rates(bfvm_solver* s, int per_voxel, const float* supply, const float* uptake, const float* target);
+int launch_bulk(bfvm_solver* s);
+void free_bulk(bfvm_solver* s);
 
 // cell.cu
 int cell_alloc(bfvm_solver* s, int count);

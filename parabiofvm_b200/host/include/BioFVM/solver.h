@@ -59,6 +59,19 @@ public:
 	void solve(microenvironment& m);
 };
 
+// Bulk supply/uptake (src/solver/host/bulk_solver.h of the reference).  initialize() evaluates the
+// microenvironment's three callbacks once for every voxel and keeps the table on the GPU;
+// call it again when the rates change.  solve() applies one step.
+class bulk_solver
+{
+	context& ctx_;
+
+public:
+	explicit bulk_solver(context& ctx) : ctx_(ctx) {}
+	void initialize(microenvironment& m);
+	void solve(microenvironment& m);
+};
+
 class cell_solver
 {
 	context& ctx_;
@@ -87,6 +100,7 @@ public:
 	diffusion_solver diffusion;
 	gradient_solver gradient;
 	dirichlet_solver dirichlet;
+	bulk_solver bulk;
 
 	void initialize(microenvironment& m);
 

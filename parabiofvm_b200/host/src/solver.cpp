@@ -5,6 +5,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../../include/bfvm.h"
 
@@ -28,7 +29,9 @@ static bfvm_solver* require(const context& ctx)
 // ------------------------------------------------------------------------------------------------
 // solver
 
-solver::solver(int device) : ctx_ { nullptr, device }, cell(ctx_), diffusion(ctx_), gradient(ctx_), dirichlet(ctx_) {}
+solver::solver(int device)
+	: ctx_ { nullptr, device }, cell(ctx_), diffusion(ctx_), gradient(ctx_), dirichlet(ctx_), bulk(ctx_)
+{}
 
 solver::~solver()
 {
@@ -112,6 +115,32 @@ void diffusion_solver::solve_axis(microenvironment&, index_t axis)
 void dirichlet_solver::solve(microenvironment&) { check(bfvm_dirichlet_solve(require(ctx_)), "bfvm_dirichlet_solve"); }
 
 void gradient_solver::solve(microenvironment&) { check(bfvm_gradient_solve(require(ctx_)), "bfvm_gradient_solve"); }
+
+void bulk_solver::initialize(microenvironment& m)
+{
+	bfvm_solver* h = require(ctx_);
+	if (!m.supply_rate_func || !m.uptake_rate_func || !m.supply_target_densities_func)
+	{
+		check(bfvm_set_bulk_rates(h, 0, nullptr, nullptr, nullptr), "bfvm_set_bulk_rates");
+		return;
+	}
+	const cartesian_mesh& mesh = m.mesh;
+	const std::size_t S = m.substrates_count;
+	const std::size_t n = mesh.voxel_count() * S;
+	std::vector<real_t> supply(n), uptake(n), target(n);
+	std::size_t v = 0;
+	for (index_t z = 0; z < mesh.grid_shape[2]; z++)
+		for (index_t y = 0; y < mesh.grid_shape[1]; y++)
+			for (index_t x = 0; x < mesh.grid_shape[0]; x++, v++)
+			{
+				m.supply_rate_func(m, { x, y, z }, supply.data() + v * S);
+				m.uptake_rate_func(m, { x, y, z }, uptake.data() + v * S);
+				m.supply_target_densities_func(m, { x, y, z }, target.data() + v * S);
+			}
+	check(bfvm_set_bulk_rates(h, 1, supply.data(), uptake.data(), target.data()), "bfvm_set_bulk_rates");
+}
+
+void bulk_solver::solve(microenvironment&) { check(bfvm_bulk_solve(require(ctx_)), "bfvm_bulk_solve"); }
 
 void cell_solver::initialize(microenvironment&) {}
 

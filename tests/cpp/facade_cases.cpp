@@ -6,6 +6,7 @@
 //   facade_cases host       mesh, builder and agent-container behaviour (no GPU)
 //   facade_cases uniform3d  one diffusion step of the uniform 3D case (test/test.cpp:98-113)
 //   facade_cases step       steps with boundary and interior Dirichlet and agents, plus a release
+//   facade_cases bulk       bulk supply/uptake from the builder's callbacks
 
 #include <cmath>
 #include <cstdio>
@@ -193,6 +194,43 @@ static int mode_step()
 	return 0;
 }
 
+// Bulk supply/uptake through the builder's callbacks (src/solver/host/bulk_solver.cpp): two
+// steps on a 2D mesh with rates that depend on the voxel and the substrate.
+static int mode_bulk()
+{
+	microenvironment_builder b;
+	b.set_time_step(0.5f);
+	b.resize(2, { 0, 0, 0 }, { 140, 100, 0 }, { 20, 20, 20 });
+	b.add_density("a", "u", 10, 0.1f, 2);
+	b.add_density("b", "u", 20, 0.2f, 0.5f);
+	b.add_density("c", "u", 30, 0.3f, 0);
+	b.set_bulk_functions(
+		[](microenvironment& m, point_t<index_t, 3> v, real_t* out) {
+			for (index_t s = 0; s < m.substrates_count; s++)
+				out[s] = 0.1f * (real_t)(v[0] + 1) + 0.01f * (real_t)s;
+		},
+		[](microenvironment& m, point_t<index_t, 3> v, real_t* out) {
+			for (index_t s = 0; s < m.substrates_count; s++)
+				out[s] = 0.05f * (real_t)(v[1] + 1);
+		},
+		[](microenvironment& m, point_t<index_t, 3> v, real_t* out) {
+			for (index_t s = 0; s < m.substrates_count; s++)
+				out[s] = (real_t)(1 + v[0] + 2 * v[1] + s);
+		});
+	microenvironment m = b.build();
+	solver sv;
+	sv.initialize(m);
+	sv.store_data_to_solver(m);
+	sv.bulk.initialize(m);
+	sv.bulk.solve(m);
+	sv.bulk.solve(m);
+	sv.load_data_from_solver(m);
+	std::printf("{");
+	print_array("densities", m.substrate_densities.get(), m.mesh.voxel_count() * m.substrates_count, true);
+	std::printf("}\n");
+	return 0;
+}
+
 int main(int argc, char** argv)
 {
 	const std::string mode = argc > 1 ? argv[1] : "host";
@@ -204,6 +242,8 @@ int main(int argc, char** argv)
 			return mode_uniform3d();
 		if (mode == "step")
 			return mode_step();
+		if (mode == "bulk")
+			return mode_bulk();
 	}
 	catch (const std::exception& e)
 	{

@@ -96,3 +96,24 @@ def test_steps_with_dirichlet_and_agents_match_oracle(program):
     assert rel_err(np.asarray(out["densities"]), o.densities()) < 1e-6
     assert rel_err(np.asarray(out["gradients"]), o.gradients()) < 1e-6
     assert rel_err(np.asarray(out["internalized"]), o.internalized()) < 1e-6
+
+
+@pytest.mark.gpu
+def test_bulk_from_builder_callbacks(program):
+    """The builder's three bulk callbacks, tabulated by bulk.initialize, two bulk.solve steps."""
+    out = run(program, "bulk")
+    f32 = np.float32
+    X, Y, S = 7, 5, 3
+    v = np.arange(X * Y)
+    x, y = (v % X).astype(f32), (v // X).astype(f32)
+    s = np.arange(S, dtype=f32)
+    supply = f32(0.1) * (x[:, None] + f32(1)) + f32(0.01) * s[None, :]
+    uptake = np.broadcast_to(f32(0.05) * (y[:, None] + f32(1)), (X * Y, S)).astype(f32)
+    target = (f32(1) + x[:, None] + f32(2) * y[:, None] + s[None, :]).astype(f32)
+    scn = Scenario(dims=2, bbox_min=(0, 0, 0), bbox_max=(140, 100, 0), voxel_shape=(20, 20, 20),
+                   diffusion_coefficients=[10.0, 20.0, 30.0], decay_rates=[0.1, 0.2, 0.3], time_step=0.5,
+                   initial_conditions=[2.0, 0.5, 0.0])
+    o = make_oracle(scn)
+    for _ in range(2):
+        o.bulk(supply, uptake, target, True)
+    np.testing.assert_array_equal(np.asarray(out["densities"], np.float32), o.densities())
