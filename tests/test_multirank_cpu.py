@@ -46,7 +46,7 @@ def test_replica_timing_takes_the_slowest_rank():
     import torch.multiprocessing as mp
 
     world = 2
-    with mp.Manager() as manager:
+    with mp.get_context("spawn").Manager() as manager:
         results = manager.dict()
         mp.start_processes(_rank_main, args=(world, _free_port(), results), nprocs=world, join=True,
                            start_method="spawn")
