@@ -16,6 +16,11 @@ internalized substrates loaded back, all inside the timed region); ``roofline`` 
 kernel; ``cpu_baseline`` = the CPU oracle on the host cores.  ``--impl reference`` times the CPU
 restatement of the reference's host solvers (the reference itself cannot be built in this image).
 
+``--workload batch-256`` measures the batched-ensemble form instead: 256 independent meshes (edge
+U{24..96} voxels, 1..8 substrates, 100..20,000 agents, per-instance coefficients) stepped together
+as one CUDA graph (bfvm_batch_run_steps), against the same instances stepped one after another on
+one stream.
+
 Multi-GPU: the plain single-mesh step does not shard (its z sweep couples the whole mesh), so
 ``--gpus N`` runs N independent replicas, one per GPU (weak scaling, no collective on the data
 path); the device time is the maximum over ranks.
@@ -261,6 +266,97 @@ def run_reference(args):
     return 0
 
 
+BATCH_INSTANCES = 256
+
+
+def make_batch(seed=20261204, count=BATCH_INSTANCES):
+    """The ensemble of the batch-256 workload: per instance a cubic mesh of edge U{24..96},
+    U{1..8} substrates and U{100..20000} clustered agents, each with its own coefficients."""
+    from parabiofvm_b200.workloads import synthetic
+
+    rng = np.random.default_rng(seed)
+    ws = []
+    for i in range(count):
+        edge = int(rng.integers(24, 97))
+        S = int(rng.integers(1, 9))
+        A = int(rng.integers(100, 20001))
+        ws.append(synthetic(edge, S, A, seed + 1 + i, clustered=True, sigma=100.0, interior_fraction=0.0))
+    return ws
+
+
+def run_batch(args):
+    """The batched-ensemble workload on one GPU: batched (one graph) and sequential (one stream)."""
+    import torch
+
+    from parabiofvm_b200 import Batch
+    from parabiofvm_b200.workloads import make_solver
+
+    t_setup = time.perf_counter()
+    ws = make_batch()
+    units = sum(w.voxel_count * w.S for w in ws)
+    log(f"batch: {len(ws)} instances, {units / 1e6:.1f} M voxel*substrates, built in "
+        f"{time.perf_counter() - t_setup:.1f}s")
+    solvers = [make_solver(w) for w in ws]
+    stream = torch.cuda.Stream()
+
+    def timed(run):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    # batched: the batch's own stream, ordered after / before `stream` through the solvers
+    for s in solvers:
+        s.set_stream(stream.cuda_stream)
+    b = Batch(solvers)
+    b.run_steps(args.warmup, 0)
+    b.synchronize()
+    sampler = ClockSampler(physical_gpu_index(0))
+    sampler.start()
+    time.sleep(1.0)
+    launches0 = sum(s.launch_count for s in solvers)
+    ms_batch = timed(lambda: b.run_steps(args.steps, args.warmup))
+    launches = sum(s.launch_count for s in solvers) - launches0
+    clocks = sampler.stop()
+    b.close()
+
+    # sequential: the same instances, one after another on one stream
+    def sequential():
+        for k in range(args.steps):
+            for s in solvers:
+                s.run_steps(1, args.warmup + args.steps + k)
+
+    for s in solvers:
+        s.run_steps(1, 1)  # graphs of both step kinds exist before timing
+        s.run_steps(1, 10)
+    ms_seq = timed(sequential)
+    for s in solvers:
+        s.close()
+
+    value = units * args.steps / (ms_batch / 1e3)
+    seq = units * args.steps / (ms_seq / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_batch / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"batch-256: {len(ws)} independent meshes, edge U{{24..96}}, 1..8 substrates, "
+                               "100..20,000 clustered agents, per-instance coefficients, recompute every 10th step",
+                   "instances": len(ws), "voxel_substrates": units,
+                   "l2": "ensemble fields 4x the L2, no flush"},
+        "sequential": {"value": seq, "ms_per_step": ms_seq / args.steps,
+                       "what": "the same instances stepped one after another on one stream (bfvm_run_steps)"},
+        "speedup_vs_sequential": value / seq,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def reduce_max_over_ranks(x, world, device):
     """The largest of every rank's ``x`` (the job's time is its slowest replica's)."""
     if world == 1:
@@ -496,7 +592,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plain-320")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch-256"], default="plain-320")
     ap.add_argument("--kernel-reps", type=int, default=5)
     ap.add_argument("--option", action="append", default=[],
                     help="solver tuning option name=value (bfvm_set_option), e.g. tma_sweeps=0")
@@ -512,6 +608,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch-256":
+        return run_batch(args)
     return run_ours(args)
 
 

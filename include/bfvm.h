@@ -166,6 +166,21 @@ int bfvm_bulk_solve(bfvm_solver* s);
 int bfvm_launch_count(const bfvm_solver* s, int64_t* launches);
 
 /*
+ * Batched ensembles (no counterpart in the reference): independent solvers of one device, with
+ * uneven meshes, substrate and agent counts, stepped together.  bfvm_batch_run_steps runs
+ * `steps` steps of every instance (each exactly what bfvm_run_steps runs on that solver alone)
+ * as one CUDA graph whose branches are the instances, so their kernels share the GPU; it is
+ * ordered after work already queued on the instances' streams, and later calls on a solver see
+ * its results.  The batch does not own the solvers; destroy it before them.
+ * bfvm_batch_synchronize waits and returns the first instance's device-side error, if any.
+ */
+typedef struct bfvm_batch bfvm_batch;
+int bfvm_batch_create(bfvm_batch** out, int32_t count, bfvm_solver* const* solvers);
+int bfvm_batch_destroy(bfvm_batch* b);
+int bfvm_batch_run_steps(bfvm_batch* b, int32_t steps, int32_t first_step);
+int bfvm_batch_synchronize(bfvm_batch* b);
+
+/*
  * Secretion and uptake with recompute, for callers that cannot allocate GPU memory: code that runs
  * under a memory budget planned ahead of time, inside a host framework that owns every device
  * allocation, or while another library's stream capture forbids cudaMalloc.  No counterpart in the

@@ -16,7 +16,7 @@ import numpy as np
 from . import _abi
 from ._abi import BfvmError, check
 
-__all__ = ["Solver", "BfvmError", "library_path"]
+__all__ = ["Solver", "Batch", "BfvmError", "library_path"]
 
 
 def library_path() -> str:
@@ -196,3 +196,33 @@ class Solver:
         n = ctypes.c_int64()
         check(self._lib.bfvm_launch_count(self._h, ctypes.byref(n)))
         return int(n.value)
+
+
+class Batch:
+    """Independent solvers of one device stepped together (bfvm_batch_*): each instance runs
+    exactly its own bfvm_run_steps, as branches of one CUDA graph."""
+
+    def __init__(self, solvers):
+        self._lib = _abi.load()
+        self.solvers = list(solvers)
+        arr = (ctypes.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        h = ctypes.c_void_p()
+        check(self._lib.bfvm_batch_create(ctypes.byref(h), len(self.solvers), arr))
+        self._h = h
+
+    def run_steps(self, steps, first_step=0):
+        check(self._lib.bfvm_batch_run_steps(self._h, int(steps), int(first_step)))
+
+    def synchronize(self):
+        check(self._lib.bfvm_batch_synchronize(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.bfvm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

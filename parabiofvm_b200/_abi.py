@@ -53,6 +53,10 @@ SIGNATURES = {
     "bfvm_device_densities": (c_int, [c_void_p, P(P(c_float)), P(c_int64)]),
     "bfvm_device_gradients": (c_int, [c_void_p, P(P(c_float)), P(c_int64)]),
     "bfvm_launch_count": (c_int, [c_void_p, P(c_int64)]),
+    "bfvm_batch_create": (c_int, [P(c_void_p), c_int32, P(c_void_p)]),
+    "bfvm_batch_destroy": (c_int, [c_void_p]),
+    "bfvm_batch_run_steps": (c_int, [c_void_p, c_int32, c_int32]),
+    "bfvm_batch_synchronize": (c_int, [c_void_p]),
     "bfvm_secretion_solve_noalloc": (c_int, [c_void_p, c_int, P(c_int32), P(c_int32), P(c_int32), c_int32, c_float,
                                              c_int32] + [c_void_p] * 8 + [c_void_p]),
 }

@@ -46,8 +46,55 @@ __global__ void secrete_kernel(long long total, int S, float* __restrict__ dens,
 							   const float* __restrict__ red_fac, float* __restrict__ intern, int internalized,
 							   float voxel_volume);
 
+// One (voxel segment, substrate) pair of the secretion update; t < segments * S (secrete_kernel of
+// cell.cu, and the ensemble update of batch_kernels.cu).  See cell.cu for the formulas.
+__device__ __forceinline__ void secrete_element(long long t, int S, float* __restrict__ dens,
+												const int* __restrict__ counts, const int* __restrict__ seg_start,
+												const int* __restrict__ order, const unsigned int* __restrict__ keys,
+												const float* __restrict__ num, const float* __restrict__ den,
+												const float* __restrict__ fac, const float* __restrict__ red_num,
+												const float* __restrict__ red_den, const float* __restrict__ red_fac,
+												float* __restrict__ intern, int internalized, float voxel_volume)
+{
+	const int seg = (int)(t / S);
+	const int s = (int)(t % S);
+	if (seg >= counts[0])
+		return;
+	const int b = seg_start[seg];
+	const size_t dv = (size_t)keys[b] * S + s;
+	const float D = dens[dv];
+	const float rn = red_num[t], rd = red_den[t], rf = red_fac[t];
+
+	if (internalized)
+	{
+		if (!counts[2])
+		{
+			// compute_fused: the voxel holds this one agent
+			const size_t k = (size_t)order[b] * S + s;
+			const float term = __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(__fsub_rn(1.f, rd), D), rn), rd), rf);
+			intern[k] = __fsub_rn(intern[k], __fmul_rn(voxel_volume, term));
+		}
+		else
+		{
+			// compute_internalized for every agent of the voxel, with its own intermediates
+			const int e = seg_start[seg + 1];
+			for (int p = b; p < e; p++)
+			{
+				const size_t k = (size_t)order[p] * S + s;
+				const float dk = den[k];
+				const float term =
+					__fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(-dk, D), num[k]), __fadd_rn(1.f, dk)), fac[k]);
+				intern[k] = __fsub_rn(intern[k], __fmul_rn(voxel_volume, term));
+			}
+		}
+	}
+	dens[dv] = __fadd_rn(__fdiv_rn(__fadd_rn(D, rn), rd), rf);
+}
+
 __global__ void __launch_bounds__(SCAN_THREADS) scan_tile_kernel(const int* in, int* out, long long n, int* tile_sums);
 __global__ void scan_add_kernel(int* out, long long n, const int* tile_offsets);
+
+int rebuild_bins(bfvm_solver* s); // cell.cu: keys, sort, segments, intermediates, reductions
 
 // number of 8-bit radix passes for keys in [0, V] (V marks agents outside the mesh)
 inline int sort_passes(long long V)

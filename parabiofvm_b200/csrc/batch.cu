@@ -1,0 +1,311 @@
+// Batched ensembles: many independent microenvironments (parameter sweeps of an agent-based
+// model, with uneven meshes, substrate and agent counts) stepped together on one GPU.
+//
+// A batch groups existing solvers.  Its step is one CUDA graph built around the ensemble kernels
+// (batch_kernels.cu): one launch per phase (Dirichlet, x/y/z sweeps, gradient, secretion) covers
+// every mesh those kernels take, so a step of 256 meshes is about a dozen launches, not
+// thousands.  Around that chain the graph has parallel branches, on branch streams the batch owns:
+// on recompute steps each mesh with agents rebuilds its voxel binning (it reads agent data only, so
+// it overlaps the diffusion), and a mesh the ensemble kernels do not take (an axis of one voxel,
+// lines of more than 512 voxels, more than 32 substrates) runs its own step.  As for one solver
+// there is one graph for recompute steps and one for the others, rebuilt when any instance changes
+// (its graph epoch advances).
+
+#include <algorithm>
+#include <vector>
+
+#include "agent_kernels.cuh"
+#include "ensemble.h"
+
+struct bfvm_batch
+{
+	int device = 0;
+	std::vector<bfvm_solver*> inst;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t fork = nullptr;
+	std::vector<cudaEvent_t> join;		 // one per instance
+	std::vector<cudaStream_t> branch;	 // capture stream of each instance
+	cudaGraphExec_t graph[2] = { nullptr, nullptr }; // [recompute]
+	std::vector<long long> kernels[2];	 // kernel nodes of each instance in graph[rc]
+	std::vector<long long> epochs[2];	 // instance graph epochs when graph[rc] was captured
+	bfvm::ensemble_plan ens[2];			 // descriptors of the ensemble meshes captured in graph[rc]
+	long long ens_kernels[2] = { 0, 0 }; // ensemble launches in graph[rc] (counted on the first mesh)
+};
+
+namespace bfvm {
+
+static void batch_free_graph(bfvm_batch* b, int rc)
+{
+	if (b->graph[rc])
+		cudaGraphExecDestroy(b->graph[rc]);
+	b->graph[rc] = nullptr;
+}
+
+static bool batch_graph_current(const bfvm_batch* b, int rc)
+{
+	if (!b->graph[rc])
+		return false;
+	for (size_t i = 0; i < b->inst.size(); i++)
+		if (b->epochs[rc][i] != b->inst[i]->graph_epoch)
+			return false;
+	return true;
+}
+
+static int batch_capture(bfvm_batch* b, int rc)
+{
+	batch_free_graph(b, rc);
+	const size_t n = b->inst.size();
+	b->kernels[rc].assign(n, 0);
+	b->epochs[rc].assign(n, 0);
+	std::vector<bfvm_solver*> members;
+	std::vector<char> in_ens(n, 0);
+	for (size_t i = 0; i < n; i++)
+		if (ensemble_eligible(b->inst[i]))
+		{
+			members.push_back(b->inst[i]);
+			in_ens[i] = 1;
+		}
+	int st = ensemble_build(b->ens[rc], members);
+	if (st)
+		return st;
+	const ensemble_plan& plan = b->ens[rc];
+
+	BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+	cudaError_t e = cudaEventRecord(b->fork, b->stream);
+	if (e != cudaSuccess)
+		st = cuda_fail(e, "cudaEventRecord(fork)");
+	// side branches: rebinning of ensemble meshes (recompute steps), whole steps of the others
+	std::vector<char> branched(n, 0), binning(n, 0);
+	for (size_t i = 0; i < n && !st; i++)
+	{
+		bfvm_solver* s = b->inst[i];
+		const bool rebin = in_ens[i] && rc == 1 && s->ag.count > 0;
+		if (in_ens[i] && !rebin)
+			continue;
+		cudaStream_t br = b->branch[i];
+		if ((e = cudaStreamWaitEvent(br, b->fork, 0)) != cudaSuccess)
+		{
+			st = cuda_fail(e, "cudaStreamWaitEvent(fork)");
+			break;
+		}
+		branched[i] = 1;
+		binning[i] = rebin ? 1 : 0;
+		cudaStream_t own = s->stream;
+		s->stream = br;
+		const long long before = s->launches;
+		st = rebin ? rebuild_bins(s) : one_step(s, rc == 1);
+		b->kernels[rc][i] = s->launches - before;
+		s->launches = before;
+		s->stream = own;
+		if ((e = cudaEventRecord(b->join[i], br)) != cudaSuccess && !st)
+			st = cuda_fail(e, "cudaEventRecord(join)");
+	}
+	// the ensemble chain on the batch's stream
+	long long ens_launches = 0;
+	auto count = [&](int r) {
+		if (!r)
+			ens_launches++;
+		return r;
+	};
+	if (!st && plan.count > 0)
+	{
+		int maxdims = 0;
+		for (bfvm_solver* m : members)
+			maxdims = std::max(maxdims, m->dims);
+		for (int axis = 0; axis < maxdims && !st; axis++)
+		{
+			if ((st = count(ensemble_dirichlet(plan, axis, b->stream))))
+				break;
+			st = count(ensemble_sweep(plan, axis, b->stream));
+		}
+		if (!st)
+			st = count(ensemble_dirichlet(plan, maxdims, b->stream));
+		if (!st)
+			st = count(ensemble_gradient(plan, b->stream));
+		// the secretion update waits for the rebinning branches
+		for (size_t i = 0; i < n && !st; i++)
+			if (binning[i] && (e = cudaStreamWaitEvent(b->stream, b->join[i], 0)) != cudaSuccess)
+				st = cuda_fail(e, "join of a binning branch");
+		if (!st)
+			st = count(ensemble_secretion(plan, b->stream));
+	}
+	// join every branch (also after a failure, so the capture ends cleanly)
+	for (size_t i = 0; i < n; i++)
+		if (branched[i])
+			cudaStreamWaitEvent(b->stream, b->join[i], 0);
+	cudaGraph_t g = nullptr;
+	e = cudaStreamEndCapture(b->stream, &g);
+	if (!st && e != cudaSuccess)
+		st = cuda_fail(e, "cudaStreamEndCapture(batch)");
+	if (!st)
+	{
+		e = cudaGraphInstantiate(&b->graph[rc], g, 0);
+		if (e != cudaSuccess)
+		{
+			b->graph[rc] = nullptr;
+			st = cuda_fail(e, "cudaGraphInstantiate(batch)");
+		}
+	}
+	if (g)
+		cudaGraphDestroy(g);
+	if (st)
+		return st;
+	b->ens_kernels[rc] = ens_launches;
+	for (size_t i = 0; i < n; i++)
+		b->epochs[rc][i] = b->inst[i]->graph_epoch;
+	return BFVM_OK;
+}
+
+// Work on the batch's stream after everything already queued on the instances' streams, and the
+// other way round (calls on one solver afterwards see the batch's steps).
+static int batch_wait_instances(bfvm_batch* b)
+{
+	for (size_t i = 0; i < b->inst.size(); i++)
+	{
+		BFVM_CUDA(cudaEventRecord(b->join[i], b->inst[i]->stream));
+		BFVM_CUDA(cudaStreamWaitEvent(b->stream, b->join[i], 0));
+	}
+	return BFVM_OK;
+}
+
+static int instances_wait_batch(bfvm_batch* b)
+{
+	BFVM_CUDA(cudaEventRecord(b->fork, b->stream));
+	for (bfvm_solver* s : b->inst)
+		BFVM_CUDA(cudaStreamWaitEvent(s->stream, b->fork, 0));
+	return BFVM_OK;
+}
+
+} // namespace bfvm
+
+using namespace bfvm;
+
+extern "C" {
+
+int bfvm_batch_create(bfvm_batch** out, int32_t count, bfvm_solver* const* solvers)
+{
+	if (!out)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null output pointer");
+	*out = nullptr;
+	if (count <= 0 || !solvers)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "a batch needs at least one solver");
+	for (int32_t i = 0; i < count; i++)
+	{
+		if (!solvers[i])
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "null solver in the batch");
+		if (solvers[i]->device != solvers[0]->device)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "the solvers of a batch must share one device");
+		for (int32_t k = 0; k < i; k++)
+			if (solvers[k] == solvers[i])
+				return fail(BFVM_ERR_INVALID_ARGUMENT, "a solver appears twice in the batch");
+	}
+	auto* b = new (std::nothrow) bfvm_batch();
+	if (!b)
+		return fail(BFVM_ERR_OUT_OF_MEMORY, "host allocation failed");
+	b->device = solvers[0]->device;
+	b->inst.assign(solvers, solvers + count);
+	b->join.assign(count, nullptr);
+	b->branch.assign(count, nullptr);
+	int st = BFVM_OK;
+	cudaError_t e = cudaSetDevice(b->device);
+	if (e == cudaSuccess)
+		e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+	if (e == cudaSuccess)
+		e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+	for (int32_t i = 0; i < count && e == cudaSuccess; i++)
+	{
+		e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+		if (e == cudaSuccess)
+			e = cudaStreamCreateWithFlags(&b->branch[i], cudaStreamNonBlocking);
+	}
+	if (e != cudaSuccess)
+		st = cuda_fail(e, "batch stream and events");
+	if (st)
+	{
+		bfvm_batch_destroy(b);
+		return st;
+	}
+	*out = b;
+	return BFVM_OK;
+}
+
+int bfvm_batch_destroy(bfvm_batch* b)
+{
+	if (!b)
+		return BFVM_OK;
+	cudaSetDevice(b->device);
+	if (b->stream)
+		cudaStreamSynchronize(b->stream);
+	batch_free_graph(b, 0);
+	batch_free_graph(b, 1);
+	ensemble_free(b->ens[0]);
+	ensemble_free(b->ens[1]);
+	for (cudaEvent_t ev : b->join)
+		if (ev)
+			cudaEventDestroy(ev);
+	for (cudaStream_t st : b->branch)
+		if (st)
+			cudaStreamDestroy(st);
+	if (b->fork)
+		cudaEventDestroy(b->fork);
+	if (b->stream)
+		cudaStreamDestroy(b->stream);
+	delete b;
+	return BFVM_OK;
+}
+
+int bfvm_batch_run_steps(bfvm_batch* b, int32_t steps, int32_t first_step)
+{
+	if (!b)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null batch");
+	if (steps < 0)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "steps must not be negative");
+	BFVM_CUDA(cudaSetDevice(b->device));
+	int st;
+	if ((st = batch_wait_instances(b)))
+		return st;
+	for (int32_t i = 0; i < steps; i++)
+	{
+		const int rc = ((first_step + i) % 10 == 0) ? 1 : 0;
+		bool eager = false;
+		for (bfvm_solver* s : b->inst)
+			eager = eager || (!rc && s->ag.count > 0 && !s->ag.binned);
+		if (eager)
+		{
+			// an instance whose agents were never binned rebins on its own stream this once
+			if ((st = instances_wait_batch(b)))
+				return st;
+			for (bfvm_solver* s : b->inst)
+				if ((st = one_step(s, false)))
+					return st;
+			if ((st = batch_wait_instances(b)))
+				return st;
+			continue;
+		}
+		if (!batch_graph_current(b, rc) && (st = batch_capture(b, rc)))
+			return st;
+		BFVM_CUDA(cudaGraphLaunch(b->graph[rc], b->stream));
+		for (size_t k = 0; k < b->inst.size(); k++)
+			b->inst[k]->launches += b->kernels[rc][k];
+		b->inst[0]->launches += b->ens_kernels[rc];
+	}
+	return instances_wait_batch(b);
+}
+
+int bfvm_batch_synchronize(bfvm_batch* b)
+{
+	if (!b)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null batch");
+	BFVM_CUDA(cudaSetDevice(b->device));
+	BFVM_CUDA(cudaStreamSynchronize(b->stream));
+	int first = BFVM_OK;
+	for (bfvm_solver* s : b->inst)
+	{
+		const int st = check_device_errors(s);
+		if (st && !first)
+			first = st;
+	}
+	return first;
+}
+
+} // extern "C"

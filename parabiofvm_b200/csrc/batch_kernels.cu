@@ -1,0 +1,580 @@
+// Ensemble kernels: one launch per phase of the step (Dirichlet overwrite, the sweeps, gradient,
+// secretion update) for every mesh of a batch.  Each phase has a prefix list of work units over the
+// meshes; a CTA maps its unit to the mesh that owns it (binary search of the prefix list) and runs
+// that mesh's arithmetic, the same as the mesh's own kernels, so a batch reproduces every mesh
+// stepped alone bit for bit.
+//
+// The sweep kernel reads its lines straight from global memory (coalesced 128-byte rows, 32
+// independent loads per thread) rather than through TMA stages: ensemble meshes are small, and
+// many small CTAs keep the GPU busy where staging depth would not.  It uses the front-padded block
+// algebra of sweep_tma.cu (precompute_padded), and also serves a single mesh whose shape the TMA
+// path does not take.
+
+#include <algorithm>
+
+#include "agent_kernels.cuh"
+#include "ensemble.h"
+#include "sweep_common.cuh"
+
+namespace bfvm {
+
+// mesh that owns work unit u: the last i with first[i] <= u
+__device__ __forceinline__ int find_mesh(const long long* __restrict__ first, int count, long long u)
+{
+	int lo = 0, hi = count - 1;
+	while (lo < hi)
+	{
+		const int mid = (lo + hi + 1) >> 1;
+		if (__ldg(&first[mid]) <= u)
+			lo = mid;
+		else
+			hi = mid - 1;
+	}
+	return lo;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Dirichlet overwrite, gradient, secretion: 256-element blocks
+
+__global__ void __launch_bounds__(256) ens_dirichlet_kernel(const ens_inst* __restrict__ inst,
+															 const long long* __restrict__ first, int count,
+															 long long units, int phase)
+{
+	for (long long u = blockIdx.x; u < units; u += gridDim.x)
+	{
+		const int i = find_mesh(first, count, u);
+		const ens_inst& m = inst[i];
+		if (phase > m.dims)
+			continue;
+		const long long e = (u - first[i]) * 256 + threadIdx.x;
+		if (e < m.dir_count)
+			m.dens[__ldg(&m.dir_idx[e])] = __ldg(&m.dir_val[e]);
+	}
+}
+
+__device__ __forceinline__ float ens_axis_grad(const float* __restrict__ u, long long i, int pos, int n,
+											   long long stride, float border, float center)
+{
+	if (n == 1)
+		return 0.f;
+	if (pos == 0)
+		return __fmul_rn(__fsub_rn(__ldg(&u[i + stride]), __ldg(&u[i])), border);
+	if (pos == n - 1)
+		return __fmul_rn(__fsub_rn(__ldg(&u[i]), __ldg(&u[i - stride])), border);
+	return __fmul_rn(__fsub_rn(__ldg(&u[i + stride]), __ldg(&u[i - stride])), center);
+}
+
+// central differences (gradient.cu); output layouts 1D [x][s][1], 2D [y][x][s][2], 3D [3][z][y][x][s].
+// One unit is 256 consecutive columns of the (y, x, s) plane over up to ENS_GRAD_ZC planes: each
+// thread marches z keeping u(z-1), u(z), u(z+1) in registers (gradient3d_vec4_kernel of gradient.cu
+// for any S), reading x and y neighbours from L1/L2.
+static constexpr int ENS_GRAD_ZC = 32;
+
+__global__ void __launch_bounds__(256) ens_gradient_kernel(const ens_inst* __restrict__ inst,
+															const long long* __restrict__ first, int count,
+															long long units)
+{
+	for (long long u = blockIdx.x; u < units; u += gridDim.x)
+	{
+		const int i = find_mesh(first, count, u);
+		const ens_inst& m = inst[i];
+		const int S = m.S, X = m.X, Y = m.Y, Z = m.Z, dims = m.dims;
+		const int XS = X * S;
+		const int plane_cols = XS * Y;
+		const int ncx = (plane_cols + 255) / 256;
+		const int local = (int)(u - first[i]);
+		const int cx = local % ncx;
+		const int z0 = (local / ncx) * ENS_GRAD_ZC;
+		const int z1 = min(Z, z0 + ENS_GRAD_ZC);
+		const int c = cx * 256 + threadIdx.x; // column of the plane: y * XS + q
+		if (c >= plane_cols)
+			continue;
+		const int y = c / XS;
+		const int q = c - y * XS;
+		const int x = q / S;
+		const float* __restrict__ d = m.dens;
+		float* __restrict__ g = m.grad;
+		const long long plane = (long long)Y * XS;
+		const long long total = plane * Z;
+		const long long row = (long long)y * XS + q;
+		float prev = z0 > 0 ? __ldg(&d[(long long)(z0 - 1) * plane + row]) : 0.f;
+		float cur = __ldg(&d[(long long)z0 * plane + row]);
+		for (int z = z0; z < z1; z++)
+		{
+			const long long e = (long long)z * plane + row;
+			const float next = z + 1 < Z ? __ldg(&d[e + plane]) : cur;
+			const float gx = ens_axis_grad(d, e, x, X, S, m.bgrad[0], m.cgrad[0]);
+			if (dims == 1)
+				g[e] = gx;
+			else
+			{
+				const float gy = ens_axis_grad(d, e, y, Y, XS, m.bgrad[1], m.cgrad[1]);
+				if (dims == 2)
+				{
+					g[2 * e] = gx;
+					g[2 * e + 1] = gy;
+				}
+				else
+				{
+					float gz;
+					if (Z == 1)
+						gz = 0.f;
+					else if (z == 0)
+						gz = __fmul_rn(__fsub_rn(next, cur), m.bgrad[2]);
+					else if (z == Z - 1)
+						gz = __fmul_rn(__fsub_rn(cur, prev), m.bgrad[2]);
+					else
+						gz = __fmul_rn(__fsub_rn(next, prev), m.cgrad[2]);
+					__stcs(&g[e], gx);
+					__stcs(&g[total + e], gy);
+					__stcs(&g[2 * total + e], gz);
+				}
+			}
+			prev = cur;
+			cur = next;
+		}
+	}
+}
+
+__global__ void __launch_bounds__(256) ens_secretion_kernel(const ens_inst* __restrict__ inst,
+															 const long long* __restrict__ first, int count,
+															 long long units)
+{
+	for (long long u = blockIdx.x; u < units; u += gridDim.x)
+	{
+		const int i = find_mesh(first, count, u);
+		const ens_inst& m = inst[i];
+		const long long t = (u - first[i]) * 256 + threadIdx.x;
+		if (t >= m.AS)
+			continue;
+		secrete_element(t, m.S, m.dens, m.counts, m.seg_start, m.order, m.keys, m.num, m.den, m.fac, m.red_num,
+						m.red_den, m.red_fac, m.intern, m.internalized, m.voxel_volume);
+	}
+}
+
+// ------------------------------------------------------------------------------------------------
+// sweeps: one unit = one tile of 32 lines (the tiles of sweep_tma.cu), blockDim = (32, maxP)
+
+// staged tables of one mesh and axis: (tg, G) pairs and b' as [S][NP], NP = 32P + 1, then c [S]
+__device__ __forceinline__ void ens_stage_tables(const float* __restrict__ vtab, int P, int S, float* tab)
+{
+	const int N = 32 * P, NP = N + 1;
+	float2* tgtab = reinterpret_cast<float2*>(tab);
+	float* btab = tab + 2 * S * NP;
+	float* ctab = btab + S * NP;
+	const float2* gt = reinterpret_cast<const float2*>(vtab + (size_t)N * S);
+	const int nthr = blockDim.x * blockDim.y;
+	const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+	for (int t = tid; t < N * S; t += nthr)
+	{
+		const int v = t / S, s = t - v * S;
+		btab[s * NP + v] = __ldg(&vtab[t]);
+		tgtab[s * NP + v] = __ldg(&gt[t]);
+	}
+	for (int t = tid; t < S; t += nthr)
+		ctab[t] = __ldg(&vtab[(size_t)3 * N * S + t]);
+}
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+				 : "memory");
+}
+
+// x tiles: rows [row0, row0 + rows) of mesh m, contiguous in the field, into `xs` at `pitch`
+__device__ __forceinline__ void x_tile_rows(const ens_inst& m, long long local, long long& row0, int& rows)
+{
+	const int R = 32 / m.S;
+	row0 = local * R;
+	rows = (int)min((long long)R, (long long)m.Y * m.Z - row0);
+}
+
+__device__ __forceinline__ void x_prefetch(const ens_inst& m, long long local, float* xs, int tid, int nthr)
+{
+	long long row0;
+	int rows;
+	x_tile_rows(m, local, row0, rows);
+	const int XS = m.X * m.S;
+	const int pitch = XS | 1;
+	const float* src = m.dens + row0 * XS;
+	const int total = rows * XS;
+	for (int t = tid; t < total; t += nthr)
+	{
+		const int r = (unsigned)t / (unsigned)XS;
+		cp_async4(xs + r * pitch + (t - r * XS), src + t);
+	}
+	asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// x sweep: the R = 32/S rows of a tile are contiguous in the field; they are copied into shared
+// memory (row pitch XS | 1, so the lanes spread over the banks) and written back with coalesced
+// accesses, instead of each lane walking its own row.  Two buffers alternate: the copy of the
+// CTA's next tile is in flight (cp.async) while it solves the current one.
+template <int AXIS>
+__global__ void __launch_bounds__(512) ens_sweep_kernel(const ens_inst* __restrict__ inst,
+														 const long long* __restrict__ first, int count,
+														 long long units, long long chunk, int maxP, int table_floats,
+														 long long xstage_floats)
+{
+	constexpr int M = 32;
+	extern __shared__ __align__(16) float ens_smem[];
+	const int lane = threadIdx.x;
+	const int j = threadIdx.y;
+	const int tid = lane + 32 * j;
+	const int nthr = 32 * blockDim.y;
+	float* carry_f = ens_smem;				 // [maxP][32]
+	float* carry_t = carry_f + maxP * 32;	 // [maxP][32]
+	float* tab = carry_t + maxP * 32;		 // tables of the current mesh (16-byte aligned: maxP*64 floats)
+	float* xs_buf = tab + table_floats;		 // x sweep: two buffers of the tile's rows
+	int xstage = 0;
+	if (AXIS == 0)
+		xstage = (int)xstage_floats;
+
+	const long long u0 = (long long)blockIdx.x * chunk;
+	const long long u1 = min(units, u0 + chunk);
+	if (AXIS == 0 && u0 < u1)
+	{
+		const int i0 = find_mesh(first, count, u0);
+		x_prefetch(inst[i0], u0 - first[i0], xs_buf, tid, nthr);
+	}
+	int cur = -1;
+	int it = 0;
+	for (long long u = u0; u < u1; u++, it++)
+	{
+		const int i = find_mesh(first, count, u);
+		const ens_inst& m = inst[i];
+		const int S = m.S, P = m.vP[AXIS], pad = m.pad[AXIS];
+		const float* vtab = m.vtab[AXIS];
+		if (i != cur)
+		{
+			__syncthreads(); // the previous mesh's tables are no longer read
+			ens_stage_tables(vtab, P, S, tab);
+			__syncthreads();
+			cur = i;
+		}
+		const int N = 32 * P, NP = N + 1;
+		const float2* tgtab = reinterpret_cast<const float2*>(tab);
+		const float* btab = tab + 2 * S * NP;
+		const float* ctab = btab + S * NP;
+		const float* gqtab = vtab + (size_t)3 * N * S + S;
+		const float* tgptab = gqtab + P * S;
+		const float* Gptab = tgptab + P * S;
+
+		// the line of this lane
+		const long long local = u - first[i];
+		const long long XS = (long long)m.X * S;
+		bool active;
+		int s;
+		float* line;
+		long long stride;
+		long long row0 = 0;
+		int rows = 0, pitch = 1;
+		float* xs = xs_buf + (it & 1) * xstage;
+		if (AXIS == 0)
+		{
+			const int rl = lane / S;
+			s = lane - rl * S;
+			x_tile_rows(m, local, row0, rows);
+			pitch = (int)(XS | 1);
+			active = rl < rows;
+			// the next tile's rows into the other buffer, then wait for this tile's
+			if (u + 1 < u1)
+			{
+				const int in = find_mesh(first, count, u + 1);
+				x_prefetch(inst[in], u + 1 - first[in], xs_buf + ((it + 1) & 1) * xstage, tid, nthr);
+				asm volatile("cp.async.wait_group 1;" ::: "memory");
+			}
+			else
+				asm volatile("cp.async.wait_group 0;" ::: "memory");
+			__syncthreads();
+			line = xs + (active ? rl : 0) * pitch + s;
+			stride = S;
+		}
+		else
+		{
+			const long long ncols = AXIS == 1 ? XS : XS * m.Y;
+			const long long col_tiles = (ncols + 31) / 32;
+			const long long outer = AXIS == 1 ? local / col_tiles : 0;
+			const long long q = (AXIS == 1 ? local % col_tiles : local) * 32 + lane;
+			active = q < ncols;
+			const long long qq = active ? q : 0;
+			s = (int)(qq % S);
+			line = m.dens + outer * XS * m.Y + qq;
+			stride = AXIS == 1 ? XS : XS * m.Y;
+		}
+		const bool mine = j < P; // warps past this mesh's blocks only join the barriers
+		const int p = 32 * j;
+		float d[M];
+		float C = 0.f;
+		if (mine)
+		{
+			const float cs = ctab[s];
+			const float* bcol = btab + s * NP + p;
+#pragma unroll
+			for (int k = 0; k < M; k++)
+			{
+				const int r = p + k - pad; // real element of virtual element p + k
+				d[k] = (active && r >= 0) ? line[(long long)r * stride] : 0.f;
+			}
+			// forward and backward recurrences from zero carries (sweep_tma.cu)
+#pragma unroll
+			for (int k = 1; k < M; k++)
+				d[k] = __fsub_rn(d[k], __fmul_rn(__fmul_rn(cs, bcol[k - 1]), d[k - 1]));
+			carry_f[j * 32 + lane] = d[M - 1];
+			d[M - 1] = __fmul_rn(d[M - 1], bcol[M - 1]);
+#pragma unroll
+			for (int k = M - 2; k >= 0; k--)
+				d[k] = __fmul_rn(__fsub_rn(d[k], __fmul_rn(cs, d[k + 1])), bcol[k]);
+		}
+		__syncthreads();
+		if (mine && P > 1)
+		{
+			if (j > 0)
+			{
+				C = carry_f[lane];
+				for (int k = 1; k < j; k++)
+					C = fmaf(__ldg(&gqtab[k * S + s]), C, carry_f[k * 32 + lane]);
+			}
+			carry_t[j * 32 + lane] = fmaf(C, __ldg(&tgptab[j * S + s]), d[0]);
+		}
+		__syncthreads();
+		if (mine)
+		{
+			if (P > 1)
+			{
+				float Xc = 0.f;
+				if (j < P - 1)
+				{
+					Xc = carry_t[(P - 1) * 32 + lane];
+					for (int k = P - 2; k > j; k--)
+						Xc = fmaf(__ldg(&Gptab[k * S + s]), Xc, carry_t[k * 32 + lane]);
+				}
+				const float2* tcol = tgtab + s * NP + p;
+#pragma unroll
+				for (int k = 0; k < M; k++)
+				{
+					const float2 r = tcol[k];
+					d[k] = fmaf(Xc, r.y, fmaf(C, r.x, d[k]));
+				}
+			}
+			if (active)
+			{
+#pragma unroll
+				for (int k = 0; k < M; k++)
+				{
+					const int r = p + k - pad;
+					if (r >= 0)
+						line[(long long)r * stride] = d[k];
+				}
+			}
+		}
+		__syncthreads(); // carries of this tile read before the next tile writes them
+		if (AXIS == 0)
+		{
+			// the solved rows back to the field, coalesced
+			float* dst = m.dens + row0 * XS;
+			const int total = rows * (int)XS;
+			for (int t = tid; t < total; t += nthr)
+			{
+				const int r = (unsigned)t / (unsigned)XS;
+				dst[t] = xs[r * pitch + (t - r * (int)XS)];
+			}
+			__syncthreads(); // this buffer is read before the prefetch after next refills it
+		}
+	}
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+
+bool ensemble_eligible(const bfvm_solver* s)
+{
+	for (int d = 0; d < s->dims; d++)
+	{
+		const sweep_plan& p = s->plan[d];
+		if (!p.vtab || p.vP > ENS_MAX_P || p.n < 2)
+			return false;
+	}
+	// x tiles hold whole rows of at most 32 substrate lines; element indices fit 31 bits
+	return s->S <= 32 && s->V * s->S < (1LL << 31);
+}
+
+static size_t staged_floats(int P, int S) { return 3 * (size_t)S * (32 * P + 1) + S; }
+
+void ensemble_free(ensemble_plan& plan)
+{
+	device_free(plan.inst);
+	for (auto& f : plan.first)
+		device_free(f);
+	for (auto& f : plan.first_h)
+		f.clear();
+	plan.count = 0;
+}
+
+int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
+{
+	ensemble_free(plan);
+	const int n = (int)meshes.size();
+	if (n == 0)
+		return BFVM_OK;
+	std::vector<ens_inst> h(n);
+	for (auto& f : plan.first_h)
+		f.assign(n + 1, 0);
+	plan.maxP[0] = plan.maxP[1] = plan.maxP[2] = 1;
+	plan.table_floats[0] = plan.table_floats[1] = plan.table_floats[2] = 0;
+	plan.maxS = 1;
+	plan.xstage_floats = 0;
+	for (int i = 0; i < n; i++)
+	{
+		const bfvm_solver* s = meshes[i];
+		ens_inst& m = h[i];
+		m.dens = s->dens;
+		m.grad = s->grad;
+		m.dims = s->dims;
+		m.S = s->S;
+		m.X = s->grid[0];
+		m.Y = s->grid[1];
+		m.Z = s->grid[2];
+		for (int d = 0; d < 3; d++)
+		{
+			m.bgrad[d] = d < s->dims ? 1.f / s->voxel[d] : 0.f;
+			m.cgrad[d] = d < s->dims ? 1.f / (s->voxel[d] * 2) : 0.f;
+			m.vtab[d] = d < s->dims ? s->plan[d].vtab : nullptr;
+			m.vP[d] = d < s->dims ? s->plan[d].vP : 1;
+			m.pad[d] = d < s->dims ? s->plan[d].pad : 0;
+		}
+		m.dir_idx = s->dir_idx;
+		m.dir_val = s->dir_val;
+		m.dir_count = s->dir_count;
+		const agent_state& a = s->ag;
+		m.AS = (long long)a.count * s->S;
+		m.internalized = s->internalized ? 1 : 0;
+		m.voxel_volume = (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]);
+		m.counts = a.seg_count_dev;
+		m.seg_start = a.seg_start;
+		m.order = a.vals;
+		m.keys = a.keys;
+		m.num = a.num;
+		m.den = a.den;
+		m.fac = a.fac;
+		m.red_num = a.red_num;
+		m.red_den = a.red_den;
+		m.red_fac = a.red_fac;
+		m.intern = a.intern;
+
+		const long long X = m.X, Y = m.Y, Z = m.Z, S = m.S, XS = X * S;
+		long long units[ENS_PHASES] = { 0, 0, 0, 0, 0, 0 };
+		units[ENS_DIRICHLET] = (m.dir_count + 255) / 256;
+		const long long R = 32 / S; // x tiles: rows of at most 32 substrate lines
+		units[ENS_SWEEP_X] = R > 0 ? (Y * Z + R - 1) / R : 0;
+		units[ENS_SWEEP_Y] = s->dims >= 2 ? Z * ((XS + 31) / 32) : 0;
+		units[ENS_SWEEP_Z] = s->dims >= 3 ? (Y * XS + 31) / 32 : 0;
+		units[ENS_GRADIENT] = ((XS * Y + 255) / 256) * ((Z + ENS_GRAD_ZC - 1) / ENS_GRAD_ZC);
+		units[ENS_SECRETION] = (m.AS + 255) / 256;
+		for (int ph = 0; ph < ENS_PHASES; ph++)
+			plan.first_h[ph][i + 1] = plan.first_h[ph][i] + units[ph];
+		for (int d = 0; d < s->dims; d++)
+		{
+			plan.maxP[d] = std::max(plan.maxP[d], m.vP[d]);
+			plan.table_floats[d] = std::max(plan.table_floats[d], staged_floats(m.vP[d], m.S));
+		}
+		plan.maxS = std::max(plan.maxS, m.S);
+		if (R > 0)
+			plan.xstage_floats = std::max(plan.xstage_floats, (size_t)(R * (XS | 1)));
+	}
+	int st;
+	if ((st = device_alloc(&plan.inst, (size_t)n)))
+		return st;
+	BFVM_CUDA(cudaMemcpy(plan.inst, h.data(), n * sizeof(ens_inst), cudaMemcpyHostToDevice));
+	for (int ph = 0; ph < ENS_PHASES; ph++)
+	{
+		if ((st = device_alloc(&plan.first[ph], (size_t)n + 1)))
+			return st;
+		BFVM_CUDA(cudaMemcpy(plan.first[ph], plan.first_h[ph].data(), (n + 1) * sizeof(long long),
+							 cudaMemcpyHostToDevice));
+	}
+	plan.count = n;
+	return BFVM_OK;
+}
+
+static int current_device_sms()
+{
+	int dev = 0;
+	cudaGetDevice(&dev);
+	return sm_count_impl(dev);
+}
+
+static unsigned element_grid(long long units)
+{
+	return (unsigned)std::max<long long>(1, std::min<long long>(units, (long long)current_device_sms() * 16));
+}
+
+static int launched(const char* what)
+{
+	cudaError_t e = cudaGetLastError();
+	return e == cudaSuccess ? BFVM_OK : cuda_fail(e, what);
+}
+
+int ensemble_dirichlet(const ensemble_plan& plan, int phase, cudaStream_t stream)
+{
+	const long long units = plan.count ? plan.first_h[ENS_DIRICHLET][plan.count] : 0;
+	if (units == 0)
+		return BFVM_OK;
+	ens_dirichlet_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_DIRICHLET], plan.count,
+																   units, phase);
+	return launched("ens_dirichlet_kernel");
+}
+
+int ensemble_gradient(const ensemble_plan& plan, cudaStream_t stream)
+{
+	const long long units = plan.count ? plan.first_h[ENS_GRADIENT][plan.count] : 0;
+	if (units == 0)
+		return BFVM_OK;
+	ens_gradient_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT], plan.count,
+																  units);
+	return launched("ens_gradient_kernel");
+}
+
+int ensemble_secretion(const ensemble_plan& plan, cudaStream_t stream)
+{
+	const long long units = plan.count ? plan.first_h[ENS_SECRETION][plan.count] : 0;
+	if (units == 0)
+		return BFVM_OK;
+	ens_secretion_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_SECRETION], plan.count,
+																   units);
+	return launched("ens_secretion_kernel");
+}
+
+template <int AXIS>
+static int launch_ens_sweep(const ensemble_plan& plan, long long units, cudaStream_t stream)
+{
+	auto kernel = ens_sweep_kernel<AXIS>;
+	const int P = plan.maxP[AXIS];
+	const size_t xstage = AXIS == 0 ? plan.xstage_floats : 0;
+	const size_t smem = (2 * (size_t)P * 32 + plan.table_floats[AXIS] + 2 * xstage) * sizeof(float);
+	int rc = set_smem(kernel, smem);
+	if (rc)
+		return rc;
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * P, smem);
+	const long long slots = (long long)std::max(per_sm, 1) * current_device_sms();
+	const long long chunk = std::max<long long>(1, (units + slots - 1) / slots);
+	const unsigned grid = (unsigned)((units + chunk - 1) / chunk);
+	kernel<<<grid, dim3(32, P), smem, stream>>>(plan.inst, plan.first[ENS_SWEEP_X + AXIS], plan.count, units, chunk, P,
+												 (int)plan.table_floats[AXIS], (long long)xstage);
+	return launched("ens_sweep_kernel");
+}
+
+int ensemble_sweep(const ensemble_plan& plan, int axis, cudaStream_t stream)
+{
+	const long long units = plan.count ? plan.first_h[ENS_SWEEP_X + axis][plan.count] : 0;
+	if (units == 0)
+		return BFVM_OK;
+	if (axis == 0)
+		return launch_ens_sweep<0>(plan, units, stream);
+	if (axis == 1)
+		return launch_ens_sweep<1>(plan, units, stream);
+	return launch_ens_sweep<2>(plan, units, stream);
+}
+
+} // namespace bfvm

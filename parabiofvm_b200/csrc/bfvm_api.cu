@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "bfvm_internal.h"
+#include "ensemble.h"
 
 namespace bfvm {
 
@@ -79,6 +80,7 @@ static void free_graphs(bfvm_solver* s)
 			g = nullptr;
 		}
 	s->graphs_dirty = true;
+	s->graph_epoch++; // graphs that captured this solver's buffers (its own, a batch's) are stale
 }
 
 static void destroy_all(bfvm_solver* s)
@@ -91,6 +93,12 @@ static void destroy_all(bfvm_solver* s)
 	cell_free(s);
 	free_dirichlet(s);
 	free_bulk(s);
+	if (s->self_plan)
+	{
+		ensemble_free(*s->self_plan);
+		delete s->self_plan;
+		s->self_plan = nullptr;
+	}
 	device_free(s->dens);
 	device_free(s->grad);
 	device_free(s->dev_error);
@@ -101,7 +109,7 @@ static void destroy_all(bfvm_solver* s)
 }
 
 // error flags raised by kernels since the last check
-static int check_device_errors(bfvm_solver* s)
+int check_device_errors(bfvm_solver* s)
 {
 	BFVM_CUDA(cudaMemcpyAsync(s->host_error, s->dev_error, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
 	BFVM_CUDA(cudaStreamSynchronize(s->stream));
@@ -127,7 +135,7 @@ static int diffusion(bfvm_solver* s)
 	return BFVM_OK;
 }
 
-static int one_step(bfvm_solver* s, bool recompute)
+int one_step(bfvm_solver* s, bool recompute)
 {
 	int st;
 	if ((st = diffusion(s)) || (st = launch_gradient(s)) || (st = launch_secretion(s, recompute)))
@@ -271,6 +279,15 @@ int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_
 		}
 		for (int d = 0; d < dims && !st; d++)
 			st = upload_plan(s, d);
+		if (st)
+			break;
+		s->self_plan = new (std::nothrow) ensemble_plan();
+		if (!s->self_plan)
+		{
+			st = fail(BFVM_ERR_OUT_OF_MEMORY, "host allocation failed");
+			break;
+		}
+		st = ensemble_build(*s->self_plan, { s });
 	} while (0);
 
 	if (st)

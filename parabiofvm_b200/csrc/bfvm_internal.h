@@ -11,6 +11,8 @@
 
 namespace bfvm {
 
+struct ensemble_plan;
+
 // ------------------------------------------------------------------------------------------------
 // errors
 
@@ -133,6 +135,11 @@ struct bfvm_solver
 	cudaGraphExec_t step_graph[2] = { nullptr, nullptr };
 	long long graph_kernels[2] = { 0, 0 }; // kernel nodes per step graph
 	bool graphs_dirty = true;
+	long long graph_epoch = 0; // advances whenever captured buffers or launch shapes may have changed
+
+	// this mesh alone as an ensemble: its sweeps run the ensemble sweep kernel on shapes the TMA
+	// path does not take (built at creation, so never inside a stream capture)
+	bfvm::ensemble_plan* self_plan = nullptr;
 };
 
 namespace bfvm {
@@ -145,6 +152,10 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 int padded_table_floats(int P, int S);
 void precompute_padded(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int& P, int& pad,
 					   std::vector<float>& tab);
+
+// bfvm_api.cu
+int one_step(bfvm_solver* s, bool recompute); // diffusion, gradient, secretion on the solver's stream
+int check_device_errors(bfvm_solver* s);	  // waits for the stream, reports device-side error flags
 
 // sweep.cu
 int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);

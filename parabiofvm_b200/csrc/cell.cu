@@ -232,39 +232,8 @@ __global__ void secrete_kernel(long long total, int S, float* __restrict__ dens,
 	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= total)
 		return;
-	const int seg = (int)(t / S);
-	const int s = (int)(t % S);
-	if (seg >= counts[0])
-		return;
-	const int b = seg_start[seg];
-	const size_t dv = (size_t)keys[b] * S + s;
-	const float D = dens[dv];
-	const float rn = red_num[t], rd = red_den[t], rf = red_fac[t];
-
-	if (internalized)
-	{
-		if (!counts[2])
-		{
-			// compute_fused: the voxel holds this one agent
-			const size_t k = (size_t)order[b] * S + s;
-			const float term = __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(__fsub_rn(1.f, rd), D), rn), rd), rf);
-			intern[k] = __fsub_rn(intern[k], __fmul_rn(voxel_volume, term));
-		}
-		else
-		{
-			// compute_internalized for every agent of the voxel, with its own intermediates
-			const int e = seg_start[seg + 1];
-			for (int p = b; p < e; p++)
-			{
-				const size_t k = (size_t)order[p] * S + s;
-				const float dk = den[k];
-				const float term =
-					__fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(-dk, D), num[k]), __fadd_rn(1.f, dk)), fac[k]);
-				intern[k] = __fsub_rn(intern[k], __fmul_rn(voxel_volume, term));
-			}
-		}
-	}
-	dens[dv] = __fadd_rn(__fdiv_rn(__fadd_rn(D, rn), rd), rf);
+	secrete_element(t, S, dens, counts, seg_start, order, keys, num, den, fac, red_num, red_den, red_fac, intern,
+					internalized, voxel_volume);
 }
 
 // release_internalized_substrates (:301-346): D += I*F/Vv at the agent's current voxel, I = 0
@@ -344,7 +313,7 @@ int cell_alloc(bfvm_solver* s, int count)
 	return BFVM_OK;
 }
 
-static int rebuild_bins(bfvm_solver* s)
+int rebuild_bins(bfvm_solver* s)
 {
 	agent_state& a = s->ag;
 	const int A = a.count;
@@ -355,16 +324,19 @@ static int rebuild_bins(bfvm_solver* s)
 	int st;
 
 	BFVM_CUDA(cudaMemsetAsync(a.seg_count_dev, 0, 4 * sizeof(int), s->stream));
-	agent_keys_kernel<<<(A + 255) / 256, 256, 0, s->stream>>>(a.pos, A, s->dims, bmin, vox, grid, a.keys, a.vals,
-															   invalid, s->dev_error);
+	// The sort ping-pongs between the two buffers once per pass; starting in the buffer that makes
+	// it end in keys/vals keeps those pointers fixed, so graphs and ensemble descriptors that hold
+	// them stay valid.
+	const int passes = sort_passes(s->V);
+	unsigned int* kin = (passes % 2) ? a.keys_alt : a.keys;
+	unsigned int* kout = (passes % 2) ? a.keys : a.keys_alt;
+	int* vin = (passes % 2) ? a.vals_alt : a.vals;
+	int* vout = (passes % 2) ? a.vals : a.vals_alt;
+	agent_keys_kernel<<<(A + 255) / 256, 256, 0, s->stream>>>(a.pos, A, s->dims, bmin, vox, grid, kin, vin, invalid,
+															   s->dev_error);
 	if ((st = check_launch(s, "agent_keys_kernel")))
 		return st;
 
-	unsigned int* kin = a.keys;
-	unsigned int* kout = a.keys_alt;
-	int* vin = a.vals;
-	int* vout = a.vals_alt;
-	const int passes = sort_passes(s->V);
 	const int tiles = (A + SORT_TILE - 1) / SORT_TILE;
 	for (int pass = 0; pass < passes; pass++)
 	{
@@ -379,12 +351,7 @@ static int rebuild_bins(bfvm_solver* s)
 		std::swap(kin, kout);
 		std::swap(vin, vout);
 	}
-	// keep the sorted result in keys/vals
-	if (kin != a.keys)
-	{
-		std::swap(a.keys, a.keys_alt);
-		std::swap(a.vals, a.vals_alt);
-	}
+	// the sorted result is in a.keys / a.vals now (kin == a.keys)
 
 	seg_flags_kernel<<<(A + 255) / 256, 256, 0, s->stream>>>(a.keys, A, invalid, a.flags);
 	if ((st = check_launch(s, "seg_flags_kernel")))

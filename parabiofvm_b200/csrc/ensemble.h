@@ -1,0 +1,76 @@
+// Ensemble kernels of a batch (batch_kernels.cu): one launch per phase of the step for every mesh
+// of the batch, driven by work lists, instead of one launch per phase and mesh.
+#pragma once
+
+#include <vector>
+
+#include "bfvm_internal.h"
+
+namespace bfvm {
+
+static constexpr int ENS_MAX_P = 16; // blocks of 32 per line the ensemble sweep handles
+
+// Everything a kernel needs of one mesh (device copy in ensemble_plan::inst).
+struct ens_inst
+{
+	float* dens;
+	float* grad;
+	int dims, S, X, Y, Z;
+	float bgrad[3], cgrad[3]; // gradient factors 1/h and 1/(2h) per axis (float, as the reference)
+	// sweeps: front-padded tables of each axis (precompute_padded)
+	const float* vtab[3];
+	int vP[3], pad[3];
+	// Dirichlet overwrite list
+	const long long* dir_idx;
+	const float* dir_val;
+	long long dir_count;
+	// secretion (the binning of the mesh's cell solver)
+	long long AS; // agents * S (0 without agents)
+	int internalized;
+	float voxel_volume;
+	const int* counts;
+	const int* seg_start;
+	const int* order;
+	const unsigned int* keys;
+	const float *num, *den, *fac, *red_num, *red_den, *red_fac;
+	float* intern;
+};
+
+// Per phase, a prefix list over the meshes: mesh i owns work units [first[i], first[i+1]).
+// Units are 256-element blocks (Dirichlet, gradient, secretion) or 32-line tiles (sweeps).
+enum ens_phase : int
+{
+	ENS_DIRICHLET = 0,
+	ENS_SWEEP_X = 1,
+	ENS_SWEEP_Y = 2,
+	ENS_SWEEP_Z = 3,
+	ENS_GRADIENT = 4,
+	ENS_SECRETION = 5,
+	ENS_PHASES = 6
+};
+
+struct ensemble_plan
+{
+	int count = 0;					 // meshes in the ensemble
+	ens_inst* inst = nullptr;		 // device [count]
+	long long* first[ENS_PHASES] = {}; // device [count + 1]
+	std::vector<long long> first_h[ENS_PHASES];
+	int maxP[3] = { 1, 1, 1 };		 // largest vP per axis
+	int maxS = 1;
+	size_t table_floats[3] = { 0, 0, 0 }; // largest staged table per axis
+	size_t xstage_floats = 0;			  // largest x tile (32/S rows at pitch X*S | 1)
+};
+
+// Which meshes the ensemble kernels cover: every axis with n >= 2 and at most ENS_MAX_P blocks,
+// at most 32 substrates.
+bool ensemble_eligible(const bfvm_solver* s);
+int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes);
+void ensemble_free(ensemble_plan& plan);
+// One phase for every mesh of the plan, on `stream`.  `dirichlet_phase` k applies the overwrite to
+// meshes with k <= dims (before sweep k, or after the last sweep).
+int ensemble_dirichlet(const ensemble_plan& plan, int dirichlet_phase, cudaStream_t stream);
+int ensemble_sweep(const ensemble_plan& plan, int axis, cudaStream_t stream);
+int ensemble_gradient(const ensemble_plan& plan, cudaStream_t stream);
+int ensemble_secretion(const ensemble_plan& plan, cudaStream_t stream);
+
+} // namespace bfvm

@@ -21,6 +21,7 @@
 //   x sweep ("rows"): lines are the S interleaved substrate lines of a row; thread t holds
 //     substrate s = t % Sc of block j = (t / Sc) % P of row t / (Sc*P).
 
+#include "ensemble.h"
 #include "sweep_common.cuh"
 
 namespace bfvm {
@@ -211,6 +212,14 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 	bool handled = false;
 	if (st->use_tma)
 		rc = launch_sweep_tma(st, axis, a, handled);
+	// the same front-padded block algebra without TMA staging, where the lines fit 16 blocks
+	if (!rc && !handled && st->self_plan && pl.vtab && pl.vP <= ENS_MAX_P && (axis > 0 || st->S <= 32))
+	{
+		rc = ensemble_sweep(*st->self_plan, axis, st->stream);
+		if (!rc)
+			st->launches++;
+		handled = true;
+	}
 	if (!rc && !handled)
 		rc = pl.M == 32 ? launch_sweep_m<32>(st, axis, a) : launch_sweep_m<64>(st, axis, a);
 	if (!rc && final_dirichlet)

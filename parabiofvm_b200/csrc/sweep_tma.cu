@@ -574,6 +574,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 			   + (size_t)G * 4 * sizeof(uint64_t);
 	};
 	int G = std::max(1, std::min(8, 20 / a.vP));
+	// a field of few tiles runs as more, smaller CTAs (at least 4 tiles per group over all SMs),
+	// which also leaves room on the SMs for the kernels of other meshes in a batch
+	G = (int)std::max<long long>(1, std::min<long long>(G, tt.items / (4LL * sm_count_impl(st->device))));
 	while (G > 1 && fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)
 		G--;
 	if (fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)

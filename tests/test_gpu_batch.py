@@ -1,0 +1,82 @@
+"""Batched ensembles (bfvm_batch_*): every instance of a batch must end exactly where the same
+solver stepped alone ends, bit for bit, whatever the other instances are."""
+
+import numpy as np
+import pytest
+
+from parabiofvm_b200 import Batch
+from parabiofvm_b200.workloads import make_solver, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _ensemble():
+    ws = [
+        synthetic(24, 3, 300, seed=1, clustered=True, sigma=50.0, interior_fraction=0.02),
+        synthetic(37, 5, 800, seed=2, clustered=True, sigma=80.0),
+        synthetic(50, 4, 2000, seed=3, interior_fraction=0.01),
+        synthetic(40, 2, 0, seed=4, dims=2),
+        synthetic(33, 8, 500, seed=5, clustered=True, sigma=40.0, internalized=False),
+        synthetic(64, 1, 100, seed=6),
+    ]
+    return ws
+
+
+def _state(s):
+    out = [s.load_densities().copy(), s.load_gradients().copy()]
+    if s.agents_count:
+        out.append(s.load_internalized().copy())
+    return out
+
+
+@pytest.mark.parametrize("steps,first", [(12, 0), (3, 1)])
+def test_batch_matches_each_solver_alone(steps, first):
+    ws = _ensemble()
+    alone = []
+    for w in ws:
+        s = make_solver(w)
+        s.run_steps(steps, first)
+        s.synchronize()
+        alone.append(_state(s))
+        s.close()
+    solvers = [make_solver(w) for w in ws]
+    b = Batch(solvers)
+    b.run_steps(steps, first)
+    b.synchronize()
+    for i, s in enumerate(solvers):
+        got = _state(s)
+        for g, a in zip(got, alone[i]):
+            np.testing.assert_array_equal(g, a, err_msg=f"instance {i}")
+    # a second call continues from there, with the graphs already built
+    b.run_steps(2, first + steps)
+    b.synchronize()
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+def test_batch_follows_changes_to_an_instance():
+    ws = _ensemble()[:3]
+    solvers = [make_solver(w) for w in ws]
+    ref = [make_solver(w) for w in ws]
+    b = Batch(solvers)
+    b.run_steps(2, 0)
+    # new agents on one instance (a different count: its buffers are reallocated)
+    a = synthetic(37, 5, 400, seed=9, clustered=True, sigma=80.0).agents
+    solvers[1].store_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates,
+                            a.internalized, a.fraction_released, a.volumes, a.positions)
+    b.run_steps(3, 2)
+    b.synchronize()
+    for r in ref:
+        r.run_steps(2, 0)
+    ref[1].store_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates,
+                        a.internalized, a.fraction_released, a.volumes, a.positions)
+    for r in ref:
+        r.run_steps(3, 2)
+        r.synchronize()
+    for s, r in zip(solvers, ref):
+        for g, e in zip(_state(s), _state(r)):
+            np.testing.assert_array_equal(g, e)
+    b.close()
+    for s in solvers + ref:
+        s.close()
