@@ -47,8 +47,10 @@ __global__ void __launch_bounds__(256) ens_dirichlet_kernel(const ens_inst* __re
 		if (phase > m.dims)
 			continue;
 		const long long e = (u - first[i]) * 256 + threadIdx.x;
-		if (e < m.dir_count)
-			m.dens[__ldg(&m.dir_idx[e])] = __ldg(&m.dir_val[e]);
+		if (e < m.dir_qcount)
+			*reinterpret_cast<float4*>(m.dens + __ldg(&m.dir_qidx[e])) = __ldg(&m.dir_qval[e]);
+		else if (e - m.dir_qcount < m.dir_count)
+			m.dens[__ldg(&m.dir_idx[e - m.dir_qcount])] = __ldg(&m.dir_val[e - m.dir_qcount]);
 	}
 }
 
@@ -443,6 +445,9 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
 			m.vP[d] = d < s->dims ? s->plan[d].vP : 1;
 			m.pad[d] = d < s->dims ? s->plan[d].pad : 0;
 		}
+		m.dir_qidx = s->dir_qidx;
+		m.dir_qval = s->dir_qval;
+		m.dir_qcount = s->dir_qcount;
 		m.dir_idx = s->dir_idx;
 		m.dir_val = s->dir_val;
 		m.dir_count = s->dir_count;
@@ -464,7 +469,7 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
 
 		const long long X = m.X, Y = m.Y, Z = m.Z, S = m.S, XS = X * S;
 		long long units[ENS_PHASES] = { 0, 0, 0, 0, 0, 0 };
-		units[ENS_DIRICHLET] = (m.dir_count + 255) / 256;
+		units[ENS_DIRICHLET] = (m.dir_qcount + m.dir_count + 255) / 256;
 		const long long R = 32 / S; // x tiles: rows of at most 32 substrate lines
 		units[ENS_SWEEP_X] = R > 0 ? (Y * Z + R - 1) / R : 0;
 		units[ENS_SWEEP_Y] = s->dims >= 2 ? Z * ((XS + 31) / 32) : 0;

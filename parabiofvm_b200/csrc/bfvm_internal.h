@@ -114,7 +114,11 @@ struct bfvm_solver
 	std::vector<long long> int_vids_h;		// interior voxels, ascending linear index
 	std::vector<float> int_vals_h;			// [voxel][S]
 	std::vector<unsigned char> int_conds_h; // [voxel][S]
-	long long* dir_idx = nullptr;			// element index vid * S + s
+	// ... as aligned runs of four consecutive elements (one float4 store each) and single elements
+	long long* dir_qidx = nullptr; // first element index of each run, a multiple of 4
+	float4* dir_qval = nullptr;
+	long long dir_qcount = 0;
+	long long* dir_idx = nullptr; // element index vid * S + s
 	float* dir_val = nullptr;
 	long long dir_count = 0;
 

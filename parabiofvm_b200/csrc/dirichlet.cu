@@ -3,10 +3,11 @@
 // The reference writes the boundary faces in the order x-min, x-max, y-min, y-max, z-min, z-max
 // (a later face wins on shared edges and corners) and then the interior Dirichlet voxels.  The
 // conditions change only through the set-up calls, so the host resolves that order once, when
-// they are set: the result is a list of (element index, value) pairs holding every conditioned
-// element once with the value the reference leaves there.  The overwrite is then a scatter of the
-// list, touching only the conditioned elements; it runs four times per step (before each sweep
-// and after the last).
+// they are set: the result holds every conditioned element once with the value the reference
+// leaves there, split into aligned runs of four consecutive elements (interior voxels usually
+// pin every substrate; one 16-byte store per run) and single elements.  The overwrite is then a
+// scatter of the list, touching only the conditioned elements; it runs four times per step
+// (before each sweep and after the last).
 
 #include <algorithm>
 #include <cstring>
@@ -16,28 +17,40 @@
 namespace bfvm {
 
 __global__ void __launch_bounds__(256) dirichlet_scatter_kernel(float* __restrict__ data,
+																const long long* __restrict__ qidx,
+																const float4* __restrict__ qval, long long qcount,
 																const long long* __restrict__ idx,
 																const float* __restrict__ val, long long count)
 {
-	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x)
-		data[__ldg(&idx[t])] = __ldg(&val[t]);
+	const long long n = qcount + count;
+	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+	{
+		if (t < qcount)
+			*reinterpret_cast<float4*>(data + __ldg(&qidx[t])) = __ldg(&qval[t]);
+		else
+			data[__ldg(&idx[t - qcount])] = __ldg(&val[t - qcount]);
+	}
 }
 
 int launch_dirichlet(bfvm_solver* st)
 {
-	if (st->dir_count == 0)
+	const long long n = st->dir_qcount + st->dir_count;
+	if (n == 0)
 		return BFVM_OK;
 	const int threads = 256;
-	const long long blocks = std::min<long long>((st->dir_count + threads - 1) / threads, 148LL * 16);
-	dirichlet_scatter_kernel<<<(unsigned)blocks, threads, 0, st->stream>>>(st->dens, st->dir_idx, st->dir_val,
-																			st->dir_count);
+	const long long blocks = std::min<long long>((n + threads - 1) / threads, 148LL * 16);
+	dirichlet_scatter_kernel<<<(unsigned)blocks, threads, 0, st->stream>>>(
+		st->dens, st->dir_qidx, st->dir_qval, st->dir_qcount, st->dir_idx, st->dir_val, st->dir_count);
 	return check_launch(st, "dirichlet_scatter_kernel");
 }
 
 void free_dirichlet(bfvm_solver* s)
 {
+	device_free(s->dir_qidx);
+	device_free(s->dir_qval);
 	device_free(s->dir_idx);
 	device_free(s->dir_val);
+	s->dir_qcount = 0;
 	s->dir_count = 0;
 }
 
@@ -115,18 +128,51 @@ int rebuild_dirichlet(bfvm_solver* s)
 			}
 	}
 
+	// aligned runs of four consecutive elements, and the rest one by one
+	std::vector<size_t> order(idx.size());
+	for (size_t k = 0; k < order.size(); k++)
+		order[k] = k;
+	std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return idx[a] < idx[b]; });
+	std::vector<long long> qidx, sidx;
+	std::vector<float4> qval;
+	std::vector<float> sval;
+	for (size_t k = 0; k < order.size();)
+	{
+		const long long e = idx[order[k]];
+		if (e % 4 == 0 && k + 3 < order.size() && idx[order[k + 3]] == e + 3)
+		{
+			qidx.push_back(e);
+			qval.push_back(make_float4(val[order[k]], val[order[k + 1]], val[order[k + 2]], val[order[k + 3]]));
+			k += 4;
+		}
+		else
+		{
+			sidx.push_back(e);
+			sval.push_back(val[order[k]]);
+			k++;
+		}
+	}
+
 	free_dirichlet(s);
-	if (idx.empty())
-		return BFVM_OK;
 	int st;
-	if ((st = device_alloc(&s->dir_idx, idx.size())) || (st = device_alloc(&s->dir_val, val.size())))
+	if ((st = device_alloc(&s->dir_qidx, qidx.size())) || (st = device_alloc(&s->dir_qval, qval.size()))
+		|| (st = device_alloc(&s->dir_idx, sidx.size())) || (st = device_alloc(&s->dir_val, sval.size())))
 	{
 		free_dirichlet(s);
 		return st;
 	}
-	BFVM_CUDA(cudaMemcpy(s->dir_idx, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice));
-	BFVM_CUDA(cudaMemcpy(s->dir_val, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice));
-	s->dir_count = (long long)idx.size();
+	if (!qidx.empty())
+	{
+		BFVM_CUDA(cudaMemcpy(s->dir_qidx, qidx.data(), qidx.size() * sizeof(long long), cudaMemcpyHostToDevice));
+		BFVM_CUDA(cudaMemcpy(s->dir_qval, qval.data(), qval.size() * sizeof(float4), cudaMemcpyHostToDevice));
+	}
+	if (!sidx.empty())
+	{
+		BFVM_CUDA(cudaMemcpy(s->dir_idx, sidx.data(), sidx.size() * sizeof(long long), cudaMemcpyHostToDevice));
+		BFVM_CUDA(cudaMemcpy(s->dir_val, sval.data(), sval.size() * sizeof(float), cudaMemcpyHostToDevice));
+	}
+	s->dir_qcount = (long long)qidx.size();
+	s->dir_count = (long long)sidx.size();
 	return BFVM_OK;
 }
 

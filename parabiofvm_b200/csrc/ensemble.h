@@ -21,7 +21,10 @@ struct ens_inst
 	const float* vtab[3];
 	int vP[3], pad[3];
 	// Dirichlet overwrite list
-	const long long* dir_idx;
+	const long long* dir_qidx; // runs of four (dirichlet.cu)
+	const float4* dir_qval;
+	long long dir_qcount;
+	const long long* dir_idx; // single elements
 	const float* dir_val;
 	long long dir_count;
 	// secretion (the binning of the mesh's cell solver)
