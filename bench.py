@@ -400,6 +400,7 @@ def run_ours(args):
     for opt in args.option:
         name, val = opt.split("=", 1)
         s.set_option(name, int(val))
+    tuned = s.autotune() if args.autotune else None
     VS = w.voxel_count * w.S
 
     def barrier():
@@ -564,7 +565,7 @@ def run_ours(args):
         return 0
     w_text = WORKLOADS[args.workload]["text"]
     line = {
-        "options": args.option,
+        "options": args.option + ([f"autotuned sweep shapes (groups, stages) per axis: {tuned}"] if tuned else []),
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
@@ -598,6 +599,8 @@ def main():
                     help="solver tuning option name=value (bfvm_set_option), e.g. tma_sweeps=0")
     ap.add_argument("--eager", action="store_true",
                     help="launch each step's kernels one by one instead of replaying the step's CUDA graph")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure the sweeps' launch shapes before timing (bfvm_autotune)")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)

@@ -145,6 +145,16 @@ int bfvm_synchronize(bfvm_solver* s);
  */
 int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value);
 
+/*
+ * Autotuning (no counterpart in the reference): for every axis whose sweep is staged through
+ * shared memory, time each launch shape that fits (warp groups per CTA x pipeline stages per group)
+ * on a scratch copy of the field, and keep the fastest.  The choice is also recorded for the rest
+ * of the process under the mesh shape, so solvers of the same shape use it without measuring.
+ * choices, if not NULL, receives [dims][2] = (groups, stages), (0, 0) for an axis the staged path
+ * does not take.  Results do not depend on the launch shape.  Needs one field's worth of scratch.
+ */
+int bfvm_autotune(bfvm_solver* s, int32_t* choices);
+
 /* Device pointers to the resident field and gradients, for zero-copy use by other GPU code. */
 int bfvm_device_densities(bfvm_solver* s, float** ptr, int64_t* count);
 int bfvm_device_gradients(bfvm_solver* s, float** ptr, int64_t* count);

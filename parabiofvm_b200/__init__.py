@@ -172,6 +172,13 @@ class Solver:
     def synchronize(self):
         check(self._lib.bfvm_synchronize(self._h))
 
+    def autotune(self):
+        """Measure the staged sweeps' launch shapes and keep the fastest; returns [(groups, stages)]
+        per axis ((0, 0) where the staged path does not apply)."""
+        out = (ctypes.c_int32 * 6)()
+        check(self._lib.bfvm_autotune(self._h, out))
+        return [(out[2 * d], out[2 * d + 1]) for d in range(self.dims)]
+
     def set_option(self, name, value):
         check(self._lib.bfvm_set_option(self._h, name.encode(), int(value)))
 

@@ -50,6 +50,7 @@ SIGNATURES = {
     "bfvm_run_steps": (c_int, [c_void_p, c_int32, c_int32]),
     "bfvm_synchronize": (c_int, [c_void_p]),
     "bfvm_set_option": (c_int, [c_void_p, ctypes.c_char_p, c_int64]),
+    "bfvm_autotune": (c_int, [c_void_p, P(c_int32)]),
     "bfvm_device_densities": (c_int, [c_void_p, P(P(c_float)), P(c_int64)]),
     "bfvm_device_gradients": (c_int, [c_void_p, P(P(c_float)), P(c_int64)]),
     "bfvm_launch_count": (c_int, [c_void_p, P(c_int64)]),

@@ -13,6 +13,14 @@ namespace bfvm {
 
 struct ensemble_plan;
 
+// Launch shape of the staged sweep of one axis: warp groups per CTA and pipeline stages per group
+// (0: the built-in choice).  Set by bfvm_autotune, or from its process-wide cache of shapes.
+struct sweep_tuning
+{
+	int groups = 0;
+	int stages = 0;
+};
+
 // ------------------------------------------------------------------------------------------------
 // errors
 
@@ -134,6 +142,7 @@ struct bfvm_solver
 
 	long long launches = 0;
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
+	bfvm::sweep_tuning tune[3];	 // staged sweep launch shape per axis
 
 	// graphs for run_steps: [recompute]
 	cudaGraphExec_t step_graph[2] = { nullptr, nullptr };
@@ -163,6 +172,13 @@ int check_device_errors(bfvm_solver* s);	  // waits for the stream, reports devi
 
 // sweep.cu
 int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);
+// the staged sweep of one axis alone, with launch shape `tune` (groups 0: built-in choice);
+// `handled` is false when the staged path does not take the shape
+int launch_staged_sweep(bfvm_solver* s, int axis, const sweep_tuning& tune, bool& handled);
+// launch shapes the staged sweep of `axis` can take on this mesh (empty if none)
+std::vector<sweep_tuning> staged_sweep_shapes(bfvm_solver* s, int axis);
+// autotune.cu: a tuned launch shape of an equal mesh, from the process-wide cache
+bool cached_tuning(const bfvm_solver* s, int axis, sweep_tuning& out);
 // dirichlet.cu
 int launch_dirichlet(bfvm_solver* s);
 int rebuild_dirichlet(bfvm_solver* s);

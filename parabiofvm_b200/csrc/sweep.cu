@@ -183,13 +183,8 @@ static int launch_sweep_m(bfvm_solver* st, int axis, const sweep_args& a)
 						  : (threads <= 512 ? launch_columns<M, 2, 512, 1>(st, a) : launch_columns<M, 2, 1024, 1>(st, a));
 }
 
-// One axis of the LOD step: the Dirichlet overwrite that precedes the sweep, the sweep, and after
-// the last axis the closing overwrite.
-int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
+static sweep_args make_args(bfvm_solver* st, int axis)
 {
-	int rc = launch_dirichlet(st);
-	if (rc)
-		return rc;
 	const sweep_plan& pl = st->plan[axis];
 	sweep_args a;
 	a.data = st->dens;
@@ -209,9 +204,37 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 	a.Y = st->grid[1];
 	a.Z = st->grid[2];
 	a.err = st->dev_error;
+	return a;
+}
+
+int launch_staged_sweep(bfvm_solver* st, int axis, const sweep_tuning& tune, bool& handled)
+{
+	const sweep_args a = make_args(st, axis);
+	return launch_sweep_tma(st, axis, a, handled, &tune);
+}
+
+std::vector<sweep_tuning> staged_sweep_shapes(bfvm_solver* st, int axis)
+{
+	std::vector<sweep_tuning> shapes;
+	bool handled = false;
+	const sweep_args a = make_args(st, axis);
+	if (launch_sweep_tma(st, axis, a, handled, nullptr, &shapes))
+		shapes.clear();
+	return shapes;
+}
+
+// One axis of the LOD step: the Dirichlet overwrite that precedes the sweep, the sweep, and after
+// the last axis the closing overwrite.
+int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
+{
+	int rc = launch_dirichlet(st);
+	if (rc)
+		return rc;
+	const sweep_plan& pl = st->plan[axis];
+	const sweep_args a = make_args(st, axis);
 	bool handled = false;
 	if (st->use_tma)
-		rc = launch_sweep_tma(st, axis, a, handled);
+		rc = launch_sweep_tma(st, axis, a, handled, &st->tune[axis]);
 	// the same front-padded block algebra without TMA staging, where the lines fit 16 blocks
 	if (!rc && !handled && st->self_plan && pl.vtab && pl.vP <= ENS_MAX_P && (axis > 0 || st->S <= 32))
 	{

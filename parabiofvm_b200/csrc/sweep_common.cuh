@@ -185,6 +185,7 @@ inline int set_smem(K kernel, size_t smem)
 	return BFVM_OK;
 }
 
-int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled);
+int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled,
+					 const sweep_tuning* tune = nullptr, std::vector<sweep_tuning>* shapes = nullptr);
 
 } // namespace bfvm

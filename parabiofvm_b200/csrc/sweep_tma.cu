@@ -481,7 +481,10 @@ static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtens
 	return check_launch(st, tt.axis == 0 ? "sweep_tma<x>" : (tt.axis == 1 ? "sweep_tma<y>" : "sweep_tma<z>"));
 }
 
-int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled)
+// tune: launch shape to use (groups 0: the built-in choice).  shapes: when given, nothing is
+// launched; the launch shapes that fit are listed instead.
+int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled, const sweep_tuning* tune,
+					 std::vector<sweep_tuning>* shapes)
 {
 	handled = false;
 	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2], S = st->S;
@@ -573,16 +576,34 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		return 128 + (staged_table_floats(a.vP, (int)S) + (size_t)G * 2 * a.vP * 32) * sizeof(float) + 8
 			   + (size_t)G * 4 * sizeof(uint64_t);
 	};
-	int G = std::max(1, std::min(8, 20 / a.vP));
+	const int Gmax = std::max(1, std::min(8, 20 / a.vP));
+	auto max_stages = [&](int G) { return (int)std::min<size_t>(4, ((size_t)optin - std::min((size_t)optin, fixed_bytes(G))) / ((size_t)G * stage_bytes)); };
+	if (shapes)
+	{
+		shapes->clear();
+		for (int G = 1; G <= Gmax; G++)
+			for (int n = 2; n <= max_stages(G); n++)
+				shapes->push_back({ G, n });
+		return BFVM_OK;
+	}
+	int G = Gmax;
 	// a field of few tiles runs as more, smaller CTAs (at least 4 tiles per group over all SMs),
 	// which also leaves room on the SMs for the kernels of other meshes in a batch
 	G = (int)std::max<long long>(1, std::min<long long>(G, tt.items / (4LL * sm_count_impl(st->device))));
-	while (G > 1 && fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)
+	while (G > 1 && max_stages(G) < 2)
 		G--;
-	if (fixed_bytes(G) + (size_t)G * 2 * stage_bytes > (size_t)optin)
+	if (max_stages(G) < 2)
 		return BFVM_OK;
+	int NST = max_stages(G);
+	sweep_tuning cached;
+	const sweep_tuning* want = (tune && tune->groups > 0) ? tune : (cached_tuning(st, axis, cached) ? &cached : nullptr);
+	if (want && want->groups <= Gmax && want->stages >= 2 && want->stages <= max_stages(want->groups))
+	{
+		G = want->groups;
+		NST = want->stages;
+	}
 	tt.groups = G;
-	tt.stages = (int)std::min<size_t>(4, ((size_t)optin - fixed_bytes(G)) / ((size_t)G * stage_bytes));
+	tt.stages = NST;
 	const size_t smem = fixed_bytes(G) + (size_t)G * tt.stages * stage_bytes;
 
 	handled = true;

@@ -109,6 +109,9 @@ public:
 
 	void wait_for_all();
 
+	// time the staged sweeps' launch shapes on a scratch copy of the field and keep the fastest
+	void autotune();
+
 	// `steps` steps of the reference driver's loop (diffusion, gradient, secretion with recompute
 	// every 10th step), replayed from CUDA graphs
 	void run_steps(microenvironment& m, index_t steps, index_t first_step = 0);

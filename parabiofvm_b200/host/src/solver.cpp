@@ -95,6 +95,8 @@ void solver::load_data_from_solver(microenvironment& m)
 
 void solver::wait_for_all() { check(bfvm_synchronize(require(ctx_)), "bfvm_synchronize"); }
 
+void solver::autotune() { check(bfvm_autotune(require(ctx_), nullptr), "bfvm_autotune"); }
+
 void solver::run_steps(microenvironment&, index_t steps, index_t first_step)
 {
 	check(bfvm_run_steps(require(ctx_), steps, first_step), "bfvm_run_steps");
