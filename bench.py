@@ -177,6 +177,67 @@ def physical_gpu_index(local_rank):
     return str(local_rank)
 
 
+def make_oracle_for(w, dtype):
+    import oracle
+
+    oracle.build()
+    oracle.set_threads(os.cpu_count() or 1)
+    o = oracle.Oracle(w.dims, w.bbox_min, w.bbox_max, w.voxel_shape, w.diffusion_coefficients, w.decay_rates,
+                      w.time_step, w.initial_conditions, w.compute_internalized, dtype=dtype)
+    for (dim, is_max), (vals, conds) in w.boundary.items():
+        o.set_boundary_dirichlet(dim, is_max, vals, conds)
+    if w.interior_voxels is not None:
+        o.set_interior_dirichlet(w.interior_voxels, w.interior_values, w.interior_conditions)
+    o.set_densities(w.densities)
+    if w.agents is not None:
+        a = w.agents
+        o.set_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates, a.internalized,
+                     a.fraction_released, a.volumes, a.positions)
+    o.initialize()
+    return o
+
+
+def _max_rel(a, r):
+    a = np.asarray(a, np.float64).reshape(-1)
+    r = np.asarray(r, np.float64).reshape(-1)
+    floor = max(float(np.abs(r).max()) * 1e-6, 1e-30)
+    return float((np.abs(a - r) / np.maximum(np.abs(r), floor)).max())
+
+
+def _rel_l2(a, r):
+    a = np.asarray(a, np.float64).reshape(-1)
+    r = np.asarray(r, np.float64).reshape(-1)
+    return float(np.linalg.norm(a - r) / max(np.linalg.norm(r), 1e-300))
+
+
+def parity_report(workload, steps, with_fp64):
+    """The GPU step against the oracle (FP32, and FP64 when asked) after `steps` full steps of the
+    workload from its initial state: max relative error (floor 1e-6 of max|ref|) and rel-L2."""
+    from parabiofvm_b200.workloads import make_solver
+
+    w = make_workload(workload)
+    g = make_solver(w)
+    g.run_steps(steps, 0)
+    g.synchronize()
+    got = g.load_densities().copy()
+    g.close()
+    out = {"workload": workload, "steps": steps}
+    for name, dt in (("fp32", np.float32),) + ((("fp64", np.float64),) if with_fp64 else ()):
+        o = make_oracle_for(w, dt)
+        o.run_steps(steps, 0)
+        ref = o.densities()
+        o.close()
+        out[f"max_rel_vs_{name}"] = _max_rel(got, ref)
+        out[f"rel_l2_vs_{name}"] = _rel_l2(got, ref)
+        if name == "fp64":
+            # the FP32 reference algorithm's own distance to the FP64 one, for scale
+            o32 = make_oracle_for(w, np.float32)
+            o32.run_steps(steps, 0)
+            out["rel_l2_fp32_oracle_vs_fp64"] = _rel_l2(o32.densities(), ref)
+            o32.close()
+    return out
+
+
 def cpu_oracle_rate(w, budget_s=20.0, max_steps=3):
     """Time the CPU oracle (all host threads) on the workload: voxel*substrate updates/s."""
     import oracle
@@ -558,6 +619,12 @@ def run_ours(args):
                "sample": f"{len(times)} full step(s) of the same workload on {threads} host threads "
                          f"({', '.join(f'{t:.2f}s' for t in times)})"}
 
+    parity = None
+    if rank == 0 and world == 1 and not args.skip_parity:
+        t_par = time.perf_counter()
+        parity = [parity_report(args.workload, 1, with_fp64=False), parity_report("plain-50", 100, with_fp64=True)]
+        log(f"parity checks took {time.perf_counter() - t_par:.1f}s")
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -579,6 +646,7 @@ def run_ours(args):
         "step_hbm": step_hbm,
         "kernels": kernels,
         "cpu_baseline": cpu,
+        "parity": parity,
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks,
@@ -603,6 +671,8 @@ def main():
                     help="measure the sweeps' launch shapes before timing (bfvm_autotune)")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-parity", action="store_true",
+                    help="leave out the oracle comparisons (one full-size step, 100 steps of plain-50)")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     args = ap.parse_args()
