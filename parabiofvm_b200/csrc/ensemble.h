@@ -61,7 +61,6 @@ struct ensemble_plan
 	int maxP[3] = { 1, 1, 1 };		 // largest vP per axis
 	int maxS = 1;
 	size_t table_floats[3] = { 0, 0, 0 }; // largest staged table per axis
-	size_t xstage_floats = 0;			  // largest x tile (32/S rows at pitch X*S | 1)
 };
 
 // Which meshes the ensemble kernels cover: every axis with n >= 2 and at most ENS_MAX_P blocks,
