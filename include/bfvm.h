@@ -191,6 +191,61 @@ int bfvm_batch_run_steps(bfvm_batch* b, int32_t steps, int32_t first_step);
 int bfvm_batch_synchronize(bfvm_batch* b);
 
 /*
+ * z-slabs (no counterpart in the reference, whose solvers hold a whole mesh on one device): one 3D
+ * mesh split along z into slab_count slabs, each held by its own solver, normally one per GPU.
+ * slab_planes[slab_count + 1] lists the plane boundaries, 0 = slab_planes[0] < ... <
+ * slab_planes[slab_count] = the mesh's z plane count; slab k holds planes [slab_planes[k],
+ * slab_planes[k + 1]), at least 2 and, with more than one slab, at most 512 of them, and X *
+ * substrates must then be a multiple of 4.  bfvm_create_slab takes the whole mesh as bfvm_create
+ * does (dims 3) and creates the solver of slab `slab`: its grid_shape, field, gradients and
+ * Dirichlet conditions are the slab's planes only (local z = mesh z - slab_planes[slab]; agent
+ * positions stay in mesh coordinates).  The caller gives each slab its part of the conditions (the
+ * z-min face to slab 0, the z-max face to the last) and the agents whose voxel it holds.
+ *
+ * The x and y sweeps, Dirichlet overwrites, secretion and release stay within a slab.  The z sweep
+ * and the z gradient cross slabs, so with slab_count > 1 bfvm_diffusion_solve, the z axis of
+ * bfvm_diffusion_sweep, bfvm_gradient_solve and bfvm_run_steps return BFVM_ERR_STATE, and a step
+ * of the split mesh is, on every slab in the same order:
+ *   bfvm_slab_diffusion_begin(s, mine)   Dirichlet, x sweep, Dirichlet, y sweep, Dirichlet, and the
+ *                                        reduce pass of the z sweep, writing mine [2][X*Y*S]
+ *   (the caller gathers every slab's `mine`, in slab order, into all [slab_count][2][X*Y*S])
+ *   bfvm_slab_diffusion_end(s, all)      the rest of the z sweep, closing Dirichlet overwrite
+ *   bfvm_slab_edge_planes(s, lo, hi)     copies the slab's first and last planes [Y][X][S]
+ *   (the caller hands slab k's `hi` to slab k+1 as plane_below, its `lo` to slab k-1 as plane_above)
+ *   bfvm_slab_gradient_solve(s, below, above)
+ *   bfvm_secretion_solve(s, recompute)
+ * Buffers are device memory of the slab's device; the exchanges between the calls are the caller's
+ * (an all-gather and a neighbour exchange over NCCL, or copies between solvers of one GPU), ordered
+ * on the solver's stream.  The result is the single-solver step of the whole mesh up to float
+ * rounding in the z sweep.  A solver created with slab_count 1 is an ordinary solver.
+ */
+int bfvm_create_slab(bfvm_solver** out, int device, const int32_t bounding_box_mins[3],
+                     const int32_t bounding_box_maxs[3], const int32_t voxel_shape[3], int32_t substrates,
+                     float time_step, const float* diffusion_coefficients, const float* decay_rates,
+                     int compute_internalized_substrates, int32_t slab_count, const int32_t* slab_planes, int32_t slab);
+/* slab_count, this solver's slab, its first plane in the mesh and the mesh's plane count (1, 0, 0,
+ * grid z for a solver made by bfvm_create).  Any output may be NULL. */
+int bfvm_slab_info(const bfvm_solver* s, int32_t* slab_count, int32_t* slab, int32_t* first_plane,
+                   int32_t* mesh_planes);
+int bfvm_slab_diffusion_begin(bfvm_solver* s, float* exchange);
+int bfvm_slab_diffusion_end(bfvm_solver* s, const float* exchange_all);
+/* Either output may be NULL. */
+int bfvm_slab_edge_planes(bfvm_solver* s, float* first_plane, float* last_plane);
+/* plane_below is required except on slab 0, plane_above except on the last slab. */
+int bfvm_slab_gradient_solve(bfvm_solver* s, const float* plane_below, const float* plane_above);
+/*
+ * Host only (no GPU needed): the coefficients that couple the slabs of a z line, [slab_count][3]
+ * [substrates] = (Gamma, beta, Lambda) per slab.  Slab k, solved from zero carries, yields A (its
+ * last forward-eliminated value) and B (its first solution value); with the true carries C_k
+ * (forward value before the slab) and X_k (solution after it),
+ *   C_{k+1} = A_k + Gamma_k C_k  (C_0 = 0),   X_{k-1} = B_k + beta_k C_k + Lambda_k X_k  (X_last = 0).
+ * This is what bfvm_slab_diffusion_end evaluates per line.
+ */
+int bfvm_slab_coefficients(int32_t planes, int32_t voxel_z, int32_t substrates, float time_step,
+                           const float* diffusion_coefficients, const float* decay_rates, int32_t slab_count,
+                           const int32_t* slab_planes, float* coefficients);
+
+/*
  * Secretion and uptake with recompute, for callers that cannot allocate GPU memory: code that runs
  * under a memory budget planned ahead of time, inside a host framework that owns every device
  * allocation, or while another library's stream capture forbids cudaMalloc.  No counterpart in the

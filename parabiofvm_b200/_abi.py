@@ -58,6 +58,15 @@ SIGNATURES = {
     "bfvm_batch_destroy": (c_int, [c_void_p]),
     "bfvm_batch_run_steps": (c_int, [c_void_p, c_int32, c_int32]),
     "bfvm_batch_synchronize": (c_int, [c_void_p]),
+    "bfvm_create_slab": (c_int, [P(c_void_p), c_int, P(c_int32), P(c_int32), P(c_int32), c_int32, c_float,
+                                 P(c_float), P(c_float), c_int, c_int32, P(c_int32), c_int32]),
+    "bfvm_slab_info": (c_int, [c_void_p, P(c_int32), P(c_int32), P(c_int32), P(c_int32)]),
+    "bfvm_slab_diffusion_begin": (c_int, [c_void_p, c_void_p]),
+    "bfvm_slab_diffusion_end": (c_int, [c_void_p, c_void_p]),
+    "bfvm_slab_edge_planes": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "bfvm_slab_gradient_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "bfvm_slab_coefficients": (c_int, [c_int32, c_int32, c_int32, c_float, P(c_float), P(c_float), c_int32,
+                                       P(c_int32), P(c_float)]),
     "bfvm_secretion_solve_noalloc": (c_int, [c_void_p, c_int, P(c_int32), P(c_int32), P(c_int32), c_int32, c_float,
                                              c_int32] + [c_void_p] * 8 + [c_void_p]),
 }

@@ -195,6 +195,8 @@ int bfvm_batch_create(bfvm_batch** out, int32_t count, bfvm_solver* const* solve
 			return fail(BFVM_ERR_INVALID_ARGUMENT, "null solver in the batch");
 		if (solvers[i]->device != solvers[0]->device)
 			return fail(BFVM_ERR_INVALID_ARGUMENT, "the solvers of a batch must share one device");
+		if (solvers[i]->slab_count > 1)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "a slab of a split mesh steps through bfvm_slab_*, not in a batch");
 		for (int32_t k = 0; k < i; k++)
 			if (solvers[k] == solvers[i])
 				return fail(BFVM_ERR_INVALID_ARGUMENT, "a solver appears twice in the batch");

@@ -54,7 +54,17 @@ static int upload_plan(bfvm_solver* s, int axis)
 	if (n >= 2)
 	{
 		std::vector<float> vt;
-		precompute_padded(n, s->S, bp, c, p.vP, p.pad, vt);
+		if (axis == 2 && s->slab_global_z > 0)
+		{
+			// a z-slab: the whole line's b', restricted to the slab's planes
+			std::vector<float> wbp, wep, wg, wG, wc, wgq, wGp;
+			int wP, wbl, wex;
+			precompute_axis(s->slab_global_z, s->voxel[2], s->dims, s->S, s->dt, s->D.data(), s->decay.data(), 32, wbp,
+							wep, wg, wG, wc, wgq, wGp, wP, wbl, wex);
+			precompute_padded_range(s->slab_global_z, s->slab_z0, s->slab_z0 + n, s->S, wbp, wc, p.vP, p.pad, vt);
+		}
+		else
+			precompute_padded(n, s->S, bp, c, p.vP, p.pad, vt);
 		if ((st = device_alloc(&p.vtab, vt.size())))
 			return st;
 		BFVM_CUDA(cudaMemcpy(p.vtab, vt.data(), vt.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -101,6 +111,8 @@ static void destroy_all(bfvm_solver* s)
 	}
 	device_free(s->dens);
 	device_free(s->grad);
+	device_free(s->slab_coef);
+	device_free(s->slab_carry);
 	device_free(s->dev_error);
 	if (s->host_error)
 		cudaFreeHost(s->host_error);
@@ -156,6 +168,26 @@ using namespace bfvm;
 			return cuda_fail(cudaGetLastError(), "cudaSetDevice");                                                     \
 	} while (0)
 
+// the slab a solver created by bfvm_create_slab holds
+struct slab_spec
+{
+	int count = 1, index = 0;
+	std::vector<int> bounds; // [count + 1] plane boundaries of the mesh
+};
+
+// multi-slab solvers step through bfvm_slab_*; the whole-mesh calls that cross z refuse them
+#define REFUSE_SLABS(s, what)                                                                                          \
+	do                                                                                                                 \
+	{                                                                                                                  \
+		if ((s)->slab_count > 1)                                                                                       \
+			return fail(BFVM_ERR_STATE, std::string(what) + " couples the slabs of a mesh: use bfvm_slab_*");         \
+	} while (0)
+
+static int create_solver(bfvm_solver** out, int device, int dims, const int32_t bounding_box_mins[3],
+						 const int32_t bounding_box_maxs[3], const int32_t voxel_shape[3], int32_t substrates,
+						 float time_step, const float* diffusion_coefficients, const float* decay_rates,
+						 int compute_internalized_substrates, const slab_spec* slab);
+
 extern "C" {
 
 const char* bfvm_last_error(void) { return g_last_error.c_str(); }
@@ -181,6 +213,55 @@ int bfvm_version(void) { return 10000; }
 int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_box_mins[3],
 				const int32_t bounding_box_maxs[3], const int32_t voxel_shape[3], int32_t substrates, float time_step,
 				const float* diffusion_coefficients, const float* decay_rates, int compute_internalized_substrates)
+{
+	return create_solver(out, device, dims, bounding_box_mins, bounding_box_maxs, voxel_shape, substrates, time_step,
+						 diffusion_coefficients, decay_rates, compute_internalized_substrates, nullptr);
+}
+
+int bfvm_create_slab(bfvm_solver** out, int device, const int32_t bounding_box_mins[3],
+					 const int32_t bounding_box_maxs[3], const int32_t voxel_shape[3], int32_t substrates,
+					 float time_step, const float* diffusion_coefficients, const float* decay_rates,
+					 int compute_internalized_substrates, int32_t slab_count, const int32_t* slab_planes, int32_t slab)
+{
+	g_last_error.clear();
+	if (!out)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "out is null");
+	*out = nullptr;
+	if (!bounding_box_mins || !bounding_box_maxs || !voxel_shape || !slab_planes)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "mesh and slab arrays must not be null");
+	if (voxel_shape[2] <= 0 || bounding_box_maxs[2] <= bounding_box_mins[2])
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "the mesh needs a positive z extent");
+	const int Z = (bounding_box_maxs[2] - bounding_box_mins[2] + voxel_shape[2] - 1) / voxel_shape[2];
+	if (slab_count < 1 || slab_count > 64)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab_count must be 1..64");
+	if (slab < 0 || slab >= slab_count)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab index out of range");
+	if (slab_planes[0] != 0 || slab_planes[slab_count] != Z)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab_planes must run from 0 to the mesh's " + std::to_string(Z)
+												   + " z planes");
+	for (int k = 0; k < slab_count; k++)
+		if (slab_planes[k + 1] - slab_planes[k] < 2)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "every slab needs at least 2 planes");
+	const int z0 = slab_planes[slab], z1 = slab_planes[slab + 1];
+	if (slab_count > 1 && z1 - z0 > 512)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "a slab holds at most 512 planes");
+	slab_spec spec;
+	spec.count = slab_count;
+	spec.index = slab;
+	spec.bounds.assign(slab_planes, slab_planes + slab_count + 1);
+	int32_t mins[3] = { bounding_box_mins[0], bounding_box_mins[1], bounding_box_mins[2] + z0 * voxel_shape[2] };
+	int32_t maxs[3] = { bounding_box_maxs[0], bounding_box_maxs[1],
+						z1 == Z ? bounding_box_maxs[2] : bounding_box_mins[2] + z1 * voxel_shape[2] };
+	return create_solver(out, device, 3, mins, maxs, voxel_shape, substrates, time_step, diffusion_coefficients,
+						 decay_rates, compute_internalized_substrates, &spec);
+}
+
+} // extern "C"
+
+static int create_solver(bfvm_solver** out, int device, int dims, const int32_t bounding_box_mins[3],
+						 const int32_t bounding_box_maxs[3], const int32_t voxel_shape[3], int32_t substrates,
+						 float time_step, const float* diffusion_coefficients, const float* decay_rates,
+						 int compute_internalized_substrates, const slab_spec* slab)
 {
 	g_last_error.clear();
 	if (!out)
@@ -234,6 +315,13 @@ int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_
 	s->V = (long long)grid[0] * grid[1] * grid[2];
 	s->face_vals_h.assign(6 * (size_t)substrates, 0.f);
 	s->face_conds_h.assign(6 * (size_t)substrates, 0);
+	if (slab)
+	{
+		s->slab_count = slab->count;
+		s->slab_index = slab->index;
+		s->slab_z0 = slab->bounds[slab->index];
+		s->slab_global_z = slab->bounds[slab->count];
+	}
 
 	int st = BFVM_OK;
 	do
@@ -281,6 +369,27 @@ int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_
 			st = upload_plan(s, d);
 		if (st)
 			break;
+		if (slab)
+		{
+			if (slab->count > 1 && (long long)grid[0] * substrates % 4 != 0)
+			{
+				st = fail(BFVM_ERR_INVALID_ARGUMENT, "slabs need X * substrates to be a multiple of 4");
+				break;
+			}
+			std::vector<float> bp, ep, g, G, c, gq, Gp, coef;
+			int P, bl, ex;
+			precompute_axis(s->slab_global_z, s->voxel[2], 3, s->S, s->dt, s->D.data(), s->decay.data(), 32, bp, ep, g,
+							G, c, gq, Gp, P, bl, ex);
+			slab_coefficients(s->slab_global_z, s->S, bp, c, slab->count, slab->bounds.data(), coef);
+			const size_t lines = (size_t)grid[0] * grid[1] * substrates;
+			if ((st = device_alloc(&s->slab_coef, coef.size())) || (st = device_alloc(&s->slab_carry, 2 * lines)))
+				break;
+			if (cudaMemcpy(s->slab_coef, coef.data(), coef.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+			{
+				st = cuda_fail(cudaGetLastError(), "cudaMemcpy");
+				break;
+			}
+		}
 		s->self_plan = new (std::nothrow) ensemble_plan();
 		if (!s->self_plan)
 		{
@@ -299,6 +408,8 @@ int bfvm_create(bfvm_solver** out, int device, int dims, const int32_t bounding_
 	*out = s;
 	return BFVM_OK;
 }
+
+extern "C" {
 
 int bfvm_destroy(bfvm_solver* s)
 {
@@ -532,6 +643,7 @@ int bfvm_load_internalized(bfvm_solver* s, float* host)
 int bfvm_diffusion_solve(bfvm_solver* s)
 {
 	CHECK_SOLVER(s);
+	REFUSE_SLABS(s, "bfvm_diffusion_solve");
 	return diffusion(s);
 }
 
@@ -540,6 +652,8 @@ int bfvm_diffusion_sweep(bfvm_solver* s, int axis)
 	CHECK_SOLVER(s);
 	if (axis < 0 || axis >= s->dims)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "axis must be in [0, dims)");
+	if (axis == 2)
+		REFUSE_SLABS(s, "the z sweep");
 	return launch_sweep(s, axis, axis == s->dims - 1);
 }
 
@@ -552,6 +666,7 @@ int bfvm_dirichlet_solve(bfvm_solver* s)
 int bfvm_gradient_solve(bfvm_solver* s)
 {
 	CHECK_SOLVER(s);
+	REFUSE_SLABS(s, "bfvm_gradient_solve");
 	return launch_gradient(s);
 }
 
@@ -590,6 +705,7 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
 	CHECK_SOLVER(s);
 	if (steps < 0)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "steps must not be negative");
+	REFUSE_SLABS(s, "bfvm_run_steps");
 	for (int i = 0; i < steps; i++)
 	{
 		const int rc = ((first_step + i) % 10 == 0) ? 1 : 0;

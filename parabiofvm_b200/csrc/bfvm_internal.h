@@ -153,6 +153,18 @@ struct bfvm_solver
 	// this mesh alone as an ensemble: its sweeps run the ensemble sweep kernel on shapes the TMA
 	// path does not take (built at creation, so never inside a stream capture)
 	bfvm::ensemble_plan* self_plan = nullptr;
+
+	// z-slab of a larger mesh (bfvm_create_slab): planes [slab_z0, slab_z0 + grid[2]) of a mesh of
+	// slab_global_z planes, slab slab_index of slab_count.  Its z tables are the whole line's,
+	// restricted to the slab (precompute_padded_range), and its z sweep runs as two passes around
+	// an exchange of 2 floats per z line with the other slabs.
+	int slab_count = 1;
+	int slab_index = 0;
+	int slab_z0 = 0;
+	int slab_global_z = 0;
+	float* slab_coef = nullptr;	 // device [slab_count][3][S]: Gamma, beta, Lambda of slab_coefficients
+	float* slab_carry = nullptr; // device [2][X*Y*S]: this slab's left and right carries of the step
+	int slab_phase = 0;			 // 1 between bfvm_slab_diffusion_begin and _end
 };
 
 namespace bfvm {
@@ -165,6 +177,11 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 int padded_table_floats(int P, int S);
 void precompute_padded(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int& P, int& pad,
 					   std::vector<float>& tab);
+// the tables of elements [i0, i1) of a line of n, with the responses to carries across i0 and i1
+void precompute_padded_range(int n, int i0, int i1, int S, const std::vector<float>& bp, const std::vector<float>& c,
+							 int& P, int& pad, std::vector<float>& tab);
+void slab_coefficients(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int count,
+					   const int* bounds, std::vector<float>& out);
 
 // bfvm_api.cu
 int one_step(bfvm_solver* s, bool recompute); // diffusion, gradient, secretion on the solver's stream
@@ -179,6 +196,9 @@ int launch_staged_sweep(bfvm_solver* s, int axis, const sweep_tuning& tune, bool
 std::vector<sweep_tuning> staged_sweep_shapes(bfvm_solver* s, int axis);
 // autotune.cu: a tuned launch shape of an equal mesh, from the process-wide cache
 bool cached_tuning(const bfvm_solver* s, int axis, sweep_tuning& out);
+// the z sweep of a slab solver: mode 1 (reduce) writes A and B of every z line to `out` [2][lines]
+// and leaves the field alone; mode 2 (solve) solves with the carries in s->slab_carry
+int launch_slab_z(bfvm_solver* s, int mode, float* out);
 // dirichlet.cu
 int launch_dirichlet(bfvm_solver* s);
 int rebuild_dirichlet(bfvm_solver* s);

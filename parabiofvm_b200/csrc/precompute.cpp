@@ -122,11 +122,12 @@ void precompute_axis(int n, int h, int dims, int S, float dt, const float* D, co
 // evaluated in double from the float b' and e = c b' and rounded once.
 int padded_table_floats(int P, int S) { return 3 * 32 * P * S + S + 3 * P * S; }
 
-void precompute_padded(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int& P, int& pad,
-					   std::vector<float>& tab)
+void precompute_padded_range(int n, int i0, int i1, int S, const std::vector<float>& bp, const std::vector<float>& c,
+							 int& P, int& pad, std::vector<float>& tab)
 {
-	P = (n + 31) / 32;
-	pad = 32 * P - n;
+	const int nl = i1 - i0;
+	P = (nl + 31) / 32;
+	pad = 32 * P - nl;
 	const int N = 32 * P;
 	tab.assign((size_t)padded_table_floats(P, S), 0.f);
 	float* vbp = tab.data();
@@ -137,10 +138,11 @@ void precompute_padded(int n, int S, const std::vector<float>& bp, const std::ve
 	float* Gp = tgp + (size_t)P * S;
 	for (int v = pad; v < N; v++)
 		for (int s = 0; s < S; s++)
-			vbp[(size_t)v * S + s] = bp[(size_t)(v - pad) * S + s];
+			vbp[(size_t)v * S + s] = bp[(size_t)(i0 + v - pad) * S + s];
 	for (int s = 0; s < S; s++)
 		ct[s] = c[s];
-	if (P == 1)
+	const bool left_carry = i0 > 0, right_carry = i1 < n;
+	if (P == 1 && !left_carry && !right_carry)
 		return; // a single block uses no carries
 	double gd[32];
 	for (int j = 0; j < P; j++)
@@ -149,7 +151,7 @@ void precompute_padded(int n, int S, const std::vector<float>& bp, const std::ve
 		for (int s = 0; s < S; s++)
 		{
 			const double cs = (double)c[s];
-			if (j < P - 1)
+			if (j < P - 1 || right_carry)
 			{
 				// response to the right carry: G_v = prod_{m=v}^{q} (-c b'_m)
 				double acc = 1.0;
@@ -160,13 +162,22 @@ void precompute_padded(int n, int S, const std::vector<float>& bp, const std::ve
 				}
 				Gp[(size_t)j * S + s] = (float)acc;
 			}
-			if (j > 0)
+			if (j > 0 || left_carry)
 			{
-				// forward response g_v = prod_{m=p-1}^{v-1} (-e_m), e_m = c b'_m the float product
+				// forward response g_v = prod_{m=p-1}^{v-1} (-e_m), e_m = c b'_m the float product.  In
+				// block 0 of a sub-line the carry enters at its first real element, v = pad, through
+				// e of the element before the sub-line; the virtual elements before it stay 0.
 				double acc = 1.0;
 				for (int v = p; v <= q; v++)
 				{
-					acc *= -(double)(c[s] * vbp[(size_t)(v - 1) * S + s]);
+					if (v < pad)
+					{
+						gd[v - p] = 0.0;
+						continue;
+					}
+					const float e = (j == 0 && v == pad) ? c[s] * bp[(size_t)(i0 - 1) * S + s]
+														 : c[s] * vbp[(size_t)(v - 1) * S + s];
+					acc *= -(double)e;
 					gd[v - p] = acc;
 				}
 				gq[(size_t)j * S + s] = (float)acc;
@@ -179,6 +190,62 @@ void precompute_padded(int n, int S, const std::vector<float>& bp, const std::ve
 					tgG[((size_t)v * S + s) * 2] = (float)t;
 				}
 				tgp[(size_t)j * S + s] = (float)t;
+			}
+		}
+	}
+}
+
+void precompute_padded(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int& P, int& pad,
+					   std::vector<float>& tab)
+{
+	precompute_padded_range(n, 0, n, S, bp, c, P, pad, tab);
+}
+
+// Coefficients of the system that couples the slabs of a line split at bounds[0] = 0 < bounds[1] <
+// ... < bounds[count] = n.  Slab k holds elements [i0, i1) and, solved from zero carries, yields A
+// = its last forward value d'_{i1-1} and B = its first solution x_{i0}.  With the true carries C_k
+// = d'_{i0-1} (left) and X_k = x_{i1} (right), both are linear:
+//   d'_{i1-1} = A + Gamma C_k,   x_{i0} = B + beta C_k + Lambda X_k,
+// so C_{k+1} = A_k + Gamma_k C_k from C_0 = 0, and X_{k-1} = B_k + beta_k C_k + Lambda_k X_k from
+// X_{count-1} = 0.  out[k][3][S] = (Gamma, beta, Lambda), evaluated in double from the float b' and
+// e = c b' of the whole line: Gamma = prod (-e), Lambda = prod (-c b'), and beta the Thomas solve
+// of the slab for a unit left carry.  Terms without a neighbour are 0.
+void slab_coefficients(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int count,
+					   const int* bounds, std::vector<float>& out)
+{
+	out.assign((size_t)count * 3 * S, 0.f);
+	std::vector<double> u;
+	for (int k = 0; k < count; k++)
+	{
+		const int i0 = bounds[k], i1 = bounds[k + 1];
+		for (int s = 0; s < S; s++)
+		{
+			const double cs = (double)c[s];
+			auto b = [&](int i) { return (double)bp[(size_t)i * S + s]; };
+			auto e = [&](int i) { return (double)(c[s] * bp[(size_t)i * S + s]); };
+			float* o = out.data() + (size_t)k * 3 * S;
+			if (i0 > 0)
+			{
+				// forward response of the slab to C = 1, then its backward substitution
+				u.assign((size_t)(i1 - i0), 0.0);
+				double acc = 1.0;
+				for (int i = i0; i < i1; i++)
+				{
+					acc *= -e(i - 1);
+					u[i - i0] = acc;
+				}
+				o[s] = (float)acc;
+				double t = 0.0;
+				for (int i = i1 - 1; i >= i0; i--)
+					t = (i == i1 - 1) ? u[i - i0] * b(i) : (u[i - i0] - cs * t) * b(i);
+				o[S + s] = (float)t;
+			}
+			if (i1 < n)
+			{
+				double acc = 1.0;
+				for (int i = i1 - 1; i >= i0; i--)
+					acc *= -cs * b(i);
+				o[2 * S + s] = (float)acc;
 			}
 		}
 	}

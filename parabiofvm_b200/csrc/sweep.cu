@@ -204,6 +204,9 @@ static sweep_args make_args(bfvm_solver* st, int axis)
 	a.Y = st->grid[1];
 	a.Z = st->grid[2];
 	a.err = st->dev_error;
+	a.slab_carry = nullptr;
+	a.slab_out = nullptr;
+	a.slab_lines = 0;
 	return a;
 }
 
@@ -221,6 +224,22 @@ std::vector<sweep_tuning> staged_sweep_shapes(bfvm_solver* st, int axis)
 	if (launch_sweep_tma(st, axis, a, handled, nullptr, &shapes))
 		shapes.clear();
 	return shapes;
+}
+
+int launch_slab_z(bfvm_solver* st, int mode, float* out)
+{
+	sweep_args a = make_args(st, 2);
+	a.slab_lines = (long long)st->grid[0] * st->grid[1] * st->S;
+	a.slab_carry = st->slab_carry;
+	a.slab_out = out;
+	bool handled = false;
+	int rc = BFVM_OK;
+	if (st->use_tma)
+		rc = launch_sweep_tma(st, 2, a, handled, &st->tune[2], nullptr, mode);
+	if (!rc && !handled)
+		rc = fail(BFVM_ERR_INVALID_ARGUMENT, "the z sweep of a slab needs the TMA-staged kernel: at most 512 planes "
+											 "per slab, X * substrates a multiple of 4, and the tma_sweeps option on");
+	return rc;
 }
 
 // One axis of the LOD step: the Dirichlet overwrite that precedes the sweep, the sweep, and after

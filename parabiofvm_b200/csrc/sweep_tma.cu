@@ -231,7 +231,12 @@ __device__ __forceinline__ void store_element(float* p, float v)
 		*p = v;
 }
 
-template <bool ROWS, bool NOALLOC>
+// SLAB (y/z tiles only): 0 a plain sweep; 1 the reduce pass of a z-slab, which solves from zero
+// outer carries and writes, per line, A = the forward value after the last block and B = the first
+// real solution element, but no field; 2 the solve pass of a z-slab, which enters the line with the
+// carries C (left) and X (right) of slab_carry and writes the field.  The slab passes always run the
+// carry folds, from C and X instead of zero, with the tables of precompute_padded_range.
+template <bool ROWS, bool NOALLOC, int SLAB>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt)
@@ -365,7 +370,48 @@ __global__ void __launch_bounds__(640, 1)
 		if (leader)
 			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st]);
 
-		if (P > 1)
+		if (SLAB != 0)
+		{
+			// the slab's line: column q of the y*x*s plane
+			const long long q = (w % tt.col_tiles) * 32 + lane;
+			const bool active = q < tt.ncols;
+			float C = 0.f, Xc = 0.f;
+			if (SLAB == 2 && active)
+			{
+				C = __ldg(&a.slab_carry[q]);
+				Xc = __ldg(&a.slab_carry[a.slab_lines + q]);
+			}
+			// C_k = f^{k-1}_q + gq_{k-1} C_{k-1} from C_0 = the slab's left carry
+			for (int k = 0; k < j; k++)
+				C = fmaf(__ldg(&gqtab[k * S + s]), C, carry_f[k * 32 + lane]);
+			carry_t[j * 32 + lane] = fmaf(C, __ldg(&tgptab[j * S + s]), d[0]);
+			group_sync(bar_id, gthr);
+			// X_k = x^{k+1}_p + Gp_{k+1} X_{k+1} from X_{P-1} = the slab's right carry
+			for (int k = P - 1; k > j; k--)
+				Xc = fmaf(__ldg(&Gptab[k * S + s]), Xc, carry_t[k * 32 + lane]);
+			const float2* tcol = tgtab + s * NP + p;
+#pragma unroll
+			for (int k = 0; k < M; k++)
+			{
+				const float2 r = tcol[k];
+				d[k] = fmaf(Xc, r.y, fmaf(C, r.x, d[k]));
+			}
+			if (SLAB == 1 && active)
+			{
+				if (j == P - 1)
+					a.slab_out[q] = fmaf(__ldg(&gqtab[j * S + s]), C, carry_f[j * 32 + lane]);
+				if (j == 0)
+				{
+					float first = 0.f;
+#pragma unroll
+					for (int k = 0; k < M; k++)
+						if (k == a.pad)
+							first = d[k];
+					a.slab_out[a.slab_lines + q] = first;
+				}
+			}
+		}
+		else if (P > 1)
 		{
 			// left carry C = d'_{p-1}: fold the blocks to the left, C_k = f^k_q + gq_k C_{k-1}
 			float C = 0.f;
@@ -395,6 +441,7 @@ __global__ void __launch_bounds__(640, 1)
 			}
 		}
 
+		if (SLAB != 1)
 		{
 			// recompute the line from an opaque copy of the tile index, so nothing of the load
 			// phase stays live across the solve
@@ -467,25 +514,28 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 static constexpr int TMA_MAX_P = 16;
 
-template <bool ROWS, bool NOALLOC>
+template <bool ROWS, bool NOALLOC, int SLAB = 0>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem)
 {
-	auto kernel = sweep_tma_kernel<ROWS, NOALLOC>;
+	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
 	const int threads = 32 * a.vP * tt.groups;
 	const int grid = persistent_grid(kernel, threads, smem, (tt.items + tt.groups - 1) / tt.groups, st->device);
 	kernel<<<grid, dim3(32, a.vP, tt.groups), smem, st->stream>>>(a, map, tt);
-	return check_launch(st, tt.axis == 0 ? "sweep_tma<x>" : (tt.axis == 1 ? "sweep_tma<y>" : "sweep_tma<z>"));
+	return check_launch(st, tt.axis == 0 ? "sweep_tma<x>"
+										 : (tt.axis == 1 ? "sweep_tma<y>" : (SLAB ? "sweep_tma<z slab>" : "sweep_tma<z>")));
 }
 
 // tune: launch shape to use (groups 0: the built-in choice).  shapes: when given, nothing is
 // launched; the launch shapes that fit are listed instead.
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled, const sweep_tuning* tune,
-					 std::vector<sweep_tuning>* shapes)
+					 std::vector<sweep_tuning>* shapes, int slab_mode)
 {
+	if (slab_mode && axis != 2)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab passes exist for the z sweep only");
 	handled = false;
 	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2], S = st->S;
 	const long long XS = X * S;
@@ -609,8 +659,13 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	handled = true;
 	if (axis == 0)
 		return launch_tma_variant<true, true>(st, a, map, tt, smem);
-	return axis == 1 ? launch_tma_variant<false, true>(st, a, map, tt, smem)
-					 : launch_tma_variant<false, false>(st, a, map, tt, smem);
+	if (axis == 1)
+		return launch_tma_variant<false, true>(st, a, map, tt, smem);
+	if (slab_mode == 1)
+		return launch_tma_variant<false, false, 1>(st, a, map, tt, smem);
+	if (slab_mode == 2)
+		return launch_tma_variant<false, false, 2>(st, a, map, tt, smem);
+	return launch_tma_variant<false, false>(st, a, map, tt, smem);
 }
 
 } // namespace bfvm
