@@ -24,6 +24,12 @@ one stream.
 Multi-GPU: the plain single-mesh step does not shard (its z sweep couples the whole mesh), so
 ``--gpus N`` runs N independent replicas, one per GPU (weak scaling, no collective on the data
 path); the device time is the maximum over ranks.
+
+``--workload zslab-320`` splits the plain-320 mesh along z instead (parabiofvm_b200.slabs): under
+torchrun one slab per rank, joined by an NCCL all-gather of the z sweep's line carries and a
+neighbour exchange of edge planes (strong scaling: one mesh over all ranks); in a single process
+``--slabs K`` slabs on one GPU joined by copies, which measures what the split itself costs against
+the same mesh in one solver.
 """
 
 from __future__ import annotations
@@ -273,32 +279,59 @@ def cpu_oracle_rate(w, budget_s=20.0, max_steps=3):
     return VS * len(times) / total, threads, times
 
 
+def run_reference_batch(args, threads):
+    """The reference arm of batch-256: the reference steps one mesh at a time, so the CPU port steps
+    the instances one after another, as many as fit the time budget (one warm-up step each)."""
+    ws = make_batch()
+    budget = args.reference_budget_s
+    units = 0
+    elapsed = 0.0
+    done = 0
+    for w in ws:
+        o = make_oracle_for(w, np.float32)
+        o.run_steps(1, 1)
+        t0 = time.perf_counter()
+        o.run_steps(1, 2)
+        elapsed += time.perf_counter() - t0
+        units += w.voxel_count * w.S
+        done += 1
+        o.close()
+        if elapsed > budget:
+            break
+    value = units / elapsed
+    sample = f"one step of each of the first {done} of {len(ws)} instances, one after another (budget {budget:.0f}s)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(args.gpus),
+        "steps": 1, "warmup": 1, "ms_per_step": 1e3 * elapsed * len(ws) / done, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": "batch-256: 256 independent meshes, edge U{24..96}, 1..8 substrates, 100..20,000 "
+                               "clustered agents, per-instance coefficients",
+                   "implementation": "CPU restatement of src/solver/host (OpenMP, -O3, no FP contraction)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     """The reference arm: the CPU restatement of the reference's host step on all host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    t_setup = time.perf_counter()
-    w = make_workload(args.workload)
-    log(f"reference arm: workload built in {time.perf_counter() - t_setup:.1f}s")
     import oracle
 
     oracle.build()
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    from oracle import Oracle
-
-    o = Oracle(w.dims, w.bbox_min, w.bbox_max, w.voxel_shape, w.diffusion_coefficients, w.decay_rates, w.time_step,
-               w.initial_conditions, w.compute_internalized, dtype=np.float32)
-    for (dim, is_max), (vals, conds) in w.boundary.items():
-        o.set_boundary_dirichlet(dim, is_max, vals, conds)
-    if w.interior_voxels is not None:
-        o.set_interior_dirichlet(w.interior_voxels, w.interior_values, w.interior_conditions)
-    o.set_densities(w.densities)
-    a = w.agents
-    o.set_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates, a.internalized,
-                 a.fraction_released, a.volumes, a.positions)
-    o.initialize()
+    if args.workload == "batch-256":
+        return run_reference_batch(args, threads)
+    # the reference holds a mesh in one solver: a split mesh is timed whole
+    name = "plain-320" if args.workload == "zslab-320" else args.workload
+    t_setup = time.perf_counter()
+    w = make_workload(name)
+    log(f"reference arm: workload built in {time.perf_counter() - t_setup:.1f}s")
+    o = make_oracle_for(w, np.float32)
     # warm-up steps, then as many timed steps of --steps as fit in the time budget
     t_step = None
     for i in range(args.warmup):
@@ -318,7 +351,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(args.gpus),
         "steps": timed, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / timed, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['text']}",
+        "config": {"workload": f"{args.workload}: {WORKLOADS[name]['text']}",
                    "implementation": "CPU restatement of src/solver/host (OpenMP, -O3, no FP contraction)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -433,6 +466,105 @@ def reduce_max_over_ranks(x, world, device):
 def whole_job_rate(world, units_per_rank, steps, ms):
     """Units every rank processed over the slowest rank's time: replicas do equal work."""
     return world * units_per_rank * steps / (ms / 1e3)
+
+
+def run_zslab(args):
+    """The plain-320 mesh split along z: one slab per rank (NCCL), or --slabs slabs on one GPU."""
+    import torch
+    import torch.distributed as dist
+
+    from parabiofvm_b200 import slabs as sl
+    from parabiofvm_b200.workloads import make_solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+    t_setup = time.perf_counter()
+    w = make_workload("plain-320")  # one mesh: the same seed on every rank
+    count = world if world > 1 else args.slabs
+    bounds = sl.plan_slabs(w.grid[2], count)
+    mine = [rank] if world > 1 else list(range(count))
+    stream = torch.cuda.Stream()
+    parts = [sl.make_slab(w, bounds, k, device=local_rank, stream=stream) for k in mine]
+    exchange = sl.GroupExchange() if world > 1 else sl.LocalExchange()
+    log(f"rank {rank}: slabs {mine} of {bounds} built in {time.perf_counter() - t_setup:.1f}s")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    sl.run_steps(parts, exchange, args.warmup, 0)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(physical_gpu_index(local_rank))
+    sampler.start()
+    time.sleep(1.0)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = sum(p.launch_count for p in parts)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sl.run_steps(parts, exchange, args.steps, args.warmup)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = sum(p.launch_count for p in parts) - launches0
+    ms = reduce_max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
+    VS = w.voxel_count * w.S
+    value = VS * args.steps / (ms / 1e3)
+
+    single = None
+    if world == 1:
+        # the same mesh in one solver on the same GPU, the same steps: the cost of the split, and
+        # the agreement of the two (the split z sweep rounds differently)
+        s = make_solver(w, device=local_rank)
+        s.set_stream(stream.cuda_stream)
+        s.run_steps(args.warmup, 0)
+        s.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.run_steps(args.steps, args.warmup)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms_single = a.elapsed_time(b)
+        ref = s.load_densities()
+        s.close()
+        got = np.concatenate([p.load_densities() for p in parts])
+        single = {"ms_per_step": ms_single / args.steps, "value": VS * args.steps / (ms_single / 1e3),
+                  "split_overhead": ms / ms_single,
+                  "rel_l2_vs_single": _rel_l2(got, ref), "max_rel_vs_single": _max_rel(got, ref)}
+    for p in parts:
+        p.close()
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        step_bytes = algorithmic_step_bytes(w)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"zslab-320: {WORKLOADS['plain-320']['text']}; split along z into {count} slabs "
+                                   f"at planes {bounds}" + (" (one per rank, NCCL exchanges)" if world > 1 else
+                                                            " on one GPU (exchanges as copies)"),
+                       "slabs": count, "l2": "field 17x the L2, no flush"},
+            "step_hbm": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
+                         "frac": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak, "peak_gbs": peak,
+                         "peak_kind": peak_kind},
+            "single_solver": single,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
 
 
 def run_ours(args):
@@ -661,7 +793,9 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch-256"], default="plain-320")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch-256", "zslab-320"], default="plain-320")
+    ap.add_argument("--slabs", type=int, default=2,
+                    help="zslab-320 in one process: slabs emulated on the one GPU")
     ap.add_argument("--kernel-reps", type=int, default=5)
     ap.add_argument("--option", action="append", default=[],
                     help="solver tuning option name=value (bfvm_set_option), e.g. tma_sweeps=0")
@@ -683,6 +817,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch-256":
         return run_batch(args)
+    if args.workload == "zslab-320":
+        return run_zslab(args)
     return run_ours(args)
 
 
