@@ -92,6 +92,10 @@ int bfvm_set_interior_dirichlet(bfvm_solver* s, int32_t count, const int32_t* vo
 int bfvm_store_densities(bfvm_solver* s, const float* host_densities);
 int bfvm_load_densities(bfvm_solver* s, float* host_densities);
 int bfvm_load_gradients(bfvm_solver* s, float* host_gradients);
+/* The field from / to device memory of the solver's device, ordered on its stream (no wait): for
+ * callers whose data already lives on the GPU. */
+int bfvm_store_densities_device(bfvm_solver* s, const float* device_densities);
+int bfvm_load_densities_device(bfvm_solver* s, float* device_densities);
 
 /*
  * Replace the agent set (device_context::copy_to_device, src/solver/device/CUDA/device_context.cpp:
@@ -244,6 +248,67 @@ int bfvm_slab_gradient_solve(bfvm_solver* s, const float* plane_below, const flo
 int bfvm_slab_coefficients(int32_t planes, int32_t voxel_z, int32_t substrates, float time_step,
                            const float* diffusion_coefficients, const float* decay_rates, int32_t slab_count,
                            const int32_t* slab_planes, float* coefficients);
+
+/*
+ * The learned surrogate (no counterpart in the reference): a 3D convolutional operator that
+ * advances a field of `substrates` (1..10) by 16 steps at once,
+ *   field(t + 16 dt) = field(t) + net(field(t), 16 x sources, 16 x sinks)
+ * where sources and sinks are one step's secretion terms per voxel (bfvm_sur_agent_rates).  The
+ * network: a 3x3x3 convolution to 32 channels with ReLU, 4 residual blocks of two 3x3x3 convolutions
+ * (ReLU between), a 3x3x3 projection to the substrates; bf16 weights and activations, f32
+ * accumulation on the tensor cores, f32 master weights trained with Adam on the mean squared error.
+ * The mesh needs at least 128 voxels along x.  Fields, sources, sinks, targets and predictions are
+ * device arrays [batch][voxels][substrates], f32, voxels in the field's [z][y][x] order; batch is
+ * 1..max_batch.  Parameters: bfvm_sur_parameter_count floats, layer by layer, each W[27][32 out][32
+ * in] (tap t = 9 (dz+1) + 3 (dy+1) + (dx+1)) then b[32].  Work runs on the surrogate's stream; calls
+ * that return a loss (non-NULL) or host data wait for it.
+ */
+typedef struct bfvm_surrogate bfvm_surrogate;
+int bfvm_sur_create(bfvm_surrogate** out, int device, const int32_t grid_shape[3], int32_t substrates,
+                    int32_t max_batch, uint64_t seed);
+int bfvm_sur_destroy(bfvm_surrogate* n);
+int bfvm_sur_set_stream(bfvm_surrogate* n, void* stream);
+int bfvm_sur_parameter_count(const bfvm_surrogate* n, int64_t* count);
+/* Replace the parameters (host array) and reset the optimiser; save copies them out. */
+int bfvm_sur_load(bfvm_surrogate* n, const float* parameters);
+int bfvm_sur_save(bfvm_surrogate* n, float* parameters);
+/* prediction of field(t + 16 dt) into out */
+int bfvm_sur_infer(bfvm_surrogate* n, int32_t batch, const float* field, const float* sources, const float* sinks,
+                   float* out);
+/* forward and backward: prediction, the parameters' gradients (bfvm_sur_load_gradients) and the mean
+ * squared error against target */
+int bfvm_sur_gradients(bfvm_surrogate* n, int32_t batch, const float* field, const float* sources, const float* sinks,
+                       const float* target, float* prediction, float* loss);
+int bfvm_sur_load_gradients(bfvm_surrogate* n, float* gradients);
+/* bfvm_sur_gradients, then one Adam step (beta 0.9, 0.999, eps 1e-8) */
+int bfvm_sur_train_step(bfvm_surrogate* n, int32_t batch, const float* field, const float* sources,
+                        const float* sinks, const float* target, float* prediction, float learning_rate, float* loss);
+/* wait for the stream; BFVM_ERR_TIMEOUT if a kernel's bounded wait gave up */
+int bfvm_sur_synchronize(bfvm_surrogate* n);
+/* One step's secretion terms per voxel, summed over the agents (cell_solver.cpp:63-85 of the
+ * reference): sources = sum S T dt vol / V_vox + N dt / V_vox, sinks = sum (U + S) dt vol / V_vox.
+ * Device arrays; sources and sinks [voxels][substrates] are overwritten.  Positions [agents][3]. */
+int bfvm_sur_agent_rates(const int32_t bounding_box_mins[3], const int32_t voxel_shape[3], const int32_t grid_shape[3],
+                         int32_t substrates, float time_step, int32_t agent_count, const float* secretion_rates,
+                         const float* saturation_densities, const float* uptake_rates, const float* net_export_rates,
+                         const float* volumes, const float* positions, float* sources, float* sinks,
+                         int32_t* error_flags, void* stream);
+/* field [voxels][substrates] (device) = sum of Gaussian bumps, bump_params (host) [substrates][bumps][5] =
+ * (x, y, z, width, amplitude) in voxel units; synchronous */
+int bfvm_sur_random_field(const int32_t grid_shape[3], int32_t substrates, int32_t bumps, const float* bump_params,
+                          float* field, void* stream);
+/*
+ * One convolution layer on device tensors, the kernels the network runs (exported for tests and
+ * other networks).  shape = (X, Y, Z, batch); tensors [batch][Z][Y][X][32] bf16; weights bf16
+ * [27][32 out][32 in].  out = mask(relu(conv + bias + residual)) as bf16 and/or out_f32[voxel]
+ * [:out_channels] (+ base_f32); any of bias, residual, mask, base_f32 may be NULL.  The weight
+ * gradient adds sum_v grad[v][co] input[v + off_t][ci] into weight_grad [27][32][32] (f32).
+ */
+int bfvm_sur_conv3d(const int32_t shape[4], const void* input, const void* weights, const float* bias,
+                    const void* residual, int32_t relu, const void* mask, void* out, float* out_f32,
+                    const float* base_f32, int32_t out_channels, int32_t* error_flags, void* stream);
+int bfvm_sur_conv3d_wgrad(const int32_t shape[4], const void* input, const void* grad, float* weight_grad,
+                          int32_t* error_flags, void* stream);
 
 /*
  * Secretion and uptake with recompute, for callers that cannot allocate GPU memory: code that runs

@@ -105,6 +105,17 @@ class Solver:
         check(self._lib.bfvm_load_densities(self._h, _fp(out)))
         return out
 
+    def store_densities_device(self, tensor):
+        """The field from a device tensor (float32, voxels x substrates) on the solver's stream."""
+        if tensor.numel() != self.voxel_count * self.S or not tensor.is_contiguous():
+            raise ValueError("expected a contiguous device tensor of voxels x substrates floats")
+        check(self._lib.bfvm_store_densities_device(self._h, ctypes.c_void_p(tensor.data_ptr())))
+
+    def load_densities_device(self, tensor):
+        if tensor.numel() != self.voxel_count * self.S or not tensor.is_contiguous():
+            raise ValueError("expected a contiguous device tensor of voxels x substrates floats")
+        check(self._lib.bfvm_load_densities_device(self._h, ctypes.c_void_p(tensor.data_ptr())))
+
     def load_gradients(self, out=None):
         out = np.empty(self.voxel_count * self.S * self.dims, np.float32) if out is None else out
         check(self._lib.bfvm_load_gradients(self._h, _fp(out)))

@@ -36,6 +36,8 @@ SIGNATURES = {
     "bfvm_store_densities": (c_int, [c_void_p, P(c_float)]),
     "bfvm_load_densities": (c_int, [c_void_p, P(c_float)]),
     "bfvm_load_gradients": (c_int, [c_void_p, P(c_float)]),
+    "bfvm_store_densities_device": (c_int, [c_void_p, c_void_p]),
+    "bfvm_load_densities_device": (c_int, [c_void_p, c_void_p]),
     "bfvm_store_agents": (c_int, [c_void_p, c_int32] + [P(c_float)] * 8),
     "bfvm_store_agent_positions": (c_int, [c_void_p, c_int32, P(c_float)]),
     "bfvm_load_internalized": (c_int, [c_void_p, P(c_float)]),
@@ -67,6 +69,23 @@ SIGNATURES = {
     "bfvm_slab_gradient_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
     "bfvm_slab_coefficients": (c_int, [c_int32, c_int32, c_int32, c_float, P(c_float), P(c_float), c_int32,
                                        P(c_int32), P(c_float)]),
+    "bfvm_sur_create": (c_int, [P(c_void_p), c_int, P(c_int32), c_int32, c_int32, ctypes.c_uint64]),
+    "bfvm_sur_destroy": (c_int, [c_void_p]),
+    "bfvm_sur_set_stream": (c_int, [c_void_p, c_void_p]),
+    "bfvm_sur_parameter_count": (c_int, [c_void_p, P(c_int64)]),
+    "bfvm_sur_load": (c_int, [c_void_p, P(c_float)]),
+    "bfvm_sur_save": (c_int, [c_void_p, P(c_float)]),
+    "bfvm_sur_infer": (c_int, [c_void_p, c_int32] + [c_void_p] * 4),
+    "bfvm_sur_gradients": (c_int, [c_void_p, c_int32] + [c_void_p] * 5 + [P(c_float)]),
+    "bfvm_sur_load_gradients": (c_int, [c_void_p, P(c_float)]),
+    "bfvm_sur_train_step": (c_int, [c_void_p, c_int32] + [c_void_p] * 5 + [c_float, P(c_float)]),
+    "bfvm_sur_synchronize": (c_int, [c_void_p]),
+    "bfvm_sur_agent_rates": (c_int, [P(c_int32), P(c_int32), P(c_int32), c_int32, c_float, c_int32]
+                             + [c_void_p] * 8 + [c_void_p, c_void_p]),
+    "bfvm_sur_random_field": (c_int, [P(c_int32), c_int32, c_int32, P(c_float), c_void_p, c_void_p]),
+    "bfvm_sur_conv3d": (c_int, [P(c_int32), c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_int32, c_void_p, c_void_p]),
+    "bfvm_sur_conv3d_wgrad": (c_int, [P(c_int32)] + [c_void_p] * 5),
     "bfvm_secretion_solve_noalloc": (c_int, [c_void_p, c_int, P(c_int32), P(c_int32), P(c_int32), c_int32, c_float,
                                              c_int32] + [c_void_p] * 8 + [c_void_p]),
 }

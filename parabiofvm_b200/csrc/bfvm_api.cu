@@ -558,6 +558,26 @@ int bfvm_load_densities(bfvm_solver* s, float* host)
 	return check_device_errors(s);
 }
 
+int bfvm_store_densities_device(bfvm_solver* s, const float* device_densities)
+{
+	CHECK_SOLVER(s);
+	if (!device_densities)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null device buffer");
+	BFVM_CUDA(cudaMemcpyAsync(s->dens, device_densities, (size_t)s->V * s->S * sizeof(float), cudaMemcpyDeviceToDevice,
+							  s->stream));
+	return BFVM_OK;
+}
+
+int bfvm_load_densities_device(bfvm_solver* s, float* device_densities)
+{
+	CHECK_SOLVER(s);
+	if (!device_densities)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null device buffer");
+	BFVM_CUDA(cudaMemcpyAsync(device_densities, s->dens, (size_t)s->V * s->S * sizeof(float), cudaMemcpyDeviceToDevice,
+							  s->stream));
+	return BFVM_OK;
+}
+
 int bfvm_load_gradients(bfvm_solver* s, float* host)
 {
 	CHECK_SOLVER(s);

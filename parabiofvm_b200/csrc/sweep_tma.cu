@@ -30,66 +30,10 @@
 
 #include <cstring>
 
+#include "sm100_common.cuh"
 #include "sweep_common.cuh"
 
 namespace bfvm {
-
-static constexpr long long WAIT_LIMIT_CYCLES = 4000000000LL; // about two seconds
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-				 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-	uint32_t ok;
-	asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-				 "selp.u32 %0, 1, 0, p;\n}"
-				 : "=r"(ok)
-				 : "r"(smem_addr(bar)), "r"(parity)
-				 : "memory");
-	return ok != 0;
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
-{
-	const long long t0 = clock64();
-	while (!mbar_try_wait(bar, parity))
-		if (clock64() - t0 > WAIT_LIMIT_CYCLES)
-			return false;
-	return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar)
-{
-	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-				 ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_addr(bar))
-				 : "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar)
-{
-	asm volatile(
-		"cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-		::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
-		: "memory");
-}
-
-__device__ __forceinline__ void bulk_load(float* dst, const float* src, uint32_t bytes, uint64_t* bar)
-{
-	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-				 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
-				 : "memory");
-}
 
 struct tma_tile
 {
@@ -494,7 +438,7 @@ __global__ void __launch_bounds__(640, 1)
 // ------------------------------------------------------------------------------------------------
 // host side
 
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
 	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
 	static bool tried = false;
@@ -543,7 +487,7 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	// the x sweep whole rows of at most 32 substrate lines per tile
 	if (!a.vtab || a.vP > TMA_MAX_P || XS % 4 != 0 || (axis == 0 && S > 32) || a.n < 2)
 		return BFVM_OK;
-	auto encode = encode_fn();
+	auto encode = tensor_map_encoder();
 	if (!encode)
 		return BFVM_OK;
 
