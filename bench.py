@@ -326,6 +326,11 @@ def run_reference(args):
     oracle.set_threads(threads)
     if args.workload == "batch-256":
         return run_reference_batch(args, threads)
+    if args.workload == "surrogate-128":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned surrogate; its CPU step "
+                                                              "is timed by the plain workloads' reference arm"}),
+              flush=True)
+        return 0
     # the reference holds a mesh in one solver: a split mesh is timed whole
     name = "plain-320" if args.workload == "zslab-320" else args.workload
     t_setup = time.perf_counter()
@@ -466,6 +471,229 @@ def reduce_max_over_ranks(x, world, device):
 def whole_job_rate(world, units_per_rank, steps, ms):
     """Units every rank processed over the slowest rank's time: replicas do equal work."""
     return world * units_per_rank * steps / (ms / 1e3)
+
+
+def measured_tensor_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured (cuBLAS bf16, burst)"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+SURROGATE_TEXT = ("128^3 voxels (dx 20 um) x 4 FP32 substrates; network: 3x3x3 conv to 32 channels, 4 residual "
+                  "blocks of two 3x3x3 convs, 3x3x3 projection, bf16 weights and activations, f32 accumulate; "
+                  "training pairs from the plain GPU solver (fields of 8 Gaussian bumps, 10k-100k uniform agents, "
+                  "16 steps), Adam lr 1e-3 batch 4; inference with 200,000 clustered agents, 100 macro-steps of 16 "
+                  "steps, every 8th re-run plain, plain takes over above 1e-3 relative L2")
+
+
+def run_surrogate(args):
+    """The learned surrogate at 128^3 x 4: training throughput, one convolution against the tensor
+    peak, a macro-step against 16 plain steps, and the fallback controller over 1,600 steps."""
+    import ctypes
+
+    import torch
+
+    from parabiofvm_b200 import _abi
+    from parabiofvm_b200 import surrogate as su
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(20261205)
+    S = 4
+    env = su.Microenvironment((128, 128, 128), 20, list(np.exp(rng.uniform(np.log(1e3), np.log(1e5), S))),
+                              list(rng.uniform(0.01, 1.0, S)), 0.01)
+    if args.conv_only:
+        return surrogate_conv_only(args, env)
+    B = 4
+    net = su.Surrogate(env.grid, S, max_batch=B, seed=7)
+    gen = su.PairGenerator(env, seed=11)
+    VS = env.voxels * S
+    with torch.cuda.stream(net.stream):
+        field, src, sink, target, pred = [torch.empty((B, VS), device="cuda") for _ in range(5)]
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # pairs from the plain solver
+    t0 = time.perf_counter()
+    gen.batch(field, src, sink, target)
+    torch.cuda.synchronize()
+    pair_s = (time.perf_counter() - t0) / B
+
+    # training steps on that batch (device-timed; no loss read-back inside the timed region)
+    net.stream.wait_stream(gen.stream)
+    train_steps = max(args.steps, 3)
+    for _ in range(args.warmup):
+        net.train_step(field, src, sink, target, pred, 1e-3, read_loss=False)
+    net.synchronize()
+    e0, e1 = events()
+    e0.record(net.stream)
+    for _ in range(train_steps):
+        net.train_step(field, src, sink, target, pred, 1e-3, read_loss=False)
+    e1.record(net.stream)
+    net.synchronize()
+    ms_train = e0.elapsed_time(e1) / train_steps
+    conv_flop = 2.0 * 27 * 32 * 32 * env.voxels * B
+    train_flop = conv_flop * (10 + 9 + 10)  # forward, input gradients (not of layer 0), weight gradients
+
+    # a little training on fresh pairs, so the controller below runs a network that has learned
+    losses = su.train(net, gen, steps=args.surrogate_train_steps, batch=B, learning_rate=1e-3)
+
+    # one forward convolution at batch 4: the roofline numerator
+    lib = _abi.load()
+    xin = torch.randn((B, env.voxels, 32), device="cuda").to(torch.bfloat16)
+    w = (torch.randn((27, 32, 32), device="cuda") * 0.05).to(torch.bfloat16)
+    yout = torch.empty_like(xin)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    shape = (ctypes.c_int32 * 4)(*env.grid, B)
+    stream = torch.cuda.current_stream()
+
+    def conv_once():
+        _abi.check(lib.bfvm_sur_conv3d(shape, ctypes.c_void_p(xin.data_ptr()), ctypes.c_void_p(w.data_ptr()), None, None,
+                                       0, None, ctypes.c_void_p(yout.data_ptr()), None, None, 0,
+                                       ctypes.c_void_p(err.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
+
+    for _ in range(3):
+        conv_once()
+    torch.cuda.synchronize()
+    reps = 10
+    e0, e1 = events()
+    e0.record(stream)
+    for _ in range(reps):
+        conv_once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ms_conv = e0.elapsed_time(e1) / reps
+    peak, peak_kind = measured_tensor_peak()
+    achieved = conv_flop / (ms_conv / 1e3) / 1e12
+
+    # a macro-step of the network against 16 plain steps, 200,000 clustered agents
+    agents = su.random_agents(env, np.random.default_rng(13), 200_000, clustered=True)
+    s = env.solver()
+    s.set_stream(net.stream.cuda_stream)
+    s.store_agents(agents["sec"], agents["sat"], agents["upt"], agents["nex"], np.zeros_like(agents["sec"]), None,
+                   agents["vol"], agents["pos"])
+    f1 = field[0]
+    s.store_densities_device(f1)
+    s.run_steps(16, 0)
+    s.synchronize()
+    e0, e1 = events()
+    e0.record(net.stream)
+    s.run_steps(160, 16)
+    e1.record(net.stream)
+    s.synchronize()
+    ms_plain16 = e0.elapsed_time(e1) / 10
+    s.close()
+    with torch.cuda.stream(net.stream):
+        out1 = torch.empty_like(f1)
+    for _ in range(3):
+        net.infer(f1, src[0], sink[0], out1)
+    net.synchronize()
+    e0, e1 = events()
+    e0.record(net.stream)
+    for _ in range(10):
+        net.infer(f1, src[0], sink[0], out1)
+    e1.record(net.stream)
+    net.synchronize()
+    ms_macro = e0.elapsed_time(e1) / 10
+
+    # the controller over 1,600 steps
+    run_field = f1.clone()
+    report = su.run_with_fallback(net, env, run_field, agents, macro_steps=100, check_every=8, tolerance=1e-3)
+    s = env.solver()
+    s.store_agents(agents["sec"], agents["sat"], agents["upt"], agents["nex"], np.zeros_like(agents["sec"]), None,
+                   agents["vol"], agents["pos"])
+    s.store_densities_device(f1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.run_steps(1600, 0)
+    s.synchronize()
+    plain_s = time.perf_counter() - t0
+    plain_field = torch.empty_like(f1)
+    s.load_densities_device(plain_field)
+    s.synchronize()
+    s.close()
+    net.close()
+    gen.close()
+
+    line = {
+        "metric": METRIC, "value": VS * 16 / (ms_macro / 1e3), "unit": UNIT, "n_gpus": 1, "steps": 10,
+        "warmup": 3, "ms_per_step": ms_macro, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 weights/activations, f32 accumulate", "data": "synthetic (seeded)",
+        "config": {"workload": f"surrogate-128: {SURROGATE_TEXT}", "l2": "activations 4x the L2 at batch 4"},
+        "macro_step": {"ms": ms_macro, "plain_16_steps_ms": ms_plain16, "speedup_vs_plain": ms_plain16 / ms_macro},
+        "training": {"ms_per_step_batch4": ms_train, "tflops": train_flop / (ms_train / 1e3) / 1e12,
+                     "pairs_per_s_generated": 1.0 / pair_s, "steps_on_fresh_pairs": len(losses),
+                     "loss_first": losses[0] if losses else None, "loss_last": losses[-1] if losses else None},
+        "roofline": {"bound": "tensor", "kernel": "sur_conv_kernel (forward, batch 4)", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None, "ms": ms_conv},
+        "fallback_run": {"macro_steps": report.macro_steps, "surrogate_macro_steps": report.surrogate_steps,
+                         "checks": [[m, e] for m, e in report.checks], "fell_back_at": report.fell_back_at,
+                         "seconds": report.seconds, "plain_seconds": plain_s,
+                         "speedup_vs_plain": plain_s / report.seconds,
+                         "rel_l2_vs_plain": su.rel_l2(run_field, plain_field)},
+        "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def time_sur_conv(grid, B, reps=10, wgrad=False):
+    """Device time of one convolution (or weight gradient) launch on [B][grid][32] bf16 tensors."""
+    import ctypes
+
+    import torch
+
+    from parabiofvm_b200 import _abi
+
+    lib = _abi.load()
+    V = grid[0] * grid[1] * grid[2]
+    xin = torch.randn((B, V, 32), device="cuda").to(torch.bfloat16)
+    w = (torch.randn((27, 32, 32), device="cuda") * 0.05).to(torch.bfloat16)
+    yout = torch.empty_like(xin)
+    dW = torch.zeros((27, 32, 32), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    shape = (ctypes.c_int32 * 4)(*grid, B)
+    stream = torch.cuda.current_stream()
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def once():
+        if wgrad:
+            _abi.check(lib.bfvm_sur_conv3d_wgrad(shape, p(xin), p(yout), p(dW), p(err),
+                                                 ctypes.c_void_p(stream.cuda_stream)))
+        else:
+            _abi.check(lib.bfvm_sur_conv3d(shape, p(xin), p(w), None, None, 0, None, p(yout), None, None, 0, p(err),
+                                           ctypes.c_void_p(stream.cuda_stream)))
+
+    for _ in range(3):
+        once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if int(err.item()):
+        raise RuntimeError("a surrogate kernel timed out")
+    return e0.elapsed_time(e1) / reps
+
+
+def surrogate_conv_only(args, env):
+    """The forward convolution and the weight gradient alone (profiling size: --conv-batch)."""
+    B = args.conv_batch
+    flop = 2.0 * 27 * 32 * 32 * env.voxels * B
+    peak, peak_kind = measured_tensor_peak()
+    out = {}
+    for name, wg in (("conv", False), ("wgrad", True)):
+        ms = time_sur_conv(env.grid, B, reps=args.steps, wgrad=wg)
+        out[name] = {"ms": ms, "tflops": flop / (ms / 1e3) / 1e12, "frac": flop / (ms / 1e3) / 1e12 / peak}
+    print(json.dumps({"workload": f"surrogate-128 convolutions, batch {B}", "peak_tflops": peak,
+                      "peak_kind": peak_kind, **out}), flush=True)
+    return 0
 
 
 def run_zslab(args):
@@ -793,7 +1021,13 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch-256", "zslab-320"], default="plain-320")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch-256", "zslab-320", "surrogate-128"],
+                    default="plain-320")
+    ap.add_argument("--conv-only", action="store_true",
+                    help="surrogate-128: time the convolution kernels alone (profiling)")
+    ap.add_argument("--conv-batch", type=int, default=4)
+    ap.add_argument("--surrogate-train-steps", type=int, default=100,
+                    help="surrogate-128: Adam steps on fresh pairs before the controller runs")
     ap.add_argument("--slabs", type=int, default=2,
                     help="zslab-320 in one process: slabs emulated on the one GPU")
     ap.add_argument("--kernel-reps", type=int, default=5)
@@ -819,6 +1053,8 @@ def main():
         return run_batch(args)
     if args.workload == "zslab-320":
         return run_zslab(args)
+    if args.workload == "surrogate-128":
+        return run_surrogate(args)
     return run_ours(args)
 
 

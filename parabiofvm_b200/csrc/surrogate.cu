@@ -135,11 +135,25 @@ __device__ __forceinline__ void give_up(volatile int* flag, int* err)
 // ------------------------------------------------------------------------------------------------
 // convolution (forward, and backward of the input with flipped weights)
 
-static constexpr int CONV_STAGES = 8;
-static constexpr uint32_t A_TILE_BYTES = SUR_TILE * SUR_C * 2; // 8192
+static constexpr uint32_t A_TILE_BYTES = SUR_TILE * SUR_C * 2; // 8192: 128 voxels x 32 channels
 static constexpr uint32_t W_TAP_BYTES = SUR_C * SUR_C * 2;	   // 2048
 static constexpr uint32_t W_BYTES = SUR_TAPS * W_TAP_BYTES;	   // 55296 (54 x 1024)
-static constexpr size_t CONV_SMEM = 1024 + W_BYTES + CONV_STAGES * A_TILE_BYTES + 256;
+// A stage holds the 130 voxels x0 - 1 .. x0 + 128 of one (y + dy, z + dz) row, which serve the three
+// taps dx = -1, 0, +1 as 128-row operands starting 0, 1 and 2 rows (64 bytes each) into the box.
+static constexpr int CONV_ROWS = SUR_TILE + 2;
+static constexpr uint32_t A_BOX_BYTES = CONV_ROWS * SUR_C * 2; // 8320
+static constexpr uint32_t A_STAGE_BYTES = 9216;					// rounded up to 1024
+static constexpr int CONV_PIPES = 3;  // independent pipelines per CTA, sharing the weights
+static constexpr int CONV_STAGES = 6; // stages per pipeline
+static constexpr int CONV_THREADS = 32 * (2 * CONV_PIPES + 4 * CONV_PIPES);
+// barriers per pipeline: full and empty per stage, 2 accumulator full, 2 accumulator empty, drain;
+// then the shared weight barrier, the tensor-memory address and the abort flag
+static constexpr int CONV_PIPE_BARS = 2 * CONV_STAGES + 5;
+static constexpr size_t CONV_BAR_BYTES = (CONV_PIPES * CONV_PIPE_BARS + 1) * sizeof(uint64_t) + 2 * sizeof(uint32_t);
+static constexpr size_t CONV_SMEM =
+	1024 + W_BYTES + (size_t)CONV_PIPES * CONV_STAGES * A_STAGE_BYTES + CONV_BAR_BYTES;
+static_assert(CONV_SMEM <= 227 * 1024, "convolution stages exceed the shared memory of a CTA");
+static_assert(A_BOX_BYTES <= A_STAGE_BYTES && A_STAGE_BYTES % 1024 == 0, "stage layout");
 
 __device__ __forceinline__ void decode_tile(long long tile, const conv_params& p, int& b, int& z, int& y, int& x0)
 {
@@ -188,89 +202,120 @@ __device__ __forceinline__ void store_bf16x32(__nv_bfloat16* dst, const float (&
 	}
 }
 
-__global__ void __launch_bounds__(192, 1) sur_conv_kernel(const __grid_constant__ CUtensorMap act,
-														   const __grid_constant__ CUtensorMap wmap,
-														   const __grid_constant__ conv_params p)
+// CTA = CONV_PIPES pipelines, each with its own producer thread (warp p), MMA thread (warp
+// CONV_PIPES + p), four epilogue warps, CONV_STAGES stages and two tensor-memory accumulators of
+// 32 columns; all share the 27 weight taps.  Pipeline p of CTA c takes tiles c * CONV_PIPES + p,
+// then every gridDim.x * CONV_PIPES-th tile.
+__global__ void __launch_bounds__(CONV_THREADS, 1) sur_conv_kernel(const __grid_constant__ CUtensorMap act,
+																	const __grid_constant__ CUtensorMap wmap,
+																	const __grid_constant__ conv_params p)
 {
 	extern __shared__ __align__(1024) unsigned char conv_smem[];
 	unsigned char* base =
 		reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(conv_smem) + 1023) & ~uintptr_t(1023));
-	unsigned char* wsm = base;				// 27 taps x [32 co][64 B]
-	unsigned char* asm_tiles = base + W_BYTES; // stages x [128 voxels][64 B]
-	uint64_t* bars = reinterpret_cast<uint64_t*>(asm_tiles + CONV_STAGES * A_TILE_BYTES);
-	uint64_t* full = bars;
-	uint64_t* empty = full + CONV_STAGES;
-	uint64_t* acc_full = empty + CONV_STAGES;
-	uint64_t* acc_empty = acc_full + 2;
-	uint64_t* wbar = acc_empty + 2;
-	uint64_t* drain = wbar + 1;
-	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+	unsigned char* wsm = base; // 27 taps x [32 co][64 B]
+	unsigned char* stages0 = base + W_BYTES;
+	uint64_t* bars0 = reinterpret_cast<uint64_t*>(stages0 + (size_t)CONV_PIPES * CONV_STAGES * A_STAGE_BYTES);
+	uint64_t* wbar = bars0 + CONV_PIPES * CONV_PIPE_BARS;
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(wbar + 1);
 	volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
 	const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 	if (threadIdx.x == 0)
 	{
-		for (int s = 0; s < CONV_STAGES; s++)
+		for (int q = 0; q < CONV_PIPES; q++)
 		{
-			mbar_init(full + s, 1);
-			mbar_init(empty + s, 1);
-		}
-		for (int a = 0; a < 2; a++)
-		{
-			mbar_init(acc_full + a, 1);
-			mbar_init(acc_empty + a, 128);
+			uint64_t* b = bars0 + q * CONV_PIPE_BARS;
+			for (int s = 0; s < CONV_STAGES; s++)
+			{
+				mbar_init(b + s, 1);				// full
+				mbar_init(b + CONV_STAGES + s, 1);	// empty
+			}
+			mbar_init(b + 2 * CONV_STAGES, 1);		// accumulator 0 full
+			mbar_init(b + 2 * CONV_STAGES + 1, 1);	// accumulator 1 full
+			mbar_init(b + 2 * CONV_STAGES + 2, 128); // accumulator 0 empty
+			mbar_init(b + 2 * CONV_STAGES + 3, 128); // accumulator 1 empty
+			mbar_init(b + 2 * CONV_STAGES + 4, 1);	// drain
 		}
 		mbar_init(wbar, 1);
-		mbar_init(drain, 1);
 		*abort_flag = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
-	if (warp == 1)
+	if (warp == CONV_PIPES)
 	{
-		tmem_alloc(tmem_slot, 64); // two accumulators of 32 columns
+		tmem_alloc(tmem_slot, 256); // 2 accumulators of 32 columns per pipeline (192 used)
 		tmem_relinquish();
 	}
 	tc_fence_before();
 	__syncthreads();
 	tc_fence_after();
 	const uint32_t tmem = *tmem_slot;
-	const long long my_tiles =
-		blockIdx.x < p.tiles ? (p.tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
-	if (warp == 0 && lane == 0)
+	// this thread's role and pipeline
+	int role, pipe;
+	if (warp < CONV_PIPES)
 	{
-		// producer: the weights once, then 27 shifted boxes per tile
-		mbar_expect_tx(wbar, W_BYTES);
-		for (int t = 0; t < SUR_TAPS; t++)
-			tma_load_2d(wsm + t * W_TAP_BYTES, &wmap, 0, t * SUR_C, wbar);
+		role = 0;
+		pipe = warp;
+	}
+	else if (warp < 2 * CONV_PIPES)
+	{
+		role = 1;
+		pipe = warp - CONV_PIPES;
+	}
+	else
+	{
+		role = 2;
+		pipe = (warp - 2 * CONV_PIPES) / 4;
+	}
+	uint64_t* bars = bars0 + pipe * CONV_PIPE_BARS;
+	uint64_t* full = bars;
+	uint64_t* empty = bars + CONV_STAGES;
+	uint64_t* acc_full = bars + 2 * CONV_STAGES;
+	uint64_t* acc_empty = acc_full + 2;
+	uint64_t* drain = acc_empty + 2;
+	unsigned char* stages = stages0 + (size_t)pipe * CONV_STAGES * A_STAGE_BYTES;
+	const long long first = (long long)blockIdx.x * CONV_PIPES + pipe;
+	const long long stride = (long long)gridDim.x * CONV_PIPES;
+	const long long my_tiles = first < p.tiles ? (p.tiles - first + stride - 1) / stride : 0;
+	const uint32_t acc_col = tmem + (uint32_t)(pipe * 2 * SUR_C);
+
+	if (role == 0 && lane == 0)
+	{
+		// producer: the weights once (pipeline 0), then one 130-row box per (dy, dz) of each tile
+		if (pipe == 0)
+		{
+			mbar_expect_tx(wbar, W_BYTES);
+			for (int t = 0; t < SUR_TAPS; t++)
+				tma_load_2d(wsm + t * W_TAP_BYTES, &wmap, 0, t * SUR_C, wbar);
+		}
 		long long n = 0;
 		for (long long i = 0; i < my_tiles && !aborted(abort_flag); i++)
 		{
 			int b, z, y, x0;
-			decode_tile(blockIdx.x + i * gridDim.x, p, b, z, y, x0);
-			for (int t = 0; t < SUR_TAPS; t++, n++)
+			decode_tile(first + i * stride, p, b, z, y, x0);
+			for (int r = 0; r < 9; r++, n++)
 			{
 				const int s = (int)(n % CONV_STAGES);
-				const uint32_t u = (uint32_t)(n / CONV_STAGES);
-				if (!mbar_wait(empty + s, (u & 1) ^ 1))
+				if (!mbar_wait(empty + s, (uint32_t)(((n / CONV_STAGES) & 1) ^ 1)))
 				{
 					give_up(abort_flag, p.err);
 					break;
 				}
-				int dz, dy, dx;
-				tap_offset(t, dz, dy, dx);
-				mbar_expect_tx(full + s, A_TILE_BYTES);
-				tma_load_5d(asm_tiles + s * A_TILE_BYTES, &act, 0, x0 + dx, y + dy, z + dz, b, full + s);
+				mbar_expect_tx(full + s, A_BOX_BYTES);
+				tma_load_5d(stages + s * A_STAGE_BYTES, &act, 0, x0 - 1, y + r % 3 - 1, z + r / 3 - 1, b, full + s);
 			}
 		}
 		// the copies issued last land before the CTA exits
 		for (long long k = (n > CONV_STAGES ? n - CONV_STAGES : 0); k < n; k++)
 			mbar_wait(full + k % CONV_STAGES, (uint32_t)((k / CONV_STAGES) & 1));
-		mbar_wait(wbar, 0);
+		if (pipe == 0)
+			mbar_wait(wbar, 0);
 	}
-	else if (warp == 1 && lane == 0)
+	else if (role == 1 && lane == 0)
 	{
-		// MMA issuer
+		// MMA issuer: per box, taps dx = -1, 0, +1 from rows 0, 1, 2 of the box; two K steps of 16
+		// channels (32 bytes) each
 		constexpr uint32_t idesc = idesc_bf16(SUR_TILE, SUR_C, false, false);
 		bool ok = mbar_wait(wbar, 0);
 		if (!ok)
@@ -280,15 +325,14 @@ __global__ void __launch_bounds__(192, 1) sur_conv_kernel(const __grid_constant_
 		for (long long i = 0; ok && i < my_tiles && !aborted(abort_flag); i++)
 		{
 			const int a = (int)(i & 1);
-			const uint32_t ua = (uint32_t)(i >> 1);
-			if (!mbar_wait(acc_empty + a, (ua & 1) ^ 1))
+			if (!mbar_wait(acc_empty + a, (uint32_t)(((i >> 1) & 1) ^ 1)))
 			{
 				give_up(abort_flag, p.err);
 				break;
 			}
 			tc_fence_after();
-			const uint32_t d = tmem + (uint32_t)(a * SUR_C);
-			for (int t = 0; t < SUR_TAPS; t++, n++)
+			const uint32_t d = acc_col + (uint32_t)(a * SUR_C);
+			for (int r = 0; r < 9; r++, n++)
 			{
 				const int s = (int)(n % CONV_STAGES);
 				if (!mbar_wait(full + s, (uint32_t)((n / CONV_STAGES) & 1)))
@@ -298,12 +342,16 @@ __global__ void __launch_bounds__(192, 1) sur_conv_kernel(const __grid_constant_
 					break;
 				}
 				tc_fence_after();
-				const uint32_t a_addr = smem_addr(asm_tiles + s * A_TILE_BYTES);
-				const uint32_t b_addr = smem_addr(wsm + t * W_TAP_BYTES);
+				const uint32_t a_addr = smem_addr(stages + s * A_STAGE_BYTES);
 #pragma unroll
-				for (int k = 0; k < 2; k++) // K = 32 channels as two steps of 16 (32 bytes)
-					umma_bf16(d, sw64_desc(a_addr + 32 * k, 16, 512), sw64_desc(b_addr + 32 * k, 16, 512), idesc,
-							  (t | k) != 0);
+				for (int dx = 0; dx < 3; dx++)
+				{
+					const uint32_t b_addr = smem_addr(wsm + (3 * r + dx) * W_TAP_BYTES);
+#pragma unroll
+					for (int k = 0; k < 2; k++)
+						umma_bf16(d, sw64_desc(a_addr + 64 * dx + 32 * k, 16, 512), sw64_desc(b_addr + 32 * k, 16, 512),
+								  idesc, (r | dx | k) != 0);
+				}
 				umma_commit(empty + s); // the stage is free once these MMAs have read it
 			}
 			if (ok)
@@ -313,7 +361,7 @@ __global__ void __launch_bounds__(192, 1) sur_conv_kernel(const __grid_constant_
 		umma_commit(drain);
 		mbar_wait(drain, 0);
 	}
-	else if (warp >= 2)
+	else if (role == 2)
 	{
 		// epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31, i.e. voxels x0 + 32 (w % 4) + lane
 		const int q = warp & 3;
@@ -330,12 +378,12 @@ __global__ void __launch_bounds__(192, 1) sur_conv_kernel(const __grid_constant_
 			}
 			tc_fence_after();
 			float v[32];
-			tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * SUR_C), v);
+			tmem_ld32(acc_col + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * SUR_C), v);
 			tc_fence_before();
 			mbar_arrive(acc_empty + a);
 
 			int b, z, y, x0;
-			decode_tile(blockIdx.x + i * gridDim.x, p, b, z, y, x0);
+			decode_tile(first + i * stride, p, b, z, y, x0);
 			const int x = x0 + m;
 			if (x >= p.X)
 				continue;
@@ -381,10 +429,10 @@ __global__ void __launch_bounds__(192, 1) sur_conv_kernel(const __grid_constant_
 	}
 	tc_fence_before();
 	__syncthreads();
-	if (warp == 1)
+	if (warp == CONV_PIPES)
 	{
 		tc_fence_after();
-		tmem_dealloc(tmem, 64);
+		tmem_dealloc(tmem, 256);
 	}
 }
 
@@ -398,9 +446,12 @@ __global__ void __launch_bounds__(192, 1) sur_conv_kernel(const __grid_constant_
 // voxel rows step by 64 bytes with 8-row groups 512 bytes apart.  At the end the accumulator is
 // added to dW with atomics (one per weight per CTA).
 
-static constexpr int WG_STAGES = 4;
+static constexpr int WG_STAGES = 5;
 static constexpr uint32_t WG_STAGE_BYTES = 5 * A_TILE_BYTES; // 4 input boxes + 1 gradient box
-static constexpr size_t WG_SMEM = 1024 + WG_STAGES * WG_STAGE_BYTES + 256;
+// barriers: full and empty per stage, accumulator full, drain; the tensor-memory address, the abort flag
+static constexpr size_t WG_BAR_BYTES = (2 * WG_STAGES + 2) * sizeof(uint64_t) + 2 * sizeof(uint32_t);
+static constexpr size_t WG_SMEM = 1024 + WG_STAGES * WG_STAGE_BYTES + WG_BAR_BYTES;
+static_assert(WG_SMEM <= 227 * 1024, "weight-gradient stages exceed the shared memory of a CTA");
 
 __global__ void __launch_bounds__(192, 1) sur_wgrad_kernel(const __grid_constant__ CUtensorMap act,
 															const __grid_constant__ CUtensorMap grad,
@@ -543,7 +594,7 @@ __global__ void __launch_bounds__(192, 1) sur_wgrad_kernel(const __grid_constant
 // ------------------------------------------------------------------------------------------------
 // host side
 
-static bool encode_act_map(CUtensorMap* map, const void* ptr, int X, int Y, int Z, int B)
+static bool encode_act_map(CUtensorMap* map, const void* ptr, int X, int Y, int Z, int B, int rows = SUR_TILE)
 {
 	auto encode = tensor_map_encoder();
 	if (!encode)
@@ -552,7 +603,7 @@ static bool encode_act_map(CUtensorMap* map, const void* ptr, int X, int Y, int 
 	cuuint64_t dims[5] = { (cuuint64_t)SUR_C, (cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z, (cuuint64_t)B };
 	const cuuint64_t row = SUR_C * 2;
 	cuuint64_t strides[4] = { row, row * X, row * X * Y, row * X * Y * Z };
-	cuuint32_t box[5] = { (cuuint32_t)SUR_C, (cuuint32_t)SUR_TILE, 1, 1, 1 };
+	cuuint32_t box[5] = { (cuuint32_t)SUR_C, (cuuint32_t)rows, 1, 1, 1 };
 	cuuint32_t estr[5] = { 1, 1, 1, 1, 1 };
 	return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(ptr), dims, strides, box, estr,
 				  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -591,14 +642,15 @@ int launch_sur_conv(const __nv_bfloat16* in, const __nv_bfloat16* w, conv_params
 	if ((st = sur_check_shape(p.X, p.Y, p.Z, p.B)))
 		return st;
 	CUtensorMap act, wmap;
-	if (!encode_act_map(&act, in, p.X, p.Y, p.Z, p.B) || !encode_weight_map(&wmap, w))
+	if (!encode_act_map(&act, in, p.X, p.Y, p.Z, p.B, CONV_ROWS) || !encode_weight_map(&wmap, w))
 		return fail(BFVM_ERR_CUDA, "cuTensorMapEncodeTiled failed for a surrogate tensor");
 	p.x_tiles = (p.X + SUR_TILE - 1) / SUR_TILE;
 	p.tiles = (long long)p.x_tiles * p.Y * p.Z * p.B;
 	if ((st = set_smem(sur_conv_kernel, CONV_SMEM)))
 		return st;
-	const long long grid = std::min<long long>(p.tiles, (long long)sm_count_impl(device));
-	sur_conv_kernel<<<(unsigned)std::max(1LL, grid), 192, CONV_SMEM, stream>>>(act, wmap, p);
+	const long long grid =
+		std::min<long long>((p.tiles + CONV_PIPES - 1) / CONV_PIPES, (long long)sm_count_impl(device));
+	sur_conv_kernel<<<(unsigned)std::max(1LL, grid), CONV_THREADS, CONV_SMEM, stream>>>(act, wmap, p);
 	const cudaError_t e = cudaGetLastError();
 	return e == cudaSuccess ? BFVM_OK : cuda_fail(e, "sur_conv_kernel");
 }
