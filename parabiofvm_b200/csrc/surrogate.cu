@@ -439,100 +439,121 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) sur_conv_kernel(const __grid_
 // ------------------------------------------------------------------------------------------------
 // weight gradient: dW[t][co][ci] += sum_v dY[v][co] in[v + off_t][ci]
 //
-// A CTA owns one group of 4 taps (M = 4 x 32 input channels) and a strided share of the 128-voxel
-// rows; for each row it copies the 4 shifted input boxes and the output-gradient box, and
-// accumulates M128 N32 K16 MMAs over the row's voxels.  Both operands are [voxels][32 channels]
-// boxes, i.e. MN-major with the voxels along K: A's 4 tap boxes follow one another (lbo 8192), the
-// voxel rows step by 64 bytes with 8-row groups 512 bytes apart.  At the end the accumulator is
-// added to dW with atomics (one per weight per CTA).
+// A CTA owns one (dy, dz) row of the stencil, i.e. the three taps dx = -1, 0, +1, and a strided
+// share of the 128-voxel rows of the mesh, split over WG_PIPES pipelines with their own
+// accumulators.  For each voxel row a pipeline copies the 130 input voxels x0 - 1 .. x0 + 128 of
+// row (y + dy, z + dz) and the 128 output-gradient voxels of row (y, z), and accumulates M128 N32
+// K16 MMAs over the row: M = (dx, input channel), N = output channel, K = voxel.  Both operands are
+// [voxels][32 channels] boxes read MN-major (the voxels along K, 8-row groups 512 bytes apart); the
+// three dx taps are the same box one row (64 bytes) apart, so A's 32-channel groups of M start 64
+// bytes apart (the fourth group, rows 96-127 of the accumulator, reads past the taps and is
+// dropped).  At the end every pipeline adds its accumulator to dW with one atomic per weight.
 
-static constexpr int WG_STAGES = 5;
-static constexpr uint32_t WG_STAGE_BYTES = 5 * A_TILE_BYTES; // 4 input boxes + 1 gradient box
-// barriers: full and empty per stage, accumulator full, drain; the tensor-memory address, the abort flag
-static constexpr size_t WG_BAR_BYTES = (2 * WG_STAGES + 2) * sizeof(uint64_t) + 2 * sizeof(uint32_t);
-static constexpr size_t WG_SMEM = 1024 + WG_STAGES * WG_STAGE_BYTES + WG_BAR_BYTES;
+static constexpr int WG_PIPES = 3;
+static constexpr int WG_STAGES = 4;
+static constexpr uint32_t WG_GRAD_OFFSET = A_STAGE_BYTES;					 // gradient box after the input box
+static constexpr uint32_t WG_STAGE_BYTES = A_STAGE_BYTES + A_TILE_BYTES; // 17408 (17 x 1024)
+static constexpr int WG_THREADS = 32 * (2 * WG_PIPES + 4 * WG_PIPES);
+// barriers per pipeline: full and empty per stage, accumulator full, drain; then the tensor-memory
+// address and the abort flag
+static constexpr int WG_PIPE_BARS = 2 * WG_STAGES + 2;
+static constexpr size_t WG_BAR_BYTES = WG_PIPES * WG_PIPE_BARS * sizeof(uint64_t) + 2 * sizeof(uint32_t);
+static constexpr size_t WG_SMEM = 1024 + (size_t)WG_PIPES * WG_STAGES * WG_STAGE_BYTES + WG_BAR_BYTES;
 static_assert(WG_SMEM <= 227 * 1024, "weight-gradient stages exceed the shared memory of a CTA");
+// the dropped fourth M group reads rows 3 .. 130 of the input box: still inside the stage
+static_assert((CONV_ROWS + 1) * SUR_C * 2 <= A_STAGE_BYTES, "wgrad input box overrun");
 
-__global__ void __launch_bounds__(192, 1) sur_wgrad_kernel(const __grid_constant__ CUtensorMap act,
-															const __grid_constant__ CUtensorMap grad,
-															const __grid_constant__ conv_params p, float* __restrict__ dW,
-															int row_groups)
+__global__ void __launch_bounds__(WG_THREADS, 1) sur_wgrad_kernel(const __grid_constant__ CUtensorMap act,
+																   const __grid_constant__ CUtensorMap grad,
+																   const __grid_constant__ conv_params p,
+																   float* __restrict__ dW, int shares)
 {
 	extern __shared__ __align__(1024) unsigned char wg_smem[];
 	unsigned char* base =
 		reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(wg_smem) + 1023) & ~uintptr_t(1023));
-	uint64_t* bars = reinterpret_cast<uint64_t*>(base + WG_STAGES * WG_STAGE_BYTES);
-	uint64_t* full = bars;
-	uint64_t* empty = full + WG_STAGES;
-	uint64_t* acc_full = empty + WG_STAGES;
-	uint64_t* drain = acc_full + 1;
-	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+	uint64_t* bars0 = reinterpret_cast<uint64_t*>(base + (size_t)WG_PIPES * WG_STAGES * WG_STAGE_BYTES);
+	uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars0 + WG_PIPES * WG_PIPE_BARS);
 	volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
-	const int group = blockIdx.x % 7;	   // taps 4g .. 4g+3 (27 = 6 x 4 + 3)
-	const int share = blockIdx.x / 7;	   // this CTA's share of the rows
-	const int taps = group < 6 ? 4 : 3;
+	const int row = blockIdx.x % 9; // (dy, dz) = (row % 3 - 1, row / 3 - 1): taps 3 row .. 3 row + 2
+	const int share = blockIdx.x / 9;
 	const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 	if (threadIdx.x == 0)
 	{
-		for (int s = 0; s < WG_STAGES; s++)
+		for (int q = 0; q < WG_PIPES; q++)
 		{
-			mbar_init(full + s, 1);
-			mbar_init(empty + s, 1);
+			uint64_t* b = bars0 + q * WG_PIPE_BARS;
+			for (int s = 0; s < WG_STAGES; s++)
+			{
+				mbar_init(b + s, 1);
+				mbar_init(b + WG_STAGES + s, 1);
+			}
+			mbar_init(b + 2 * WG_STAGES, 1);	 // accumulator full
+			mbar_init(b + 2 * WG_STAGES + 1, 1); // drain
 		}
-		mbar_init(acc_full, 1);
-		mbar_init(drain, 1);
 		*abort_flag = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
-	if (warp == 1)
+	if (warp == WG_PIPES)
 	{
-		tmem_alloc(tmem_slot, 32);
+		tmem_alloc(tmem_slot, 128); // 32 columns per pipeline
 		tmem_relinquish();
-	}
-	// a group of 3 taps leaves its fourth box zero in every stage (never copied); the tensor cores
-	// read it through the async proxy
-	if (taps < 4)
-	{
-		for (int s = 0; s < WG_STAGES; s++)
-			for (int k = threadIdx.x; k < (int)(A_TILE_BYTES / 16); k += blockDim.x)
-				reinterpret_cast<uint4*>(base + s * WG_STAGE_BYTES + 3 * A_TILE_BYTES)[k] = make_uint4(0, 0, 0, 0);
-		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 	}
 	tc_fence_before();
 	__syncthreads();
 	tc_fence_after();
 	const uint32_t tmem = *tmem_slot;
-	const long long rows = p.tiles; // 128-voxel rows
-	const long long my_rows = share < row_groups && share < rows ? (rows - share + row_groups - 1) / row_groups : 0;
 
-	if (warp == 0 && lane == 0)
+	int role, pipe;
+	if (warp < WG_PIPES)
+	{
+		role = 0;
+		pipe = warp;
+	}
+	else if (warp < 2 * WG_PIPES)
+	{
+		role = 1;
+		pipe = warp - WG_PIPES;
+	}
+	else
+	{
+		role = 2;
+		pipe = (warp - 2 * WG_PIPES) / 4;
+	}
+	uint64_t* bars = bars0 + pipe * WG_PIPE_BARS;
+	uint64_t* full = bars;
+	uint64_t* empty = bars + WG_STAGES;
+	uint64_t* acc_full = bars + 2 * WG_STAGES;
+	uint64_t* drain = acc_full + 1;
+	unsigned char* stages = base + (size_t)pipe * WG_STAGES * WG_STAGE_BYTES;
+	const long long first = (long long)share * WG_PIPES + pipe;
+	const long long stride = (long long)shares * WG_PIPES;
+	const long long my_rows = first < p.tiles ? (p.tiles - first + stride - 1) / stride : 0;
+	const uint32_t acc = tmem + (uint32_t)(pipe * SUR_C);
+	const int dy = row % 3 - 1, dz = row / 3 - 1;
+
+	if (role == 0 && lane == 0)
 	{
 		long long n = 0;
 		for (long long i = 0; i < my_rows && !aborted(abort_flag); i++, n++)
 		{
 			int b, z, y, x0;
-			decode_tile(share + i * row_groups, p, b, z, y, x0);
+			decode_tile(first + i * stride, p, b, z, y, x0);
 			const int s = (int)(n % WG_STAGES);
 			if (!mbar_wait(empty + s, (uint32_t)(((n / WG_STAGES) & 1) ^ 1)))
 			{
 				give_up(abort_flag, p.err);
 				break;
 			}
-			unsigned char* st = base + s * WG_STAGE_BYTES;
-			mbar_expect_tx(full + s, (uint32_t)(taps + 1) * A_TILE_BYTES);
-			for (int k = 0; k < taps; k++)
-			{
-				int dz, dy, dx;
-				tap_offset(4 * group + k, dz, dy, dx);
-				tma_load_5d(st + k * A_TILE_BYTES, &act, 0, x0 + dx, y + dy, z + dz, b, full + s);
-			}
-			tma_load_5d(st + 4 * A_TILE_BYTES, &grad, 0, x0, y, z, b, full + s);
+			unsigned char* st = stages + s * WG_STAGE_BYTES;
+			mbar_expect_tx(full + s, A_BOX_BYTES + A_TILE_BYTES);
+			tma_load_5d(st, &act, 0, x0 - 1, y + dy, z + dz, b, full + s);
+			tma_load_5d(st + WG_GRAD_OFFSET, &grad, 0, x0, y, z, b, full + s);
 		}
 		for (long long k = (n > WG_STAGES ? n - WG_STAGES : 0); k < n; k++)
 			mbar_wait(full + k % WG_STAGES, (uint32_t)((k / WG_STAGES) & 1));
 	}
-	else if (warp == 1 && lane == 0)
+	else if (role == 1 && lane == 0)
 	{
 		constexpr uint32_t idesc = idesc_bf16(SUR_TILE, SUR_C, true, true);
 		bool ok = true;
@@ -546,12 +567,12 @@ __global__ void __launch_bounds__(192, 1) sur_wgrad_kernel(const __grid_constant
 				break;
 			}
 			tc_fence_after();
-			const uint32_t a_addr = smem_addr(base + s * WG_STAGE_BYTES);
-			const uint32_t b_addr = a_addr + 4 * A_TILE_BYTES;
+			const uint32_t a_addr = smem_addr(stages + s * WG_STAGE_BYTES);
+			const uint32_t b_addr = a_addr + WG_GRAD_OFFSET;
 #pragma unroll
 			for (int k = 0; k < SUR_TILE / 16; k++) // 16 voxels (two 8-row groups, 1024 bytes) per MMA
-				umma_bf16(tmem, sw64_desc(a_addr + 1024 * k, A_TILE_BYTES, 512),
-						  sw64_desc(b_addr + 1024 * k, A_TILE_BYTES, 512), idesc, (i | k) != 0);
+				umma_bf16(acc, sw64_desc(a_addr + 1024 * k, 64, 512), sw64_desc(b_addr + 1024 * k, A_TILE_BYTES, 512),
+						  idesc, (i | k) != 0);
 			umma_commit(empty + s);
 		}
 		if (ok && my_rows > 0)
@@ -559,20 +580,20 @@ __global__ void __launch_bounds__(192, 1) sur_wgrad_kernel(const __grid_constant
 		umma_commit(drain);
 		mbar_wait(drain, 0);
 	}
-	else if (warp >= 2 && my_rows > 0)
+	else if (role == 2 && my_rows > 0)
 	{
 		const int q = warp & 3;
-		const int m = q * 32 + lane; // tap 4g + m / 32, input channel m % 32
+		const int m = q * 32 + lane; // tap 3 row + m / 32, input channel m % 32
 		if (!aborted(abort_flag))
 		{
 			if (mbar_wait(acc_full, 0))
 			{
 				tc_fence_after();
 				float v[32];
-				tmem_ld32(tmem + ((uint32_t)(q * 32) << 16), v);
-				const int t = 4 * group + m / 32, ci = m % 32;
-				if (t < SUR_TAPS)
+				tmem_ld32(acc + ((uint32_t)(q * 32) << 16), v);
+				if (m < 3 * SUR_C)
 				{
+					const int t = 3 * row + m / 32, ci = m % 32;
 #pragma unroll
 					for (int co = 0; co < 32; co++)
 						atomicAdd(&dW[((size_t)t * SUR_C + co) * SUR_C + ci], v[co]);
@@ -584,10 +605,10 @@ __global__ void __launch_bounds__(192, 1) sur_wgrad_kernel(const __grid_constant
 	}
 	tc_fence_before();
 	__syncthreads();
-	if (warp == 1)
+	if (warp == WG_PIPES)
 	{
 		tc_fence_after();
-		tmem_dealloc(tmem, 32);
+		tmem_dealloc(tmem, 128);
 	}
 }
 
@@ -662,15 +683,16 @@ int launch_sur_wgrad(const __nv_bfloat16* in, const __nv_bfloat16* grad, float* 
 	if ((st = sur_check_shape(p.X, p.Y, p.Z, p.B)))
 		return st;
 	CUtensorMap act, gmap;
-	if (!encode_act_map(&act, in, p.X, p.Y, p.Z, p.B) || !encode_act_map(&gmap, grad, p.X, p.Y, p.Z, p.B))
+	if (!encode_act_map(&act, in, p.X, p.Y, p.Z, p.B, CONV_ROWS) || !encode_act_map(&gmap, grad, p.X, p.Y, p.Z, p.B))
 		return fail(BFVM_ERR_CUDA, "cuTensorMapEncodeTiled failed for a surrogate tensor");
 	p.x_tiles = (p.X + SUR_TILE - 1) / SUR_TILE;
 	p.tiles = (long long)p.x_tiles * p.Y * p.Z * p.B;
 	if ((st = set_smem(sur_wgrad_kernel, WG_SMEM)))
 		return st;
 	const int sms = sm_count_impl(device);
-	const int row_groups = (int)std::max<long long>(1, std::min<long long>(p.tiles, std::max(1, sms / 7)));
-	sur_wgrad_kernel<<<7 * row_groups, 192, WG_SMEM, stream>>>(act, gmap, p, dW, row_groups);
+	const int shares = (int)std::max<long long>(
+		1, std::min<long long>((p.tiles + WG_PIPES - 1) / WG_PIPES, std::max(1, sms / 9)));
+	sur_wgrad_kernel<<<9 * shares, WG_THREADS, WG_SMEM, stream>>>(act, gmap, p, dW, shares);
 	const cudaError_t e = cudaGetLastError();
 	return e == cudaSuccess ? BFVM_OK : cuda_fail(e, "sur_wgrad_kernel");
 }
