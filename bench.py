@@ -949,13 +949,15 @@ def run_ours(args):
         s.store_agents(ag["secretion_rates"], ag["saturation_densities"], ag["uptake_rates"], ag["net_export_rates"],
                        ag["internalized"], ag["fraction_released"], ag["volumes"], ag["positions"])
         for k in range(args.steps):
-            s.store_agent_positions(pos_step)
+            # the agents' copies run on the solver's copy stream and overlap the step's kernels
+            s.store_agent_positions_async(pos_step)
             s.diffusion()
             s.gradient()
             s.secretion(k % 10 == 0)
-            s.load_internalized(intern_out)
+            s.load_internalized_async(intern_out)
         s.load_densities(field_out)
         s.load_gradients(grad_out)
+        s.synchronize()
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -965,7 +967,8 @@ def run_ours(args):
                "ms_total": e2e_ms,
                "what": "through the C ABI from pinned host memory: field and agents stored before the steps, "
                        "every step the agents' positions stored, diffusion, gradient and secretion called and the "
-                       "internalized substrates loaded, field and gradients loaded after the steps"}
+                       "internalized substrates loaded (the per-step copies asynchronous, overlapping the next "
+                       "step's kernels), field and gradients loaded after the steps"}
         del field_in, field_out, grad_out, intern_out, ag
 
     s.close()

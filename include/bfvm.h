@@ -114,6 +114,16 @@ int bfvm_store_agents(bfvm_solver* s, int32_t count, const float* secretion_rate
  */
 int bfvm_store_agent_positions(bfvm_solver* s, int32_t count, const float* positions);
 int bfvm_load_internalized(bfvm_solver* s, float* host_internalized);
+/*
+ * Asynchronous variants for step loops that move agent data every step (no counterpart in the
+ * reference, whose loads are synchronous).  The copy runs on a copy stream of the solver, after the
+ * work queued on the solver's stream when it is called, so it overlaps the work queued afterwards
+ * (the next step's diffusion and gradient); the next call that uses agent data (secretion, release,
+ * agent stores and loads, run_steps, batches) waits for it on the GPU.  The host buffer must stay
+ * valid, and for an overlapping copy be pinned, until bfvm_synchronize returns.
+ */
+int bfvm_store_agent_positions_async(bfvm_solver* s, int32_t count, const float* positions);
+int bfvm_load_internalized_async(bfvm_solver* s, float* host_internalized);
 
 /* One LOD diffusion-decay step with the Dirichlet overwrites between sweeps
  * (diffusion_solver::solve). */
@@ -139,7 +149,8 @@ int bfvm_release_internalized(bfvm_solver* s, int32_t index);
  */
 int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step);
 
-/* Wait for the stream (solver::wait_for_all) and report device-side errors. */
+/* Wait for the stream and the asynchronous copies (solver::wait_for_all) and report device-side
+ * errors. */
 int bfvm_synchronize(bfvm_solver* s);
 
 /*

@@ -141,6 +141,21 @@ class Solver:
         self._positions_keep = pos
         check(self._lib.bfvm_store_agent_positions(self._h, self.agents_count, _fp(pos)))
 
+    def store_agent_positions_async(self, positions):
+        """Positions through the solver's copy stream, overlapping the work queued after this call;
+        `positions` must be a float32 array that stays valid (pinned for overlap) until synchronize."""
+        pos = np.asarray(positions)
+        if pos.dtype != np.float32 or not pos.flags.c_contiguous or pos.size != self.agents_count * self.dims:
+            raise ValueError("expected a contiguous float32 array of agents x dims")
+        check(self._lib.bfvm_store_agent_positions_async(self._h, self.agents_count, _fp(pos)))
+
+    def load_internalized_async(self, out):
+        """Internalized substrates into `out` (float32, agents x substrates, pinned for overlap)
+        through the copy stream; complete after synchronize."""
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != self.agents_count * self.S:
+            raise ValueError("expected a contiguous float32 array of agents x substrates")
+        check(self._lib.bfvm_load_internalized_async(self._h, _fp(out)))
+
     def load_internalized(self, out=None):
         out = np.empty(self.agents_count * self.S, np.float32) if out is None else out
         check(self._lib.bfvm_load_internalized(self._h, _fp(out)))

@@ -41,6 +41,8 @@ SIGNATURES = {
     "bfvm_store_agents": (c_int, [c_void_p, c_int32] + [P(c_float)] * 8),
     "bfvm_store_agent_positions": (c_int, [c_void_p, c_int32, P(c_float)]),
     "bfvm_load_internalized": (c_int, [c_void_p, P(c_float)]),
+    "bfvm_store_agent_positions_async": (c_int, [c_void_p, c_int32, P(c_float)]),
+    "bfvm_load_internalized_async": (c_int, [c_void_p, P(c_float)]),
     "bfvm_diffusion_solve": (c_int, [c_void_p]),
     "bfvm_diffusion_sweep": (c_int, [c_void_p, c_int]),
     "bfvm_dirichlet_solve": (c_int, [c_void_p]),

@@ -162,6 +162,9 @@ static int batch_wait_instances(bfvm_batch* b)
 {
 	for (size_t i = 0; i < b->inst.size(); i++)
 	{
+		int st;
+		if ((st = order_after_copies(b->inst[i]))) // an instance's pending agent copies come first
+			return st;
 		BFVM_CUDA(cudaEventRecord(b->join[i], b->inst[i]->stream));
 		BFVM_CUDA(cudaStreamWaitEvent(b->stream, b->join[i], 0));
 	}

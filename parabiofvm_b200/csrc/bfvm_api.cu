@@ -114,6 +114,13 @@ static void destroy_all(bfvm_solver* s)
 	device_free(s->slab_coef);
 	device_free(s->slab_carry);
 	device_free(s->dev_error);
+	if (s->copy_stream)
+	{
+		cudaStreamSynchronize(s->copy_stream);
+		cudaStreamDestroy(s->copy_stream);
+		cudaEventDestroy(s->copy_ready);
+		cudaEventDestroy(s->copy_done);
+	}
 	if (s->host_error)
 		cudaFreeHost(s->host_error);
 	if (s->own_stream)
@@ -144,6 +151,36 @@ static int diffusion(bfvm_solver* s)
 	for (int axis = 0; axis < s->dims; axis++)
 		if ((st = launch_sweep(s, axis, axis == s->dims - 1)))
 			return st;
+	return BFVM_OK;
+}
+
+int order_after_copies(bfvm_solver* s)
+{
+	if (!s->copy_pending)
+		return BFVM_OK;
+	BFVM_CUDA(cudaStreamWaitEvent(s->stream, s->copy_done, 0));
+	s->copy_pending = false;
+	return BFVM_OK;
+}
+
+// the copy stream starts after everything queued on the solver's stream so far
+static int begin_async_copy(bfvm_solver* s)
+{
+	if (!s->copy_stream)
+	{
+		BFVM_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+		BFVM_CUDA(cudaEventCreateWithFlags(&s->copy_ready, cudaEventDisableTiming));
+		BFVM_CUDA(cudaEventCreateWithFlags(&s->copy_done, cudaEventDisableTiming));
+	}
+	BFVM_CUDA(cudaEventRecord(s->copy_ready, s->stream));
+	BFVM_CUDA(cudaStreamWaitEvent(s->copy_stream, s->copy_ready, 0));
+	return BFVM_OK;
+}
+
+static int end_async_copy(bfvm_solver* s)
+{
+	BFVM_CUDA(cudaEventRecord(s->copy_done, s->copy_stream));
+	s->copy_pending = true;
 	return BFVM_OK;
 }
 
@@ -599,6 +636,9 @@ int bfvm_store_agents(bfvm_solver* s, int32_t count, const float* secretion_rate
 		&& (!secretion_rates || !saturation_densities || !uptake_rates || !net_export_rates || !internalized_substrates
 			|| !volumes || !positions))
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "agent arrays must not be null");
+	int rc;
+	if ((rc = order_after_copies(s)))
+		return rc;
 	const bool resized = count != s->ag.count;
 	if (resized || count > s->ag.capacity)
 	{
@@ -643,9 +683,45 @@ int bfvm_store_agent_positions(bfvm_solver* s, int32_t count, const float* posit
 		return BFVM_OK;
 	if (!positions)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "null positions");
+	int rc;
+	if ((rc = order_after_copies(s)))
+		return rc;
 	BFVM_CUDA(cudaMemcpyAsync(s->ag.pos, positions, (size_t)count * s->dims * sizeof(float), cudaMemcpyHostToDevice,
 							  s->stream));
 	return BFVM_OK;
+}
+
+int bfvm_store_agent_positions_async(bfvm_solver* s, int32_t count, const float* positions)
+{
+	CHECK_SOLVER(s);
+	if (count != s->ag.count)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "count " + std::to_string(count) + " differs from the "
+												   + std::to_string(s->ag.count) + " stored agents");
+	if (count == 0)
+		return BFVM_OK;
+	if (!positions)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null positions");
+	int rc;
+	if ((rc = begin_async_copy(s)))
+		return rc;
+	BFVM_CUDA(cudaMemcpyAsync(s->ag.pos, positions, (size_t)count * s->dims * sizeof(float), cudaMemcpyHostToDevice,
+							  s->copy_stream));
+	return end_async_copy(s);
+}
+
+int bfvm_load_internalized_async(bfvm_solver* s, float* host)
+{
+	CHECK_SOLVER(s);
+	if (s->ag.count == 0)
+		return BFVM_OK;
+	if (!host)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
+	int rc;
+	if ((rc = begin_async_copy(s)))
+		return rc;
+	BFVM_CUDA(cudaMemcpyAsync(host, s->ag.intern, (size_t)s->ag.count * s->S * sizeof(float), cudaMemcpyDeviceToHost,
+							  s->copy_stream));
+	return end_async_copy(s);
 }
 
 int bfvm_load_internalized(bfvm_solver* s, float* host)
@@ -655,6 +731,9 @@ int bfvm_load_internalized(bfvm_solver* s, float* host)
 		return BFVM_OK;
 	if (!host)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
+	int rc;
+	if ((rc = order_after_copies(s)))
+		return rc;
 	BFVM_CUDA(cudaMemcpyAsync(host, s->ag.intern, (size_t)s->ag.count * s->S * sizeof(float), cudaMemcpyDeviceToHost,
 							  s->stream));
 	return check_device_errors(s);
@@ -693,6 +772,9 @@ int bfvm_gradient_solve(bfvm_solver* s)
 int bfvm_secretion_solve(bfvm_solver* s, int recompute)
 {
 	CHECK_SOLVER(s);
+	int rc;
+	if ((rc = order_after_copies(s)))
+		return rc;
 	return launch_secretion(s, recompute != 0);
 }
 
@@ -717,6 +799,9 @@ int bfvm_release_internalized(bfvm_solver* s, int32_t index)
 	CHECK_SOLVER(s);
 	if (index < 0 || index >= s->ag.count)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "agent index out of range");
+	int rc;
+	if ((rc = order_after_copies(s)))
+		return rc;
 	return launch_release(s, index);
 }
 
@@ -726,6 +811,9 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
 	if (steps < 0)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "steps must not be negative");
 	REFUSE_SLABS(s, "bfvm_run_steps");
+	int oc;
+	if ((oc = order_after_copies(s)))
+		return oc;
 	for (int i = 0; i < steps; i++)
 	{
 		const int rc = ((first_step + i) % 10 == 0) ? 1 : 0;
@@ -771,6 +859,9 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
 int bfvm_synchronize(bfvm_solver* s)
 {
 	CHECK_SOLVER(s);
+	if (s->copy_stream)
+		BFVM_CUDA(cudaStreamSynchronize(s->copy_stream));
+	s->copy_pending = false;
 	BFVM_CUDA(cudaStreamSynchronize(s->stream));
 	return check_device_errors(s);
 }

@@ -165,6 +165,13 @@ struct bfvm_solver
 	float* slab_coef = nullptr;	 // device [slab_count][3][S]: Gamma, beta, Lambda of slab_coefficients
 	float* slab_carry = nullptr; // device [2][X*Y*S]: this slab's left and right carries of the step
 	int slab_phase = 0;			 // 1 between bfvm_slab_diffusion_begin and _end
+
+	// asynchronous agent copies (bfvm_store_agent_positions_async, bfvm_load_internalized_async) run
+	// on copy_stream, each ordered after the work queued on `stream` when it was called; the next
+	// call that touches agent data makes `stream` wait for them (order_after_copies)
+	cudaStream_t copy_stream = nullptr;
+	cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
+	bool copy_pending = false;
 };
 
 namespace bfvm {
@@ -185,6 +192,7 @@ void slab_coefficients(int n, int S, const std::vector<float>& bp, const std::ve
 
 // bfvm_api.cu
 int one_step(bfvm_solver* s, bool recompute); // diffusion, gradient, secretion on the solver's stream
+int order_after_copies(bfvm_solver* s);		  // the solver's stream waits for pending asynchronous copies
 int check_device_errors(bfvm_solver* s);	  // waits for the stream, reports device-side error flags
 
 // sweep.cu
