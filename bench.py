@@ -244,6 +244,39 @@ def parity_report(workload, steps, with_fp64):
     return out
 
 
+def step_parity(workload, steps):
+    """The GPU against the FP32 and FP64 oracles, all three stepping in lockstep from the same
+    initial state (recompute every 10th step), compared after steps 1, 2, 5, 10, 20, 50, 100 (those
+    up to `steps`, and `steps`): maximum relative error (floor 1e-6 of max|ref|) and rel-L2 of the
+    densities."""
+    from parabiofvm_b200.workloads import make_solver
+
+    w = make_workload(workload)
+    g = make_solver(w)
+    o32 = make_oracle_for(w, np.float32)
+    o64 = make_oracle_for(w, np.float64)
+    checks = sorted({k for k in (1, 2, 5, 10, 20, 50, 100) if k <= steps} | {steps})
+    rows = []
+    t0 = time.perf_counter()
+    for k in range(steps):
+        g.run_steps(1, k)
+        o32.run_steps(1, k)
+        o64.run_steps(1, k)
+        if k + 1 not in checks:
+            continue
+        got = g.load_densities()
+        r32, r64 = o32.densities(), o64.densities()
+        rows.append({"step": k + 1, "max_rel_vs_fp32": _max_rel(got, r32), "rel_l2_vs_fp32": _rel_l2(got, r32),
+                     "max_rel_vs_fp64": _max_rel(got, r64), "rel_l2_vs_fp64": _rel_l2(got, r64),
+                     "rel_l2_fp32_oracle_vs_fp64": _rel_l2(r32, r64)})
+        log(f"step {k + 1}: max rel vs fp32 {rows[-1]['max_rel_vs_fp32']:.3e}, "
+            f"vs fp64 {rows[-1]['max_rel_vs_fp64']:.3e} ({time.perf_counter() - t0:.0f}s)")
+    g.close()
+    o32.close()
+    o64.close()
+    return {"workload": workload, "steps": steps, "checks": rows}
+
+
 def cpu_oracle_rate(w, budget_s=20.0, max_steps=3):
     """Time the CPU oracle (all host threads) on the workload: voxel*substrate updates/s."""
     import oracle
@@ -1026,6 +1059,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch-256", "zslab-320", "surrogate-128"],
                     default="plain-320")
+    ap.add_argument("--parity-steps", type=int, default=0,
+                    help="only compare the GPU with the FP32 and FP64 oracles over this many steps")
     ap.add_argument("--conv-only", action="store_true",
                     help="surrogate-128: time the convolution kernels alone (profiling)")
     ap.add_argument("--conv-batch", type=int, default=4)
@@ -1052,6 +1087,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.parity_steps:
+        print(json.dumps(step_parity(args.workload, args.parity_steps)), flush=True)
+        return 0
     if args.workload == "batch-256":
         return run_batch(args)
     if args.workload == "zslab-320":
