@@ -54,23 +54,46 @@ __global__ void __launch_bounds__(256) ens_dirichlet_kernel(const ens_inst* __re
 	}
 }
 
-__device__ __forceinline__ float ens_axis_grad(const float* __restrict__ u, long long i, int pos, int n,
-											   long long stride, float border, float center)
-{
-	if (n == 1)
-		return 0.f;
-	if (pos == 0)
-		return __fmul_rn(__fsub_rn(__ldg(&u[i + stride]), __ldg(&u[i])), border);
-	if (pos == n - 1)
-		return __fmul_rn(__fsub_rn(__ldg(&u[i]), __ldg(&u[i - stride])), border);
-	return __fmul_rn(__fsub_rn(__ldg(&u[i + stride]), __ldg(&u[i - stride])), center);
-}
-
 // central differences (gradient.cu); output layouts 1D [x][s][1], 2D [y][x][s][2], 3D [3][z][y][x][s].
 // One unit is 256 consecutive columns of the (y, x, s) plane over up to ENS_GRAD_ZC planes: each
 // thread marches z keeping u(z-1), u(z), u(z+1) in registers (gradient3d_vec4_kernel of gradient.cu
-// for any S), reading x and y neighbours from L1/L2.
+// for any S), reading x and y neighbours from L1/L2.  A thread's x and y never change along z, so
+// the one-sided or central form of each axis is fixed once as two neighbour offsets and a factor;
+// z advances ENS_GRAD_ZU planes at a time with every load of those planes issued before their
+// arithmetic, which keeps enough loads in flight for small meshes to stream at HBM rate.
 static constexpr int ENS_GRAD_ZC = 32;
+static constexpr int ENS_GRAD_ZU = 4;
+
+// neighbour offsets lo, hi and factor of an axis at position pos of n: (u[1] - u[0]) / h at the
+// first voxel, (u[n-1] - u[n-2]) / h at the last, (u[i+1] - u[i-1]) / (2h) inside; an axis of one
+// voxel reads nothing past it (its gradient is 0, set by the caller)
+__device__ __forceinline__ void axis_form(int pos, int n, long long stride, float border, float center, long long& lo,
+										  long long& hi, float& f)
+{
+	if (n == 1)
+	{
+		lo = hi = 0;
+		f = 0.f;
+	}
+	else if (pos == 0)
+	{
+		lo = 0;
+		hi = stride;
+		f = border;
+	}
+	else if (pos == n - 1)
+	{
+		lo = -stride;
+		hi = 0;
+		f = border;
+	}
+	else
+	{
+		lo = -stride;
+		hi = stride;
+		f = center;
+	}
+}
 
 __global__ void __launch_bounds__(256) ens_gradient_kernel(const ens_inst* __restrict__ inst,
 															const long long* __restrict__ first, int count,
@@ -99,41 +122,67 @@ __global__ void __launch_bounds__(256) ens_gradient_kernel(const ens_inst* __res
 		const long long plane = (long long)Y * XS;
 		const long long total = plane * Z;
 		const long long row = (long long)y * XS + q;
+		long long xlo, xhi, ylo = 0, yhi = 0;
+		float fx, fy = 0.f;
+		axis_form(x, X, S, m.bgrad[0], m.cgrad[0], xlo, xhi, fx);
+		if (dims >= 2)
+			axis_form(y, Y, XS, m.bgrad[1], m.cgrad[1], ylo, yhi, fy);
 		float prev = z0 > 0 ? __ldg(&d[(long long)(z0 - 1) * plane + row]) : 0.f;
 		float cur = __ldg(&d[(long long)z0 * plane + row]);
-		for (int z = z0; z < z1; z++)
+		for (int z = z0; z < z1; z += ENS_GRAD_ZU)
 		{
-			const long long e = (long long)z * plane + row;
-			const float next = z + 1 < Z ? __ldg(&d[e + plane]) : cur;
-			const float gx = ens_axis_grad(d, e, x, X, S, m.bgrad[0], m.cgrad[0]);
-			if (dims == 1)
-				g[e] = gx;
-			else
+			// every load of these planes first
+			float nx[ENS_GRAD_ZU], xa[ENS_GRAD_ZU], xb[ENS_GRAD_ZU], ya[ENS_GRAD_ZU], yb[ENS_GRAD_ZU];
+#pragma unroll
+			for (int k = 0; k < ENS_GRAD_ZU; k++)
 			{
-				const float gy = ens_axis_grad(d, e, y, Y, XS, m.bgrad[1], m.cgrad[1]);
-				if (dims == 2)
-				{
-					g[2 * e] = gx;
-					g[2 * e + 1] = gy;
-				}
+				const int zz = z + k;
+				const long long e = (long long)zz * plane + row;
+				const bool in = zz < z1;
+				nx[k] = (in && zz + 1 < Z) ? __ldg(&d[e + plane]) : 0.f;
+				xa[k] = in ? __ldg(&d[e + xhi]) : 0.f;
+				xb[k] = in ? __ldg(&d[e + xlo]) : 0.f;
+				ya[k] = (in && dims >= 2) ? __ldg(&d[e + yhi]) : 0.f;
+				yb[k] = (in && dims >= 2) ? __ldg(&d[e + ylo]) : 0.f;
+			}
+#pragma unroll
+			for (int k = 0; k < ENS_GRAD_ZU; k++)
+			{
+				const int zz = z + k;
+				if (zz >= z1)
+					break;
+				const long long e = (long long)zz * plane + row;
+				const float next = zz + 1 < Z ? nx[k] : cur;
+				const float gx = X == 1 ? 0.f : __fmul_rn(__fsub_rn(xa[k], xb[k]), fx);
+				if (dims == 1)
+					g[e] = gx;
 				else
 				{
-					float gz;
-					if (Z == 1)
-						gz = 0.f;
-					else if (z == 0)
-						gz = __fmul_rn(__fsub_rn(next, cur), m.bgrad[2]);
-					else if (z == Z - 1)
-						gz = __fmul_rn(__fsub_rn(cur, prev), m.bgrad[2]);
+					const float gy = Y == 1 ? 0.f : __fmul_rn(__fsub_rn(ya[k], yb[k]), fy);
+					if (dims == 2)
+					{
+						g[2 * e] = gx;
+						g[2 * e + 1] = gy;
+					}
 					else
-						gz = __fmul_rn(__fsub_rn(next, prev), m.cgrad[2]);
-					__stcs(&g[e], gx);
-					__stcs(&g[total + e], gy);
-					__stcs(&g[2 * total + e], gz);
+					{
+						float gz;
+						if (Z == 1)
+							gz = 0.f;
+						else if (zz == 0)
+							gz = __fmul_rn(__fsub_rn(next, cur), m.bgrad[2]);
+						else if (zz == Z - 1)
+							gz = __fmul_rn(__fsub_rn(cur, prev), m.bgrad[2]);
+						else
+							gz = __fmul_rn(__fsub_rn(next, prev), m.cgrad[2]);
+						__stcs(&g[e], gx);
+						__stcs(&g[total + e], gy);
+						__stcs(&g[2 * total + e], gz);
+					}
 				}
+				prev = cur;
+				cur = next;
 			}
-			prev = cur;
-			cur = next;
 		}
 	}
 }

@@ -18,6 +18,7 @@ def _ensemble():
         synthetic(40, 2, 0, seed=4, dims=2),
         synthetic(33, 8, 500, seed=5, clustered=True, sigma=40.0, internalized=False),
         synthetic(64, 1, 100, seed=6),
+        synthetic(48, 3, 0, seed=7, dims=1),
     ]
     return ws
 
