@@ -61,8 +61,8 @@ __global__ void __launch_bounds__(256) ens_dirichlet_kernel(const ens_inst* __re
 // the one-sided or central form of each axis is fixed once as two neighbour offsets and a factor;
 // z advances ENS_GRAD_ZU planes at a time with every load of those planes issued before their
 // arithmetic, which keeps enough loads in flight for small meshes to stream at HBM rate.
-static constexpr int ENS_GRAD_ZC = 32;
-static constexpr int ENS_GRAD_ZU = 4;
+static constexpr int ENS_GRAD_ZC = 64;
+static constexpr int ENS_GRAD_ZU = 8;
 
 // neighbour offsets lo, hi and factor of an axis at position pos of n: (u[1] - u[0]) / h at the
 // first voxel, (u[n-1] - u[n-2]) / h at the last, (u[i+1] - u[i-1]) / (2h) inside; an axis of one
