@@ -239,8 +239,10 @@ __device__ __forceinline__ void x_tile_rows(const ens_inst& m, long long local, 
 // R whole rows, so the tile's loads touch each of its cache lines, which stay in L1/L2 between
 // the lanes' neighbouring elements.  (Staging the rows through shared memory with cp.async,
 // double-buffered, measured 8% slower over a 256-mesh ensemble.)
+// Two CTAs of 512 threads per SM (64 registers): at 114 registers a mesh of 3 blocks per line ran 5
+// CTAs of 3 warps per SM, too few warps to hide the loads and barriers.
 template <int AXIS>
-__global__ void __launch_bounds__(512) ens_sweep_kernel(const ens_inst* __restrict__ inst,
+__global__ void __launch_bounds__(512, 2) ens_sweep_kernel(const ens_inst* __restrict__ inst,
 														 const long long* __restrict__ first, int count,
 														 long long units, long long chunk, int maxP)
 {
