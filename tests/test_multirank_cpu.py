@@ -83,3 +83,25 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("workload", ["batch-256", "surrogate-128"])
+def test_reference_arm_of_the_other_workloads(workload):
+    """The reference arm on the batched and surrogate workloads: the batch times the CPU port over
+    as many instances as fit its budget; the reference has no surrogate, which the line says."""
+    import oracle
+
+    oracle.build()
+    cmd = [sys.executable, "bench.py", "--impl", "reference", "--workload", workload, "--reference-budget-s", "2"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference"
+    if workload == "surrogate-128":
+        assert "unavailable" in line
+    else:
+        assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+        assert line["e2e"]["d2h_bytes_per_step"] == 0
