@@ -304,8 +304,9 @@ int bfvm_sur_agent_rates(const int32_t bounding_box_mins[3], const int32_t voxel
                          const float* saturation_densities, const float* uptake_rates, const float* net_export_rates,
                          const float* volumes, const float* positions, float* sources, float* sinks,
                          int32_t* error_flags, void* stream);
-/* field [voxels][substrates] (device) = sum of Gaussian bumps, bump_params (host) [substrates][bumps][5] =
- * (x, y, z, width, amplitude) in voxel units; synchronous */
+/* field [voxels][substrates] (device) = sum of Gaussian bumps, bump_params (host, read during the
+ * call) [substrates][bumps][5] = (x, y, z, width, amplitude) in voxel units; 1..10 substrates, 1..16
+ * bumps; ordered on `stream` */
 int bfvm_sur_random_field(const int32_t grid_shape[3], int32_t substrates, int32_t bumps, const float* bump_params,
                           float* field, void* stream);
 /*

@@ -166,8 +166,14 @@ __global__ void sur_agent_rates_kernel(int A, int S, const float* __restrict__ s
 }
 
 // field[v][s] = sum over bumps of amp * exp(-|x - c|^2 / (2 w^2)), bump parameters [S][bumps][5]
-// = (cx, cy, cz, w, amp) in voxel units
-__global__ void sur_bumps_kernel(long long V, int S, int X, int Y, int bumps, const float* __restrict__ bp,
+// = (cx, cy, cz, w, amp) in voxel units, passed by value (at most 10 substrates x 16 bumps)
+static constexpr int SUR_MAX_BUMPS = 16;
+struct bump_set
+{
+	float p[10 * SUR_MAX_BUMPS * 5];
+};
+
+__global__ void sur_bumps_kernel(long long V, int S, int X, int Y, int bumps, const __grid_constant__ bump_set bs,
 								 float* __restrict__ field)
 {
 	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < V * S; i += (long long)gridDim.x * blockDim.x)
@@ -178,7 +184,7 @@ __global__ void sur_bumps_kernel(long long V, int S, int X, int Y, int bumps, co
 		float acc = 0.f;
 		for (int k = 0; k < bumps; k++)
 		{
-			const float* b = bp + ((size_t)s * bumps + k) * 5;
+			const float* b = bs.p + ((size_t)s * bumps + k) * 5;
 			const float dx = x - b[0], dy = y - b[1], dz = z - b[2];
 			acc += b[4] * __expf(-(dx * dx + dy * dy + dz * dz) / (2.f * b[3] * b[3]));
 		}
@@ -645,26 +651,16 @@ int bfvm_sur_agent_rates(const int32_t bounding_box_mins[3], const int32_t voxel
 int bfvm_sur_random_field(const int32_t grid_shape[3], int32_t substrates, int32_t bumps, const float* bump_params,
 						  float* field, void* stream)
 {
-	if (!grid_shape || !bump_params || !field || substrates < 1 || bumps < 1 || bumps > 64)
-		return fail(BFVM_ERR_INVALID_ARGUMENT, "bad argument");
-	cudaStream_t s = static_cast<cudaStream_t>(stream);
-	const size_t np = (size_t)substrates * bumps * 5;
-	float* dp = nullptr;
-	int st;
-	if ((st = device_alloc(&dp, np)))
-		return st;
-	cudaError_t e = cudaMemcpyAsync(dp, bump_params, np * sizeof(float), cudaMemcpyHostToDevice, s);
+	if (!grid_shape || !bump_params || !field || substrates < 1 || substrates > 10 || bumps < 1
+		|| bumps > SUR_MAX_BUMPS)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "random fields take 1..10 substrates and 1..16 bumps");
+	bump_set bs;
+	std::memcpy(bs.p, bump_params, (size_t)substrates * bumps * 5 * sizeof(float));
 	const long long V = (long long)grid_shape[0] * grid_shape[1] * grid_shape[2];
-	if (e == cudaSuccess)
-	{
-		sur_bumps_kernel<<<grid_for(V * substrates), 256, 0, s>>>(V, substrates, grid_shape[0], grid_shape[1], bumps, dp,
-																  field);
-		e = cudaGetLastError();
-	}
-	if (e == cudaSuccess)
-		e = cudaStreamSynchronize(s);
-	device_free(dp);
-	return e == cudaSuccess ? BFVM_OK : cuda_fail(e, "bfvm_sur_random_field");
+	sur_bumps_kernel<<<grid_for(V * substrates), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+		V, substrates, grid_shape[0], grid_shape[1], bumps, bs, field);
+	BFVM_CUDA(cudaGetLastError());
+	return BFVM_OK;
 }
 
 int bfvm_sur_conv3d(const int32_t shape[4], const void* input, const void* weights, const float* bias,
