@@ -113,6 +113,7 @@ static void destroy_all(bfvm_solver* s)
 	device_free(s->grad);
 	device_free(s->slab_coef);
 	device_free(s->slab_carry);
+	device_free(s->slab_rw);
 	device_free(s->dev_error);
 	if (s->copy_stream)
 	{
@@ -418,10 +419,18 @@ static int create_solver(bfvm_solver** out, int device, int dims, const int32_t 
 			precompute_axis(s->slab_global_z, s->voxel[2], 3, s->S, s->dt, s->D.data(), s->decay.data(), 32, bp, ep, g,
 							G, c, gq, Gp, P, bl, ex);
 			slab_coefficients(s->slab_global_z, s->S, bp, c, slab->count, slab->bounds.data(), coef);
+			std::vector<float> rw;
+			int a_first;
+			slab_reduce_weights(s->slab_global_z, s->slab_z0, s->slab_z0 + grid[2], s->S, bp, c, rw, a_first, s->slab_na,
+								s->slab_nb);
+			s->slab_a0 = a_first - s->slab_z0;
 			const size_t lines = (size_t)grid[0] * grid[1] * substrates;
-			if ((st = device_alloc(&s->slab_coef, coef.size())) || (st = device_alloc(&s->slab_carry, 2 * lines)))
+			if ((st = device_alloc(&s->slab_coef, coef.size())) || (st = device_alloc(&s->slab_carry, 2 * lines))
+				|| (st = device_alloc(&s->slab_rw, std::max<size_t>(rw.size(), 4))))
 				break;
-			if (cudaMemcpy(s->slab_coef, coef.data(), coef.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+			if (cudaMemcpy(s->slab_coef, coef.data(), coef.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess
+				|| (!rw.empty()
+					&& cudaMemcpy(s->slab_rw, rw.data(), rw.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess))
 			{
 				st = cuda_fail(cudaGetLastError(), "cudaMemcpy");
 				break;

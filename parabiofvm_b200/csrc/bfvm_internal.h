@@ -164,6 +164,10 @@ struct bfvm_solver
 	int slab_global_z = 0;
 	float* slab_coef = nullptr;	 // device [slab_count][3][S]: Gamma, beta, Lambda of slab_coefficients
 	float* slab_carry = nullptr; // device [2][X*Y*S]: this slab's left and right carries of the step
+	// the reduce pass's weights (slab_reduce_weights): A over local planes [slab_a0, slab_a0 +
+	// slab_na), B over local planes [0, slab_nb); device [slab_na + slab_nb][S]
+	float* slab_rw = nullptr;
+	int slab_a0 = 0, slab_na = 0, slab_nb = 0;
 	int slab_phase = 0;			 // 1 between bfvm_slab_diffusion_begin and _end
 
 	// asynchronous agent copies (bfvm_store_agent_positions_async, bfvm_load_internalized_async) run
@@ -189,6 +193,9 @@ void precompute_padded_range(int n, int i0, int i1, int S, const std::vector<flo
 							 int& P, int& pad, std::vector<float>& tab);
 void slab_coefficients(int n, int S, const std::vector<float>& bp, const std::vector<float>& c, int count,
 					   const int* bounds, std::vector<float>& out);
+// the weights of A and B of the slab holding elements [i0, i1), over the planes that matter
+void slab_reduce_weights(int n, int i0, int i1, int S, const std::vector<float>& bp, const std::vector<float>& c,
+						 std::vector<float>& w, int& a_first, int& na, int& nb);
 
 // bfvm_api.cu
 int one_step(bfvm_solver* s, bool recompute); // diffusion, gradient, secretion on the solver's stream
@@ -204,9 +211,8 @@ int launch_staged_sweep(bfvm_solver* s, int axis, const sweep_tuning& tune, bool
 std::vector<sweep_tuning> staged_sweep_shapes(bfvm_solver* s, int axis);
 // autotune.cu: a tuned launch shape of an equal mesh, from the process-wide cache
 bool cached_tuning(const bfvm_solver* s, int axis, sweep_tuning& out);
-// the z sweep of a slab solver: mode 1 (reduce) writes A and B of every z line to `out` [2][lines]
-// and leaves the field alone; mode 2 (solve) solves with the carries in s->slab_carry
-int launch_slab_z(bfvm_solver* s, int mode, float* out);
+// the solve pass of a slab solver's z sweep, with the carries in s->slab_carry
+int launch_slab_z(bfvm_solver* s);
 // dirichlet.cu
 int launch_dirichlet(bfvm_solver* s);
 int rebuild_dirichlet(bfvm_solver* s);

@@ -251,4 +251,92 @@ void slab_coefficients(int n, int S, const std::vector<float>& bp, const std::ve
 	}
 }
 
+// Weights of the reduce pass of a z-slab holding elements [i0, i1) of lines of n elements
+// (slab_reduce_kernel).  Solved from zero carries, the slab's last forward value A and its first
+// solution B are linear in the slab's right-hand sides d_i:
+//   A = sum_i alpha_i d_i,   alpha_i = prod_{m=i}^{i1-2} (-e_m),
+//   B = sum_i omega_i d_i,   omega_{i1-1} = phi_{i1-1},  omega_i = phi_i - e_i omega_{i+1},
+// with e = c b' (the float product) and phi_k = b'_k prod_{m=i0}^{k-1} (-c b'_m), the weight of the
+// forward value f_k in the backward substitution's first element.  The weights shrink
+// geometrically away from the end each sum belongs to, so the sums keep only the planes whose
+// weights matter: planes are dropped from the far end while the dropped weights (the largest over
+// the substrates, summed) stay at most 2^-50.  That moves A and B by at most 2^-50 of the line's
+// largest |d|.  A is needed only below a neighbour (i1 < n), B only above one (i0 > 0); a sum not
+// needed keeps no planes.
+// Output w = alpha of planes [a_first, i1) as [na][S], then omega of planes [i0, i0 + nb) as
+// [nb][S], evaluated in double from the float b' and e and rounded once.
+void slab_reduce_weights(int n, int i0, int i1, int S, const std::vector<float>& bp, const std::vector<float>& c,
+						 std::vector<float>& w, int& a_first, int& na, int& nb)
+{
+	const int nl = i1 - i0;
+	const double drop = std::ldexp(1.0, -50);
+	std::vector<double> alpha((size_t)nl * S), omega((size_t)nl * S), phi((size_t)nl);
+	for (int s = 0; s < S; s++)
+	{
+		const double cs = (double)c[s];
+		auto b = [&](int i) { return (double)bp[(size_t)i * S + s]; };
+		auto e = [&](int i) { return (double)(c[s] * bp[(size_t)i * S + s]); };
+		double acc = 1.0;
+		for (int i = i1 - 1; i >= i0; i--)
+		{
+			alpha[(size_t)(i - i0) * S + s] = acc;
+			if (i > i0)
+				acc *= -e(i - 1);
+		}
+		double pr = 1.0;
+		for (int k = i0; k < i1; k++)
+		{
+			phi[k - i0] = b(k) * pr;
+			pr *= -cs * b(k);
+		}
+		double om = 0.0;
+		for (int i = i1 - 1; i >= i0; i--)
+		{
+			om = (i == i1 - 1) ? phi[i - i0] : phi[i - i0] - e(i) * om;
+			omega[(size_t)(i - i0) * S + s] = om;
+		}
+	}
+	auto largest = [&](const std::vector<double>& v, int i) {
+		double m = 0.0;
+		for (int s = 0; s < S; s++)
+			m = std::max(m, std::fabs(v[(size_t)(i - i0) * S + s]));
+		return m;
+	};
+	a_first = i1;
+	if (i1 < n)
+	{
+		double tail = 0.0;
+		a_first = i0;
+		for (int i = i0; i < i1; i++)
+		{
+			tail += largest(alpha, i);
+			if (tail > drop)
+				break;
+			a_first = i + 1;
+		}
+	}
+	na = i1 - a_first;
+	int b_end = i0;
+	if (i0 > 0)
+	{
+		double tail = 0.0;
+		b_end = i1;
+		for (int i = i1 - 1; i >= i0; i--)
+		{
+			tail += largest(omega, i);
+			if (tail > drop)
+				break;
+			b_end = i;
+		}
+	}
+	nb = b_end - i0;
+	w.assign((size_t)(na + nb) * S, 0.f);
+	for (int i = a_first; i < i1; i++)
+		for (int s = 0; s < S; s++)
+			w[(size_t)(i - a_first) * S + s] = (float)alpha[(size_t)(i - i0) * S + s];
+	for (int i = i0; i < b_end; i++)
+		for (int s = 0; s < S; s++)
+			w[(size_t)(na + i - i0) * S + s] = (float)omega[(size_t)(i - i0) * S + s];
+}
+
 } // namespace bfvm

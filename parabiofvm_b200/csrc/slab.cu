@@ -6,8 +6,11 @@
 // * The z sweep.  Every z line is one tridiagonal system over the whole mesh.  A slab holds the
 //   whole line's Thomas coefficients for its planes (precompute_padded_range) and solves its part
 //   of every line in two passes around one exchange:
-//     1. reduce: solve from zero carries and publish, per line, A = the forward value at the
-//        slab's last plane and B = the solution at its first plane (2 floats per line);
+//     1. reduce: publish, per line, A = the forward value at the slab's last plane and B = the
+//        solution at its first plane, both from zero carries (2 floats per line).  Both are linear
+//        in the slab's field, with weights that shrink geometrically away from the plane each
+//        belongs to (slab_reduce_weights), so slab_reduce_kernel forms them as sums over the
+//        planes near the slab's edges alone;
 //     2. the caller gathers every slab's (A, B) (an all-gather over NCCL, or copies on one GPU);
 //     3. combine: the slab's true carries follow from the gathered values by the recurrences of
 //        slab_coefficients, C_{k+1} = A_k + Gamma_k C_k and X_{k-1} = B_k + beta_k C_k + Lambda_k X_k;
@@ -57,6 +60,81 @@ __global__ void __launch_bounds__(256) slab_combine_kernel(const float* __restri
 		carry[q] = Ck[me];
 		carry[lines + q] = X;
 	}
+}
+
+// The reduce pass of a slab's z sweep.  For every z line q (s = q mod S):
+//   out[q] = A = sum_{k < na} wa[k][s] u[a0 + k][q],   out[lines + q] = B = sum_{k < nb} wb[k][s] u[k][q],
+// each summed from its smallest weights to its largest (towards the slab edge it belongs to).
+// V lines per thread: 4 when S is a multiple of 4 (16-byte loads of the field and the weights).
+template <int V>
+__global__ void __launch_bounds__(256) slab_reduce_kernel(const float* __restrict__ u, const float* __restrict__ wa,
+														   const float* __restrict__ wb, float* __restrict__ out,
+														   long long lines, int S, int a0, int na, int nb)
+{
+	const long long q = (blockIdx.x * (long long)blockDim.x + threadIdx.x) * V;
+	if (q >= lines)
+		return;
+	const int s = (int)(q % S);
+	auto load = [](const float* p, float (&x)[V]) {
+		if constexpr (V == 4)
+		{
+			const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+			x[0] = v.x;
+			x[1] = v.y;
+			x[2] = v.z;
+			x[3] = v.w;
+		}
+		else
+			x[0] = __ldg(p);
+	};
+	float A[V], B[V];
+#pragma unroll
+	for (int i = 0; i < V; i++)
+		A[i] = B[i] = 0.f;
+	const float* ua = u + (long long)a0 * lines + q;
+#pragma unroll 8
+	for (int k = 0; k < na; k++)
+	{
+		float x[V], w[V];
+		load(ua + (long long)k * lines, x);
+		load(wa + (size_t)k * S + s, w);
+#pragma unroll
+		for (int i = 0; i < V; i++)
+			A[i] = fmaf(w[i], x[i], A[i]);
+	}
+#pragma unroll 8
+	for (int k = nb - 1; k >= 0; k--)
+	{
+		float x[V], w[V];
+		load(u + (long long)k * lines + q, x);
+		load(wb + (size_t)k * S + s, w);
+#pragma unroll
+		for (int i = 0; i < V; i++)
+			B[i] = fmaf(w[i], x[i], B[i]);
+	}
+#pragma unroll
+	for (int i = 0; i < V; i++)
+	{
+		out[q + i] = A[i];
+		out[lines + q + i] = B[i];
+	}
+}
+
+static int launch_slab_reduce(bfvm_solver* s, float* out)
+{
+	const long long lines = (long long)s->grid[0] * s->grid[1] * s->S;
+	const int V = s->S % 4 == 0 ? 4 : 1;
+	const int threads = 256;
+	const long long blocks = (lines / V + threads - 1) / threads;
+	const float* wa = s->slab_rw;
+	const float* wb = s->slab_rw + (size_t)s->slab_na * s->S;
+	if (V == 4)
+		slab_reduce_kernel<4><<<(unsigned)blocks, threads, 0, s->stream>>>(s->dens, wa, wb, out, lines, s->S,
+																		   s->slab_a0, s->slab_na, s->slab_nb);
+	else
+		slab_reduce_kernel<1><<<(unsigned)blocks, threads, 0, s->stream>>>(s->dens, wa, wb, out, lines, s->S,
+																		   s->slab_a0, s->slab_na, s->slab_nb);
+	return check_launch(s, "slab_reduce_kernel");
 }
 
 // The z component of the gradient on a slab's first plane (edge 0, when `below` is given) and last
@@ -146,7 +224,7 @@ int bfvm_slab_diffusion_begin(bfvm_solver* s, float* exchange)
 	if (s->slab_phase)
 		return fail(BFVM_ERR_STATE, "bfvm_slab_diffusion_begin called twice without bfvm_slab_diffusion_end");
 	if ((st = launch_sweep(s, 0, false)) || (st = launch_sweep(s, 1, false)) || (st = launch_dirichlet(s))
-		|| (st = launch_slab_z(s, 1, exchange)))
+		|| (st = launch_slab_reduce(s, exchange)))
 		return st;
 	s->slab_phase = 1;
 	return BFVM_OK;
@@ -166,7 +244,7 @@ int bfvm_slab_diffusion_end(bfvm_solver* s, const float* exchange_all)
 	const long long blocks = std::min<long long>((lines + threads - 1) / threads, 148LL * 16);
 	slab_combine_kernel<<<(unsigned)blocks, threads, 0, s->stream>>>(exchange_all, s->slab_coef, s->slab_carry, lines,
 																	 s->S, s->slab_count, s->slab_index);
-	if ((st = check_launch(s, "slab_combine_kernel")) || (st = launch_slab_z(s, 2, nullptr))
+	if ((st = check_launch(s, "slab_combine_kernel")) || (st = launch_slab_z(s))
 		|| (st = launch_dirichlet(s)))
 		return st;
 	s->slab_phase = 0;

@@ -205,7 +205,6 @@ static sweep_args make_args(bfvm_solver* st, int axis)
 	a.Z = st->grid[2];
 	a.err = st->dev_error;
 	a.slab_carry = nullptr;
-	a.slab_out = nullptr;
 	a.slab_lines = 0;
 	return a;
 }
@@ -226,16 +225,15 @@ std::vector<sweep_tuning> staged_sweep_shapes(bfvm_solver* st, int axis)
 	return shapes;
 }
 
-int launch_slab_z(bfvm_solver* st, int mode, float* out)
+int launch_slab_z(bfvm_solver* st)
 {
 	sweep_args a = make_args(st, 2);
 	a.slab_lines = (long long)st->grid[0] * st->grid[1] * st->S;
 	a.slab_carry = st->slab_carry;
-	a.slab_out = out;
 	bool handled = false;
 	int rc = BFVM_OK;
 	if (st->use_tma)
-		rc = launch_sweep_tma(st, 2, a, handled, &st->tune[2], nullptr, mode);
+		rc = launch_sweep_tma(st, 2, a, handled, &st->tune[2], nullptr, true);
 	if (!rc && !handled)
 		rc = fail(BFVM_ERR_INVALID_ARGUMENT, "the z sweep of a slab needs the TMA-staged kernel: at most 512 planes "
 											 "per slab, X * substrates a multiple of 4, and the tma_sweeps option on");

@@ -21,10 +21,9 @@ struct sweep_args
 	int vP, pad;
 	int X, Y, Z;
 	int* err; // device error flags (DEVERR_*)
-	// z-slab passes (sweep_tma.cu): per-line carries in [2][slab_lines] (C, X), and the reduce
-	// pass's output [2][slab_lines] (A, B); null for every other sweep
+	// the solve pass of a z-slab (sweep_tma.cu): per-line carries in [2][slab_lines] (C, X); null
+	// for every other sweep
 	const float* slab_carry;
-	float* slab_out;
 	long long slab_lines;
 };
 
@@ -190,9 +189,9 @@ inline int set_smem(K kernel, size_t smem)
 	return BFVM_OK;
 }
 
-// slab_mode (z axis only): 0 a plain sweep, 1 the reduce pass, 2 the solve pass of a z-slab
+// slab_solve (z axis only): the solve pass of a z-slab's sweep
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled,
 					 const sweep_tuning* tune = nullptr, std::vector<sweep_tuning>* shapes = nullptr,
-					 int slab_mode = 0);
+					 bool slab_solve = false);
 
 } // namespace bfvm

@@ -175,11 +175,9 @@ __device__ __forceinline__ void store_element(float* p, float v)
 		*p = v;
 }
 
-// SLAB (y/z tiles only): 0 a plain sweep; 1 the reduce pass of a z-slab, which solves from zero
-// outer carries and writes, per line, A = the forward value after the last block and B = the first
-// real solution element, but no field; 2 the solve pass of a z-slab, which enters the line with the
-// carries C (left) and X (right) of slab_carry and writes the field.  The slab passes always run the
-// carry folds, from C and X instead of zero, with the tables of precompute_padded_range.
+// SLAB (y/z tiles only): 0 a plain sweep; 1 the solve pass of a z-slab, which enters every line
+// with the carries C (left) and X (right) of slab_carry: it always runs the carry folds, from C and
+// X instead of zero, with the tables of precompute_padded_range.
 template <bool ROWS, bool NOALLOC, int SLAB>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
@@ -320,7 +318,7 @@ __global__ void __launch_bounds__(640, 1)
 			const long long q = (w % tt.col_tiles) * 32 + lane;
 			const bool active = q < tt.ncols;
 			float C = 0.f, Xc = 0.f;
-			if (SLAB == 2 && active)
+			if (active)
 			{
 				C = __ldg(&a.slab_carry[q]);
 				Xc = __ldg(&a.slab_carry[a.slab_lines + q]);
@@ -339,20 +337,6 @@ __global__ void __launch_bounds__(640, 1)
 			{
 				const float2 r = tcol[k];
 				d[k] = fmaf(Xc, r.y, fmaf(C, r.x, d[k]));
-			}
-			if (SLAB == 1 && active)
-			{
-				if (j == P - 1)
-					a.slab_out[q] = fmaf(__ldg(&gqtab[j * S + s]), C, carry_f[j * 32 + lane]);
-				if (j == 0)
-				{
-					float first = 0.f;
-#pragma unroll
-					for (int k = 0; k < M; k++)
-						if (k == a.pad)
-							first = d[k];
-					a.slab_out[a.slab_lines + q] = first;
-				}
 			}
 		}
 		else if (P > 1)
@@ -385,7 +369,6 @@ __global__ void __launch_bounds__(640, 1)
 			}
 		}
 
-		if (SLAB != 1)
 		{
 			// recompute the line from an opaque copy of the tile index, so nothing of the load
 			// phase stays live across the solve
@@ -476,9 +459,9 @@ static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtens
 // tune: launch shape to use (groups 0: the built-in choice).  shapes: when given, nothing is
 // launched; the launch shapes that fit are listed instead.
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled, const sweep_tuning* tune,
-					 std::vector<sweep_tuning>* shapes, int slab_mode)
+					 std::vector<sweep_tuning>* shapes, bool slab_solve)
 {
-	if (slab_mode && axis != 2)
+	if (slab_solve && axis != 2)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab passes exist for the z sweep only");
 	handled = false;
 	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2], S = st->S;
@@ -605,10 +588,8 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		return launch_tma_variant<true, true>(st, a, map, tt, smem);
 	if (axis == 1)
 		return launch_tma_variant<false, true>(st, a, map, tt, smem);
-	if (slab_mode == 1)
+	if (slab_solve)
 		return launch_tma_variant<false, false, 1>(st, a, map, tt, smem);
-	if (slab_mode == 2)
-		return launch_tma_variant<false, false, 2>(st, a, map, tt, smem);
 	return launch_tma_variant<false, false>(st, a, map, tt, smem);
 }
 

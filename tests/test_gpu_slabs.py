@@ -140,3 +140,46 @@ def test_whole_mesh_calls_are_refused_on_a_split_mesh():
         Batch([s])
     s.synchronize()
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("planes,bounds,D", [
+    (100, [0, 37, 70, 100], [50.0, 1e3, 1e5, 1e6]),  # slow decay: the sums keep every plane
+    (300, [0, 150, 300], [50.0, 1e3, 5e3, 1e4]),      # fast decay: the sums keep the edge planes
+    (300, [0, 100, 200, 300], [1e3, 3e4, 1e5, 2e5]),
+])
+def test_reduce_pass_publishes_the_zero_carry_solve(planes, bounds, D):
+    """The exchange that bfvm_slab_diffusion_begin writes, A = the forward value at the slab's last
+    plane and B = its first solution, both from zero carries, against the float64 Thomas solve of
+    the slab's part of every z line (src/solver/host/diffusion_solver.cpp:72-142) on the field the
+    x and y sweeps left (no Dirichlet conditions, so that field is the z sweep's right-hand side)."""
+    from parabiofvm_b200 import slabs as sl
+    from test_slabs_cpu import slab_solve, thomas_coefficients
+
+    w = synthetic(8, 4, 0, seed=planes + len(bounds), boundary_substrate0=False)
+    w.diffusion_coefficients = list(D)
+    w.bbox_max = (w.bbox_max[0], w.bbox_max[1], planes * w.voxel_shape[2])
+    w.densities = np.random.default_rng(planes).uniform(0, 1, w.voxel_count * w.S).astype(np.float32)
+    bp, c = thomas_coefficients(planes, w.voxel_shape[2], 3, w.time_step, w.diffusion_coefficients, w.decay_rates)
+    for k in range(len(bounds) - 1):
+        i0, i1 = bounds[k], bounds[k + 1]
+        s = sl.make_slab(w, bounds, k)
+        s.sweep(0)
+        s.sweep(1)
+        d = s.load_densities().reshape(i1 - i0, -1).astype(np.float64)
+        s.close()
+        s = sl.make_slab(w, bounds, k)
+        s.diffusion_begin()
+        ex = s.exchange.cpu().numpy().reshape(2, -1).astype(np.float64)
+        s.close()
+        x, f = slab_solve(d, bp, c, i0, i1)
+        # every weight is positive (c < 0 in the reference's sign convention) and the field too, so
+        # the float sums carry a relative error of a few ulps per term at most
+        if i1 < planes:
+            assert np.all(np.abs(ex[0] - f[-1]) <= 8e-6 * f[-1]), k
+        else:
+            assert not ex[0].any()
+        if i0 > 0:
+            assert np.all(np.abs(ex[1] - x[0]) <= 8e-6 * x[0]), k
+        else:
+            assert not ex[1].any()
