@@ -142,6 +142,34 @@ int bfvm_gradient_solve(bfvm_solver* s);
 int bfvm_secretion_solve(bfvm_solver* s, int recompute);
 /* cell_solver::release_internalized_substrates for agent `index`. */
 int bfvm_release_internalized(bfvm_solver* s, int32_t index);
+/*
+ * Agents added and removed on the GPU, without moving the stored agents through the host (the
+ * reference re-copies every agent array after any change, src/solver/device/CUDA/cell_solver.cpp:
+ * 172-178).  The next secretion call rebuilds the voxel binning, as after bfvm_store_agents with a
+ * new count.
+ *
+ * bfvm_add_agents: agent_data::add() (src/agent_data.cpp:10-25) `count` times, the new agents
+ * taking indices [stored, stored + count) with the values of the host arrays given (shapes as in
+ * bfvm_store_agents, `count` rows each).  A NULL array leaves that quantity 0 for the new agents,
+ * as add() does.  Only the new rows cross the host link; grown storage is copied on the device.
+ *
+ * bfvm_remove_agents: agent_data::remove (src/agent_data.cpp:27-53) of indices[0], then
+ * indices[1], ... in that order, each moving the then-last agent into the freed slot.  Every index
+ * must lie below the agent count at its turn; otherwise nothing changes and the call returns
+ * BFVM_ERR_INVALID_ARGUMENT.  Only the indices cross the host link.
+ *
+ * bfvm_plan_agent_removal: the host part of bfvm_remove_agents, without a solver or a device.  For
+ * `agents` agents and the removals indices[0 .. count), it returns the agents left and the moves
+ * that bring the stored rows into the order sequential agent_data::remove calls leave: row dst[k]
+ * takes row src[k] for k < *moves (dst and src hold `count` entries; sources lie at or above
+ * *remaining and destinations below it, so the moves are independent).
+ */
+int bfvm_add_agents(bfvm_solver* s, int32_t count, const float* secretion_rates, const float* saturation_densities,
+					const float* uptake_rates, const float* net_export_rates, const float* internalized_substrates,
+					const float* fraction_released_at_death, const float* volumes, const float* positions);
+int bfvm_remove_agents(bfvm_solver* s, int32_t count, const int32_t* indices);
+int bfvm_plan_agent_removal(int32_t agents, int32_t count, const int32_t* indices, int32_t* remaining,
+							int32_t* moves, int32_t* dst, int32_t* src);
 
 /*
  * `steps` full steps of the reference driver's loop (src/main.cpp:68-107): diffusion, gradient,

@@ -34,6 +34,21 @@ def _fp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
+def plan_agent_removal(agents, indices):
+    """Host part of Solver.remove_agents (bfvm_plan_agent_removal, no device): the agents left
+    after agent_data::remove of indices[0], indices[1], ... and the moves (dst, src) of agent rows
+    that leave the stored order the reference leaves."""
+    idx = np.ascontiguousarray(indices, dtype=np.int32).reshape(-1)
+    P32 = ctypes.POINTER(ctypes.c_int32)
+    dst = np.zeros(max(idx.size, 1), np.int32)
+    src = np.zeros(max(idx.size, 1), np.int32)
+    remaining = ctypes.c_int32()
+    moves = ctypes.c_int32()
+    check(_abi.load().bfvm_plan_agent_removal(int(agents), idx.size, idx.ctypes.data_as(P32), ctypes.byref(remaining),
+                                              ctypes.byref(moves), dst.ctypes.data_as(P32), src.ctypes.data_as(P32)))
+    return int(remaining.value), dst[:moves.value].copy(), src[:moves.value].copy()
+
+
 class Solver:
     """A microenvironment resident on one GPU (bfvm_create ... bfvm_destroy)."""
 
@@ -191,6 +206,26 @@ class Solver:
 
     def release(self, index):
         check(self._lib.bfvm_release_internalized(self._h, int(index)))
+
+    def add_agents(self, count, secretion_rates=None, saturation_densities=None, uptake_rates=None,
+                   net_export_rates=None, internalized=None, fraction_released=None, volumes=None, positions=None):
+        """Append `count` agents on the GPU (agent_data::add per agent), with these rows for them;
+        an array left None stays 0.  The stored agents do not pass through the host."""
+        count = int(count)
+        rows = [self.S] * 6 + [1, self.dims]
+        arrs = [None if a is None else _f32(a, count * r)
+                for a, r in zip((secretion_rates, saturation_densities, uptake_rates, net_export_rates, internalized,
+                                 fraction_released, volumes, positions), rows)]
+        self._added_keep = arrs
+        check(self._lib.bfvm_add_agents(self._h, count, *[None if a is None else _fp(a) for a in arrs]))
+        self.agents_count += count
+
+    def remove_agents(self, indices):
+        """agent_data::remove of indices[0], indices[1], ... in order, on the GPU: each moves the
+        then-last agent into the freed slot."""
+        idx = np.ascontiguousarray(indices, dtype=np.int32).reshape(-1)
+        check(self._lib.bfvm_remove_agents(self._h, idx.size, idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        self.agents_count -= idx.size
 
     def run_steps(self, steps, first_step=0):
         check(self._lib.bfvm_run_steps(self._h, int(steps), int(first_step)))

@@ -49,6 +49,10 @@ SIGNATURES = {
     "bfvm_gradient_solve": (c_int, [c_void_p]),
     "bfvm_secretion_solve": (c_int, [c_void_p, c_int]),
     "bfvm_release_internalized": (c_int, [c_void_p, c_int32]),
+    "bfvm_add_agents": (c_int, [c_void_p, c_int32] + [P(c_float)] * 8),
+    "bfvm_remove_agents": (c_int, [c_void_p, c_int32, P(c_int32)]),
+    "bfvm_plan_agent_removal": (c_int, [c_int32, c_int32, P(c_int32), P(c_int32), P(c_int32), P(c_int32),
+                                        P(c_int32)]),
     "bfvm_set_bulk_rates": (c_int, [c_void_p, c_int, P(c_float), P(c_float), P(c_float)]),
     "bfvm_bulk_solve": (c_int, [c_void_p]),
     "bfvm_run_steps": (c_int, [c_void_p, c_int32, c_int32]),

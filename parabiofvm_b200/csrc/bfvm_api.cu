@@ -6,6 +6,7 @@
 #include <map>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "bfvm_internal.h"
@@ -812,6 +813,122 @@ int bfvm_release_internalized(bfvm_solver* s, int32_t index)
 	if ((rc = order_after_copies(s)))
 		return rc;
 	return launch_release(s, index);
+}
+
+int bfvm_add_agents(bfvm_solver* s, int32_t count, const float* secretion_rates, const float* saturation_densities,
+					const float* uptake_rates, const float* net_export_rates, const float* internalized_substrates,
+					const float* fraction_released_at_death, const float* volumes, const float* positions)
+{
+	CHECK_SOLVER(s);
+	if (count < 0)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "count must not be negative");
+	if (count == 0)
+		return BFVM_OK;
+	if ((long long)s->ag.count + count > INT32_MAX)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "more than 2^31 - 1 agents");
+	int st;
+	if ((st = order_after_copies(s)))
+		return st;
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	free_graphs(s);
+	const int old = s->ag.count;
+	if ((st = cell_grow(s, old + count)))
+		return st;
+	agent_state& a = s->ag;
+	const float* src[8] = { secretion_rates, saturation_densities, uptake_rates, net_export_rates,
+							internalized_substrates, fraction_released_at_death, volumes, positions };
+	float* dst[8] = { a.sec, a.sat, a.upt, a.nex, a.intern, a.frac, a.vol, a.pos };
+	const size_t row[8] = { (size_t)s->S, (size_t)s->S, (size_t)s->S, (size_t)s->S, (size_t)s->S, (size_t)s->S, 1,
+							(size_t)s->dims };
+	for (int k = 0; k < 8; k++)
+	{
+		float* d = dst[k] + (size_t)old * row[k];
+		const size_t bytes = (size_t)count * row[k] * sizeof(float);
+		if (src[k])
+			BFVM_CUDA(cudaMemcpyAsync(d, src[k], bytes, cudaMemcpyHostToDevice, s->stream));
+		else
+			BFVM_CUDA(cudaMemsetAsync(d, 0, bytes, s->stream));
+	}
+	a.binned = false;
+	return BFVM_OK;
+}
+
+// The moves that sequential agent_data::remove calls amount to.  Only agents at or above the final
+// count ever move (a removal moves the then-last agent, and the last slot never falls below the
+// final count), and each moves down into a slot below it: so the stored order needs one move per
+// slot below the final count whose occupant changed, from that occupant's original row.
+static int plan_removal(int agents, int count, const int32_t* indices, int& remaining, std::vector<int>& dst,
+						std::vector<int>& src)
+{
+	if (agents < 0 || count < 0)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "agent and removal counts must not be negative");
+	if (count > 0 && !indices)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null indices");
+	std::unordered_map<int, int> at; // slot -> original row of its agent, for slots whose agent changed
+	int c = agents;
+	for (int k = 0; k < count; k++)
+	{
+		const int i = indices[k];
+		if (i < 0 || i >= c)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "removal " + std::to_string(k) + ": index " + std::to_string(i)
+													   + " is not below the agent count " + std::to_string(c));
+		const int last = c - 1;
+		if (i != last)
+		{
+			const auto it = at.find(last);
+			at[i] = it != at.end() ? it->second : last;
+		}
+		at.erase(last);
+		c--;
+	}
+	remaining = c;
+	dst.clear();
+	src.clear();
+	std::vector<std::pair<int, int>> mv(at.begin(), at.end());
+	std::sort(mv.begin(), mv.end());
+	for (const auto& m : mv)
+	{
+		dst.push_back(m.first);
+		src.push_back(m.second);
+	}
+	return BFVM_OK;
+}
+
+int bfvm_plan_agent_removal(int32_t agents, int32_t count, const int32_t* indices, int32_t* remaining,
+							int32_t* moves, int32_t* dst, int32_t* src)
+{
+	if (!remaining || !moves || (count > 0 && (!dst || !src)))
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null output");
+	int r;
+	std::vector<int> d, f;
+	const int st = plan_removal(agents, count, indices, r, d, f);
+	if (st)
+		return st;
+	*remaining = r;
+	*moves = (int32_t)d.size();
+	std::copy(d.begin(), d.end(), dst);
+	std::copy(f.begin(), f.end(), src);
+	return BFVM_OK;
+}
+
+int bfvm_remove_agents(bfvm_solver* s, int32_t count, const int32_t* indices)
+{
+	CHECK_SOLVER(s);
+	int remaining, st;
+	std::vector<int> dst, src;
+	if ((st = plan_removal(s->ag.count, count, indices, remaining, dst, src)))
+		return st;
+	if (count == 0)
+		return BFVM_OK;
+	if ((st = order_after_copies(s)))
+		return st;
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	free_graphs(s);
+	if ((st = launch_agent_moves(s, dst, src)))
+		return st;
+	s->ag.count = remaining;
+	s->ag.binned = false;
+	return BFVM_OK;
 }
 
 int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)

@@ -91,6 +91,9 @@ struct agent_state
 	int tiles = 0;
 	scan_plan hist_scan, flag_scan;
 	bool binned = false;		 // a recompute has run since the last store
+
+	int* move_idx = nullptr; // [2][moves]: destinations, then sources of bfvm_remove_agents
+	int move_capacity = 0;
 };
 
 } // namespace bfvm
@@ -231,6 +234,9 @@ int cell_alloc(bfvm_solver* s, int count);
 void cell_free(bfvm_solver* s);
 int launch_secretion(bfvm_solver* s, bool recompute);
 int launch_release(bfvm_solver* s, int index);
+// storage for `count` agents keeping the stored rows; the moves dst[k] <- src[k] of every agent row
+int cell_grow(bfvm_solver* s, int count);
+int launch_agent_moves(bfvm_solver* s, const std::vector<int>& dst, const std::vector<int>& src);
 
 // scan.cu
 int scan_plan_build(scan_plan& p, long long n);

@@ -277,6 +277,8 @@ void cell_free(bfvm_solver* s)
 	device_free(a.seg_count_dev);
 	scan_plan_free(a.hist_scan);
 	scan_plan_free(a.flag_scan);
+	device_free(a.move_idx);
+	a.move_capacity = 0;
 	a.capacity = 0;
 	a.count = 0;
 	a.binned = false;
@@ -407,6 +409,109 @@ int launch_release(bfvm_solver* s, int index)
 															  (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]),
 															  s->dev_error);
 	return check_launch(s, "release_kernel");
+}
+
+// Agent storage for `count` agents that keeps the stored agents' rows (bfvm_add_agents).  Growth
+// takes at least half the capacity again, so repeated additions copy each row a bounded number of
+// times; the binning buffers are rebuilt empty, as the next secretion call rebins.
+int cell_grow(bfvm_solver* s, int count)
+{
+	agent_state& a = s->ag;
+	if (count <= a.capacity && a.capacity > 0)
+	{
+		a.count = count;
+		return BFVM_OK;
+	}
+	const int old = a.count;
+	const int cap = (int)std::min<long long>(INT32_MAX, std::max<long long>(count, (long long)a.capacity * 3 / 2));
+	float* keep[8] = { a.sec, a.sat, a.upt, a.nex, a.intern, a.frac, a.vol, a.pos };
+	for (float** p : { &a.sec, &a.sat, &a.upt, &a.nex, &a.intern, &a.frac, &a.vol, &a.pos })
+		*p = nullptr;
+	cell_free(s);
+	int st = cell_alloc(s, cap);
+	if (!st && old > 0)
+	{
+		float* now[8] = { a.sec, a.sat, a.upt, a.nex, a.intern, a.frac, a.vol, a.pos };
+		const size_t rows[8] = { (size_t)s->S, (size_t)s->S, (size_t)s->S, (size_t)s->S, (size_t)s->S, (size_t)s->S, 1,
+								 (size_t)s->dims };
+		for (int k = 0; k < 8 && !st; k++)
+		{
+			const cudaError_t e = cudaMemcpyAsync(now[k], keep[k], (size_t)old * rows[k] * sizeof(float),
+												  cudaMemcpyDeviceToDevice, s->stream);
+			if (e != cudaSuccess)
+				st = cuda_fail(e, "cudaMemcpyAsync");
+		}
+		const cudaError_t e = cudaStreamSynchronize(s->stream);
+		if (!st && e != cudaSuccess)
+			st = cuda_fail(e, "cudaStreamSynchronize");
+	}
+	for (float* p : keep)
+		device_free(p);
+	if (!st)
+		a.count = count;
+	return st;
+}
+
+struct agent_rows
+{
+	float* v[6]; // [A][S]: secretion, saturation, uptake, net export, internalized, fraction released
+	float* vol;	 // [A]
+	float* pos;	 // [A][dims]
+};
+
+// Row dst[k] of every per-agent array takes row src[k] (the moves of a batch of agent removals;
+// no source is a destination, so the moves run in any order).
+__global__ void __launch_bounds__(256) agent_move_kernel(const int* __restrict__ dst, const int* __restrict__ src,
+														  int moves, int S, int dims, agent_rows r)
+{
+	const int per = 6 * S + 1 + dims;
+	const long long n = (long long)moves * per;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+	{
+		const int k = (int)(t / per), e = (int)(t - (long long)k * per);
+		const long long d = __ldg(&dst[k]), f = __ldg(&src[k]);
+		if (e < 6 * S)
+		{
+			float* p = r.v[e / S];
+			const int j = e % S;
+			p[d * S + j] = p[f * S + j];
+		}
+		else if (e == 6 * S)
+			r.vol[d] = r.vol[f];
+		else
+		{
+			const int j = e - 6 * S - 1;
+			r.pos[d * dims + j] = r.pos[f * dims + j];
+		}
+	}
+}
+
+int launch_agent_moves(bfvm_solver* s, const std::vector<int>& dst, const std::vector<int>& src)
+{
+	agent_state& a = s->ag;
+	const int moves = (int)dst.size();
+	if (moves == 0)
+		return BFVM_OK;
+	int st;
+	if (2 * moves > a.move_capacity)
+	{
+		BFVM_CUDA(cudaStreamSynchronize(s->stream));
+		device_free(a.move_idx);
+		a.move_capacity = 0;
+		if ((st = device_alloc(&a.move_idx, (size_t)2 * moves)))
+			return st;
+		a.move_capacity = 2 * moves;
+	}
+	BFVM_CUDA(cudaMemcpyAsync(a.move_idx, dst.data(), (size_t)moves * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+	BFVM_CUDA(cudaMemcpyAsync(a.move_idx + moves, src.data(), (size_t)moves * sizeof(int), cudaMemcpyHostToDevice,
+							  s->stream));
+	agent_rows r{ { a.sec, a.sat, a.upt, a.nex, a.intern, a.frac }, a.vol, a.pos };
+	const long long n = (long long)moves * (6 * s->S + 1 + s->dims);
+	const int threads = 256;
+	const long long blocks = std::min<long long>((n + threads - 1) / threads, 148LL * 8);
+	agent_move_kernel<<<(unsigned)blocks, threads, 0, s->stream>>>(a.move_idx, a.move_idx + moves, moves, s->S,
+																	s->dims, r);
+	return check_launch(s, "agent_move_kernel");
 }
 
 } // namespace bfvm

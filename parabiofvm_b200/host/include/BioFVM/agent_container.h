@@ -15,6 +15,7 @@ namespace biofvm {
 
 namespace solvers::b200 {
 class solver;
+class cell_solver;
 }
 
 class agent_container_base;
@@ -24,6 +25,7 @@ using agent_container_ptr = std::unique_ptr<agent_container_base>;
 class agent_container_base
 {
 	friend solvers::b200::solver;
+	friend solvers::b200::cell_solver;
 
 protected:
 	virtual agent_data& get_agent_data() = 0;

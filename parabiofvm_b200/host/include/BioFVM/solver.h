@@ -14,6 +14,7 @@
 #pragma once
 
 #include <memory>
+#include <vector>
 
 #include "microenvironment.h"
 
@@ -81,6 +82,13 @@ public:
 	void initialize(microenvironment& m);
 	void simulate_secretion_and_uptake(microenvironment& m, bool recompute);
 	void release_internalized_substrates(microenvironment& m, index_t index);
+	// Agents added and removed on the GPU copy alone, keeping it in step with the host agent data
+	// without copying the stored agents again.  add_agents: the host agents [first, first + count)
+	// (added with agent_data::add and filled in) are appended; first must equal the GPU's count.
+	// remove_agents: agent_data::remove of indices[0], indices[1], ... in order, as the host
+	// container did them.
+	void add_agents(microenvironment& m, index_t first, index_t count);
+	void remove_agents(microenvironment& m, const std::vector<index_t>& indices);
 };
 
 class solver

@@ -156,4 +156,24 @@ void cell_solver::release_internalized_substrates(microenvironment&, index_t ind
 	check(bfvm_release_internalized(require(ctx_), index), "bfvm_release_internalized");
 }
 
+void cell_solver::add_agents(microenvironment& m, index_t first, index_t count)
+{
+	agent_data& a = m.agents->get_agent_data();
+	if (first < 0 || count < 0 || first + count > a.agents_count)
+		throw std::runtime_error("add_agents: agents [first, first + count) are not all in the host agent data");
+	const std::size_t S = (std::size_t)m.substrates_count, d = (std::size_t)m.mesh.dims;
+	check(bfvm_add_agents(require(ctx_), count, a.secretion_rates.data() + first * S,
+						  a.saturation_densities.data() + first * S, a.uptake_rates.data() + first * S,
+						  a.net_export_rates.data() + first * S, a.internalized_substrates.data() + first * S,
+						  a.fraction_released_at_death.data() + first * S, a.volumes.data() + first,
+						  a.positions.data() + first * d),
+		  "bfvm_add_agents");
+}
+
+void cell_solver::remove_agents(microenvironment&, const std::vector<index_t>& indices)
+{
+	std::vector<int32_t> idx(indices.begin(), indices.end());
+	check(bfvm_remove_agents(require(ctx_), (int32_t)idx.size(), idx.data()), "bfvm_remove_agents");
+}
+
 } // namespace biofvm::solvers::b200

@@ -7,6 +7,9 @@
 //   facade_cases uniform3d  one diffusion step of the uniform 3D case (test/test.cpp:98-113)
 //   facade_cases step       steps with boundary and interior Dirichlet and agents, plus a release
 //   facade_cases bulk       bulk supply/uptake from the builder's callbacks
+//   facade_cases lifecycle_device / lifecycle_host
+//                           agents released, removed and added between steps, on the GPU copy or
+//                           through load/store round trips
 
 #include <cmath>
 #include <cstdio>
@@ -125,7 +128,7 @@ static int mode_uniform3d()
 // stepped like the reference driver (src/main.cpp:76-96), then one agent releases its
 // internalized substrates.  The inputs are printed with the results so the test can rebuild the
 // same scene for the oracle.
-static int mode_step()
+static microenvironment step_scene()
 {
 	microenvironment_builder b;
 	b.set_time_step(0.01f);
@@ -158,7 +161,13 @@ static int mode_step()
 			a->fraction_released_at_death()[s] = 0.2f * ((i + s) % 5);
 		}
 	}
+	return m;
+}
 
+static int mode_step()
+{
+	microenvironment m = step_scene();
+	const index_t S = m.substrates_count;
 	solver s;
 	s.initialize(m);
 	s.store_data_to_solver(m);
@@ -190,6 +199,81 @@ static int mode_step()
 	print_array("densities", m.substrate_densities.get(), m.mesh.voxel_count() * S);
 	print_array("gradients", m.gradients.get(), 3 * m.mesh.voxel_count() * S);
 	print_array("internalized", d.internalized_substrates.data(), AS, true);
+	std::printf("}\n");
+	return 0;
+}
+
+// Agents that die, appear and leave between steps, as a model's agent loop has them.  The host
+// container does every change; the GPU copy follows either by cell.add_agents / cell.remove_agents
+// (`on_device`) or by the reference's round trip, load_data_from_solver, the change, then
+// store_data_to_solver.  Both must end identical.
+static int mode_lifecycle(bool on_device)
+{
+	microenvironment m = step_scene();
+	const index_t S = m.substrates_count;
+	solver s;
+	s.initialize(m);
+	s.store_data_to_solver(m);
+	auto steps = [&](index_t from, index_t to) {
+		for (index_t step = from; step < to; step++)
+		{
+			s.diffusion.solve(m);
+			s.gradient.solve(m);
+			s.cell.simulate_secretion_and_uptake(m, step % 10 == 0);
+		}
+	};
+	auto remove = [&](const std::vector<index_t>& indices) {
+		if (!on_device)
+			s.load_data_from_solver(m);
+		for (index_t i : indices)
+			m.agents->remove_at(i);
+		if (on_device)
+			s.cell.remove_agents(m, indices);
+		else
+			s.store_data_to_solver(m);
+	};
+	steps(0, 3);
+	// agent 5 dies: it releases its internalized substrates and leaves
+	s.cell.release_internalized_substrates(m, 5);
+	remove({ 5 });
+	steps(3, 5);
+	// six agents appear, two of them in an occupied voxel
+	if (!on_device)
+		s.load_data_from_solver(m);
+	const index_t first = m.agents->agents_count();
+	for (int i = 0; i < 6; i++)
+	{
+		agent* a = m.agents->create_agent();
+		a->volume() = 300.f + 50.f * i;
+		a->position()[0] = i < 2 ? 7.f : 11.f + 17.f * i;
+		a->position()[1] = i < 2 ? 5.f : 9.f + 13.f * i;
+		a->position()[2] = 3.f + 12.f * i;
+		for (index_t s2 = 0; s2 < S; s2++)
+		{
+			a->secretion_rates()[s2] = 0.3f * ((i + s2) % 4);
+			a->saturation_densities()[s2] = 1.5f;
+			a->uptake_rates()[s2] = 0.05f * (i + 1);
+			a->net_export_rates()[s2] = 0.02f * s2;
+			a->internalized_substrates()[s2] = 0.1f * i;
+			a->fraction_released_at_death()[s2] = 0.5f;
+		}
+	}
+	if (on_device)
+		s.cell.add_agents(m, first, 6);
+	else
+		s.store_data_to_solver(m);
+	steps(5, 8);
+	// three agents leave at once: the first, one of the new ones, and the then-last
+	remove({ 0, first + 2, m.agents->agents_count() - 3 });
+	steps(8, 11);
+	s.load_data_from_solver(m);
+
+	const agent_data& d = static_cast<const agent_container&>(*m.agents).data();
+	std::printf("{\"agents\": %d, ", d.agents_count);
+	print_array("volumes", d.volumes.data(), d.agents_count);
+	print_array("densities", m.substrate_densities.get(), m.mesh.voxel_count() * S);
+	print_array("gradients", m.gradients.get(), 3 * m.mesh.voxel_count() * S);
+	print_array("internalized", d.internalized_substrates.data(), (std::size_t)d.agents_count * S, true);
 	std::printf("}\n");
 	return 0;
 }
@@ -244,6 +328,8 @@ int main(int argc, char** argv)
 			return mode_step();
 		if (mode == "bulk")
 			return mode_bulk();
+		if (mode == "lifecycle_device" || mode == "lifecycle_host")
+			return mode_lifecycle(mode == "lifecycle_device");
 	}
 	catch (const std::exception& e)
 	{

@@ -2,8 +2,9 @@
 a paraBioFVM user drives it, from tests/cpp/facade_cases.cpp.
 
 * host behaviour (no GPU): mesh shape, voxel lookup, builder output, agent removal;
-* on the GPU: the uniform 3D diffusion case against the goldens of test/test.cpp:111-112, and a
-  scene with Dirichlet conditions and agents, stepped and released, against the oracle.
+* on the GPU: the uniform 3D diffusion case against the goldens of test/test.cpp:111-112, a
+  scene with Dirichlet conditions and agents, stepped and released, against the oracle, and agents
+  added and removed on the GPU copy against the round trip through the host.
 """
 
 import json
@@ -117,3 +118,15 @@ def test_bulk_from_builder_callbacks(program):
     for _ in range(2):
         o.bulk(supply, uptake, target, True)
     np.testing.assert_array_equal(np.asarray(out["densities"], np.float32), o.densities())
+
+
+@pytest.mark.gpu
+def test_agents_added_and_removed_on_the_gpu_copy(program):
+    """Agents released, removed and added between steps (src/agent_data.cpp:10-53) through
+    cell.add_agents / cell.remove_agents, against the reference's round trip of every agent array
+    (load_data_from_solver, the change on the host, store_data_to_solver): identical results."""
+    dev = run(program, "lifecycle_device")
+    host = run(program, "lifecycle_host")
+    assert dev["agents"] == host["agents"] == 40 - 1 + 6 - 3
+    for k in ("volumes", "densities", "gradients", "internalized"):
+        np.testing.assert_array_equal(np.asarray(dev[k], np.float32), np.asarray(host[k], np.float32), err_msg=k)
