@@ -95,9 +95,84 @@ __device__ __forceinline__ void axis_form(int pos, int n, long long stride, floa
 	}
 }
 
-__global__ void __launch_bounds__(256) ens_gradient_kernel(const ens_inst* __restrict__ inst,
-															const long long* __restrict__ first, int count,
-															long long units)
+// The z march of one column of a 3-D mesh over planes [z0, z1): p and g point at plane z0 of the
+// column in the field and in the x component of the gradient.  Planes that have a next plane run
+// ENS_GRAD_ZU at a time without guards, through pointers that advance a plane per step; the rest
+// (up to ENS_GRAD_ZU - 1 planes, and the mesh's last plane) run one at a time.
+__device__ __forceinline__ void ens_gradient_3d(const ens_inst& m, const float* __restrict__ p, float* __restrict__ g,
+												long long plane, int z0, int z1, long long xlo, long long xhi,
+												float fx, long long ylo, long long yhi, float fy)
+{
+	constexpr int U = ENS_GRAD_ZU;
+	const int Z = m.Z;
+	const long long total = plane * Z;
+	const bool hasx = m.X > 1, hasy = m.Y > 1;
+	const float bz = m.bgrad[2], cz = m.cgrad[2];
+	float prev = z0 > 0 ? __ldg(p - plane) : 0.f;
+	float cur = __ldg(p);
+	int z = z0;
+	const int zmain = min(z1, Z - 1);
+	for (; z + U <= zmain; z += U)
+	{
+		float nx[U], xa[U], xb[U], ya[U], yb[U];
+#pragma unroll
+		for (int k = 0; k < U; k++)
+		{
+			const float* q = p + k * plane;
+			nx[k] = __ldg(q + plane);
+			xa[k] = __ldg(q + xhi);
+			xb[k] = __ldg(q + xlo);
+			ya[k] = __ldg(q + yhi);
+			yb[k] = __ldg(q + ylo);
+		}
+#pragma unroll
+		for (int k = 0; k < U; k++)
+		{
+			const float next = nx[k];
+			const float gx = hasx ? __fmul_rn(__fsub_rn(xa[k], xb[k]), fx) : 0.f;
+			const float gy = hasy ? __fmul_rn(__fsub_rn(ya[k], yb[k]), fy) : 0.f;
+			const float gz = z + k == 0 ? __fmul_rn(__fsub_rn(next, cur), bz) : __fmul_rn(__fsub_rn(next, prev), cz);
+			float* o = g + k * plane;
+			__stcs(o, gx);
+			__stcs(o + total, gy);
+			__stcs(o + 2 * total, gz);
+			prev = cur;
+			cur = next;
+		}
+		p += U * plane;
+		g += U * plane;
+	}
+	for (; z < z1; z++)
+	{
+		const float next = z + 1 < Z ? __ldg(p + plane) : cur;
+		const float gx = hasx ? __fmul_rn(__fsub_rn(__ldg(p + xhi), __ldg(p + xlo)), fx) : 0.f;
+		const float gy = hasy ? __fmul_rn(__fsub_rn(__ldg(p + yhi), __ldg(p + ylo)), fy) : 0.f;
+		float gz;
+		if (Z == 1)
+			gz = 0.f;
+		else if (z == 0)
+			gz = __fmul_rn(__fsub_rn(next, cur), bz);
+		else if (z == Z - 1)
+			gz = __fmul_rn(__fsub_rn(cur, prev), bz);
+		else
+			gz = __fmul_rn(__fsub_rn(next, prev), cz);
+		__stcs(g, gx);
+		__stcs(g + total, gy);
+		__stcs(g + 2 * total, gz);
+		prev = cur;
+		cur = next;
+		p += plane;
+		g += plane;
+	}
+}
+
+// ALL3D: every mesh is 3-D.  The kernel then holds the 3-D march alone, which fits 64 registers, so
+// four CTAs share an SM: twice the loads in flight of the kernel that also holds the 1-D and 2-D
+// forms (held to 128 registers, two CTAs).
+template <bool ALL3D>
+__global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const ens_inst* __restrict__ inst,
+																		   const long long* __restrict__ first,
+																		   int count, long long units)
 {
 	for (long long u = blockIdx.x; u < units; u += gridDim.x)
 	{
@@ -127,6 +202,12 @@ __global__ void __launch_bounds__(256) ens_gradient_kernel(const ens_inst* __res
 		axis_form(x, X, S, m.bgrad[0], m.cgrad[0], xlo, xhi, fx);
 		if (dims >= 2)
 			axis_form(y, Y, XS, m.bgrad[1], m.cgrad[1], ylo, yhi, fy);
+		if (ALL3D || dims == 3)
+		{
+			const long long e0 = (long long)z0 * plane + row;
+			ens_gradient_3d(m, d + e0, g + e0, plane, z0, z1, xlo, xhi, fx, ylo, yhi, fy);
+			continue;
+		}
 		float prev = z0 > 0 ? __ldg(&d[(long long)(z0 - 1) * plane + row]) : 0.f;
 		float cur = __ldg(&d[(long long)z0 * plane + row]);
 		for (int z = z0; z < z1; z += ENS_GRAD_ZU)
@@ -417,6 +498,7 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
 	plan.maxP[0] = plan.maxP[1] = plan.maxP[2] = 1;
 	plan.table_floats[0] = plan.table_floats[1] = plan.table_floats[2] = 0;
 	plan.maxS = 1;
+	plan.all3d = true;
 	for (int i = 0; i < n; i++)
 	{
 		const bfvm_solver* s = meshes[i];
@@ -424,6 +506,7 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
 		m.dens = s->dens;
 		m.grad = s->grad;
 		m.dims = s->dims;
+		plan.all3d = plan.all3d && s->dims == 3;
 		m.S = s->S;
 		m.X = s->grid[0];
 		m.Y = s->grid[1];
@@ -524,8 +607,12 @@ int ensemble_gradient(const ensemble_plan& plan, cudaStream_t stream)
 	const long long units = plan.count ? plan.first_h[ENS_GRADIENT][plan.count] : 0;
 	if (units == 0)
 		return BFVM_OK;
-	ens_gradient_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT], plan.count,
-																  units);
+	if (plan.all3d)
+		ens_gradient_kernel<true><<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT],
+																		   plan.count, units);
+	else
+		ens_gradient_kernel<false><<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT],
+																			plan.count, units);
 	return launched("ens_gradient_kernel");
 }
 

@@ -61,6 +61,7 @@ struct ensemble_plan
 	int maxP[3] = { 1, 1, 1 };		 // largest vP per axis
 	int maxS = 1;
 	size_t table_floats[3] = { 0, 0, 0 }; // largest staged table per axis
+	bool all3d = true;					  // every mesh is 3-D (the gradient kernel without the 1-D/2-D forms)
 };
 
 // Which meshes the ensemble kernels cover: every axis with n >= 2 and at most ENS_MAX_P blocks,
