@@ -337,20 +337,26 @@ __global__ void __launch_bounds__(512, 2) ens_sweep_kernel(const ens_inst* __res
 
 	const long long u0 = (long long)blockIdx.x * chunk;
 	const long long u1 = min(units, u0 + chunk);
+	// the mesh of the current unit, looked up again only when the units cross into the next mesh
+	// (a CTA's chunk of consecutive units mostly stays in one); element offsets within a mesh fit
+	// 31 bits (ensemble_eligible), so the line arithmetic runs in 32-bit integers
 	int cur = -1;
+	long long first_i = 0, first_next = 0;
 	for (long long u = u0; u < u1; u++)
 	{
-		const int i = find_mesh(first, count, u);
-		const ens_inst& m = inst[i];
-		const int S = m.S, P = m.vP[AXIS], pad = m.pad[AXIS];
-		const float* vtab = m.vtab[AXIS];
-		if (i != cur)
+		if (u >= first_next)
 		{
+			const int i = find_mesh(first, count, u);
+			first_i = __ldg(&first[i]);
+			first_next = __ldg(&first[i + 1]);
 			__syncthreads(); // the previous mesh's tables are no longer read
-			ens_stage_tables(vtab, P, S, tab);
+			ens_stage_tables(inst[i].vtab[AXIS], inst[i].vP[AXIS], inst[i].S, tab);
 			__syncthreads();
 			cur = i;
 		}
+		const ens_inst& m = inst[cur];
+		const int S = m.S, P = m.vP[AXIS], pad = m.pad[AXIS];
+		const float* vtab = m.vtab[AXIS];
 		const int N = 32 * P, NP = N + 1;
 		const float2* tgtab = reinterpret_cast<const float2*>(tab);
 		const float* btab = tab + 2 * S * NP;
@@ -360,32 +366,30 @@ __global__ void __launch_bounds__(512, 2) ens_sweep_kernel(const ens_inst* __res
 		const float* Gptab = tgptab + P * S;
 
 		// the line of this lane
-		const long long local = u - first[i];
-		const long long XS = (long long)m.X * S;
+		const int local = (int)(u - first_i);
+		const int XS = m.X * S;
 		bool active;
-		int s;
+		int s, stride;
 		float* line;
-		long long stride;
 		if (AXIS == 0)
 		{
+			const int R = 32 / S;
 			const int rl = lane / S;
 			s = lane - rl * S;
-			long long row0;
-			int rows;
-			x_tile_rows(m, local, row0, rows);
-			active = rl < rows;
+			const int row0 = local * R;
+			active = rl < min(R, m.Y * m.Z - row0);
 			line = m.dens + (active ? row0 + rl : 0) * XS + s;
 			stride = S;
 		}
 		else
 		{
-			const long long ncols = AXIS == 1 ? XS : XS * m.Y;
-			const long long col_tiles = (ncols + 31) / 32;
-			const long long outer = AXIS == 1 ? local / col_tiles : 0;
-			const long long q = (AXIS == 1 ? local % col_tiles : local) * 32 + lane;
+			const int ncols = AXIS == 1 ? XS : XS * m.Y;
+			const int col_tiles = (ncols + 31) / 32;
+			const int outer = AXIS == 1 ? local / col_tiles : 0;
+			const int q = (local - outer * col_tiles) * 32 + lane;
 			active = q < ncols;
-			const long long qq = active ? q : 0;
-			s = (int)(qq % S);
+			const int qq = active ? q : 0;
+			s = qq % S;
 			line = m.dens + outer * XS * m.Y + qq;
 			stride = AXIS == 1 ? XS : XS * m.Y;
 		}
@@ -401,7 +405,7 @@ __global__ void __launch_bounds__(512, 2) ens_sweep_kernel(const ens_inst* __res
 			for (int k = 0; k < M; k++)
 			{
 				const int r = p + k - pad; // real element of virtual element p + k
-				d[k] = (active && r >= 0) ? line[(long long)r * stride] : 0.f;
+				d[k] = (active && r >= 0) ? line[r * stride] : 0.f;
 			}
 			// forward and backward recurrences from zero carries (sweep_tma.cu)
 #pragma unroll
@@ -451,7 +455,7 @@ __global__ void __launch_bounds__(512, 2) ens_sweep_kernel(const ens_inst* __res
 				{
 					const int r = p + k - pad;
 					if (r >= 0)
-						line[(long long)r * stride] = d[k];
+						line[r * stride] = d[k];
 				}
 			}
 		}

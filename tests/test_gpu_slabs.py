@@ -170,6 +170,7 @@ def test_reduce_pass_publishes_the_zero_carry_solve(planes, bounds, D):
         s.close()
         s = sl.make_slab(w, bounds, k)
         s.diffusion_begin()
+        s.synchronize()  # the exchange is written on the slab's own stream
         ex = s.exchange.cpu().numpy().reshape(2, -1).astype(np.float64)
         s.close()
         x, f = slab_solve(d, bp, c, i0, i1)
