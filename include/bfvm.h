@@ -287,6 +287,17 @@ int bfvm_slab_gradient_solve(bfvm_solver* s, const float* plane_below, const flo
 int bfvm_slab_coefficients(int32_t planes, int32_t voxel_z, int32_t substrates, float time_step,
                            const float* diffusion_coefficients, const float* decay_rates, int32_t slab_count,
                            const int32_t* slab_planes, float* coefficients);
+/*
+ * Host only: the weights of the reduce pass of the slab holding planes [first_plane, end_plane) of
+ * a mesh of `planes` planes.  A = sum_k weights[k][s] u[*a_first - first_plane + k] over k <
+ * *a_count, and B = sum_k weights[*a_count + k][s] u[k] over k < *b_count, with u the slab's
+ * planes (line by line).  Planes whose weights sum to at most 2^-50 (the largest over the
+ * substrates) are left out; A is empty for the last slab and B for the first.  `weights` must hold
+ * 2 * (end_plane - first_plane) * substrates floats (both sums may keep every plane).
+ */
+int bfvm_slab_reduce_weights(int32_t planes, int32_t voxel_z, int32_t substrates, float time_step,
+                             const float* diffusion_coefficients, const float* decay_rates, int32_t first_plane,
+                             int32_t end_plane, float* weights, int32_t* a_first, int32_t* a_count, int32_t* b_count);
 
 /*
  * The learned surrogate (no counterpart in the reference): a 3D convolutional operator that

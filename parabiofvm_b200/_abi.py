@@ -75,6 +75,8 @@ SIGNATURES = {
     "bfvm_slab_gradient_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
     "bfvm_slab_coefficients": (c_int, [c_int32, c_int32, c_int32, c_float, P(c_float), P(c_float), c_int32,
                                        P(c_int32), P(c_float)]),
+    "bfvm_slab_reduce_weights": (c_int, [c_int32, c_int32, c_int32, c_float, P(c_float), P(c_float), c_int32,
+                                         c_int32, P(c_float), P(c_int32), P(c_int32), P(c_int32)]),
     "bfvm_sur_create": (c_int, [P(c_void_p), c_int, P(c_int32), c_int32, c_int32, ctypes.c_uint64]),
     "bfvm_sur_destroy": (c_int, [c_void_p]),
     "bfvm_sur_set_stream": (c_int, [c_void_p, c_void_p]),

@@ -197,6 +197,27 @@ int bfvm_slab_coefficients(int32_t planes, int32_t voxel_z, int32_t substrates, 
 	return BFVM_OK;
 }
 
+int bfvm_slab_reduce_weights(int32_t planes, int32_t voxel_z, int32_t substrates, float time_step,
+							 const float* diffusion_coefficients, const float* decay_rates, int32_t first_plane,
+							 int32_t end_plane, float* weights, int32_t* a_first, int32_t* a_count, int32_t* b_count)
+{
+	if (planes < 2 || voxel_z <= 0 || substrates < 1 || !diffusion_coefficients || !decay_rates || !weights || !a_first
+		|| !a_count || !b_count)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "bad mesh, substrate or output arguments");
+	if (first_plane < 0 || end_plane <= first_plane || end_plane > planes)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "the slab's planes must lie within the mesh");
+	std::vector<float> bp, ep, g, G, c, gq, Gp, w;
+	int P, bl, ex, af, na, nb;
+	precompute_axis(planes, voxel_z, 3, substrates, time_step, diffusion_coefficients, decay_rates, 32, bp, ep, g, G,
+					c, gq, Gp, P, bl, ex);
+	slab_reduce_weights(planes, first_plane, end_plane, substrates, bp, c, w, af, na, nb);
+	std::copy(w.begin(), w.end(), weights);
+	*a_first = af;
+	*a_count = na;
+	*b_count = nb;
+	return BFVM_OK;
+}
+
 int bfvm_slab_info(const bfvm_solver* s, int32_t* slab_count, int32_t* slab, int32_t* first_plane,
 				   int32_t* mesh_planes)
 {

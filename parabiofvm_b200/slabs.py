@@ -51,6 +51,21 @@ def slab_coefficients(planes, voxel_z, diffusion_coefficients, decay_rates, time
     return out
 
 
+def slab_reduce_weights(planes, voxel_z, diffusion_coefficients, decay_rates, time_step, first_plane, end_plane):
+    """The reduce pass's weights of the slab holding planes [first_plane, end_plane)
+    (bfvm_slab_reduce_weights; host only): the first plane of A's sum, A's weights [planes][S] and
+    B's weights [planes][S] (from the slab's first plane)."""
+    lib = _abi.load()
+    D = _f32(diffusion_coefficients)
+    lam = _f32(decay_rates, D.size)
+    w = np.zeros((2 * (end_plane - first_plane), D.size), np.float32)  # both sums may keep every plane
+    af, na, nb = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    check(lib.bfvm_slab_reduce_weights(int(planes), int(voxel_z), D.size, float(time_step), _fp(D), _fp(lam),
+                                       int(first_plane), int(end_plane), _fp(w), ctypes.byref(af), ctypes.byref(na),
+                                       ctypes.byref(nb)))
+    return int(af.value), w[:na.value].copy(), w[na.value:na.value + nb.value].copy()
+
+
 def agent_slabs(positions, bbox_min_z, voxel_z, bounds):
     """The slab of each agent, from its z position, by the float arithmetic the slab's own voxel
     lookup uses ((pos - slab min) / dz, truncated); -1 where no slab takes the agent."""

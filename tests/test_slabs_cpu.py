@@ -273,3 +273,68 @@ def test_create_slab_checks_its_arguments_before_the_device():
     assert create([0, 5, 9], 0) == (1, "slab_planes must run from 0 to the mesh's 10 z planes")
     assert create([0, 9, 10], 0)[0] == 1  # a slab of one plane
     assert create([0, 5, 10], 2)[0] == 1  # slab index out of range
+
+
+def _reduce_weights_f64(bp, c, n, i0, i1):
+    """float64 alpha and omega of every plane of the slab [i0, i1) (the linear forms of its zero-carry
+    A and B), from the recurrences of the Thomas solve."""
+    S = c.size
+    e = (c[None, :] * bp).astype(np.float32).astype(np.float64)  # e = c b', the float product
+    b = bp.astype(np.float64)
+    cc = c.astype(np.float64)
+    nl = i1 - i0
+    alpha = np.ones((nl, S))
+    for i in range(nl - 2, -1, -1):
+        alpha[i] = alpha[i + 1] * -e[i0 + i]
+    phi = np.empty((nl, S))
+    pr = np.ones(S)
+    for k in range(nl):
+        phi[k] = b[i0 + k] * pr
+        pr = pr * -cc * b[i0 + k]
+    omega = np.empty((nl, S))
+    omega[-1] = phi[-1]
+    for i in range(nl - 2, -1, -1):
+        omega[i] = phi[i] - e[i0 + i] * omega[i + 1]
+    return alpha, omega
+
+
+@pytest.mark.parametrize("D,bounds", [
+    ([1000.0, 20000.0, 50.0], [0, 37, 70, 100]),
+    ([1e5, 2e5, 1e3, 10.0], [0, 45, 100]),
+    ([1e6, 3e6], [0, 20, 60, 100]),  # slow decay: every plane kept
+])
+def test_reduce_weights_give_the_zero_carry_values(D, bounds):
+    """bfvm_slab_reduce_weights (host code of the reduce pass): the weights match the float64 linear
+    forms, the planes left out weigh at most 2^-50 together, and the weighted sums give the slab's
+    zero-carry A and B."""
+    from parabiofvm_b200.slabs import slab_reduce_weights
+
+    n, h, dt = 100, 20, 0.01
+    lam = [0.1] * len(D)
+    bp, c = thomas_coefficients(n, h, 3, dt, D, lam)
+    d = np.random.default_rng(len(D)).uniform(0, 1, (n, 6 * len(D)))
+    for k in range(len(bounds) - 1):
+        i0, i1 = bounds[k], bounds[k + 1]
+        a_first, wa, wb = slab_reduce_weights(n, h, D, lam, dt, i0, i1)
+        alpha, omega = _reduce_weights_f64(bp, c, n, i0, i1)
+        if i1 == n:
+            assert wa.shape[0] == 0
+        else:
+            assert a_first + wa.shape[0] == i1
+            # float weights: relative rounding, and the smallest ones below float's normal range
+            np.testing.assert_allclose(wa, alpha[a_first - i0:], rtol=1e-6, atol=1e-30)
+            assert np.abs(alpha[:a_first - i0]).max(axis=1, initial=0).sum() <= 2.0 ** -50
+        if i0 == 0:
+            assert wb.shape[0] == 0
+        else:
+            nb = wb.shape[0]
+            np.testing.assert_allclose(wb, omega[:nb], rtol=1e-6, atol=1e-30)
+            assert np.abs(omega[nb:]).max(axis=1, initial=0).sum() <= 2.0 ** -50
+        x, f = slab_solve(d[i0:i1], bp, c, i0, i1)
+        L = d.shape[1]
+        if i1 < n:
+            A = np.einsum("kl,kl->l", expand(wa, L), d[a_first:i1])
+            np.testing.assert_allclose(A, f[-1], rtol=1e-6)
+        if i0 > 0:
+            B = np.einsum("kl,kl->l", expand(wb, L), d[i0:i0 + wb.shape[0]])
+            np.testing.assert_allclose(B, x[0], rtol=1e-6)
