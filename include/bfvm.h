@@ -152,6 +152,8 @@ int bfvm_release_internalized(bfvm_solver* s, int32_t index);
  * taking indices [stored, stored + count) with the values of the host arrays given (shapes as in
  * bfvm_store_agents, `count` rows each).  A NULL array leaves that quantity 0 for the new agents,
  * as add() does.  Only the new rows cross the host link; grown storage is copied on the device.
+ * If the storage cannot grow, the call returns BFVM_ERR_OUT_OF_MEMORY and the solver is left
+ * without agents, as after a failed bfvm_store_agents.
  *
  * bfvm_remove_agents: agent_data::remove (src/agent_data.cpp:27-53) of indices[0], then
  * indices[1], ... in that order, each moving the then-last agent into the freed slot.  Every index
