@@ -277,6 +277,18 @@ def step_parity(workload, steps):
     return {"workload": workload, "steps": steps, "checks": rows}
 
 
+def host_cpu_model():
+    """The host CPU's model name (the first 'model name' of /proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_oracle_rate(w, budget_s=20.0, max_steps=3):
     """Time the CPU oracle (all host threads) on the workload: voxel*substrate updates/s."""
     import oracle
@@ -340,7 +352,8 @@ def run_reference_batch(args, threads):
         "config": {"workload": "batch-256: 256 independent meshes, edge U{24..96}, 1..8 substrates, 100..20,000 "
                                "clustered agents, per-instance coefficients",
                    "implementation": "CPU restatement of src/solver/host (OpenMP, -O3, no FP contraction)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "cpu_model": host_cpu_model(), "kind": "port",
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -391,7 +404,8 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": {"workload": f"{args.workload}: {WORKLOADS[name]['text']}",
                    "implementation": "CPU restatement of src/solver/host (OpenMP, -O3, no FP contraction)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "cpu_model": host_cpu_model(), "kind": "port",
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -1011,7 +1025,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         rate, threads, times = cpu_oracle_rate(w, budget_s=args.cpu_budget_s)
-        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "cpu_model": host_cpu_model(), "kind": "port",
                "sample": f"{len(times)} full step(s) of the same workload on {threads} host threads "
                          f"({', '.join(f'{t:.2f}s' for t in times)})"}
 

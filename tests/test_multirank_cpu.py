@@ -82,6 +82,7 @@ def test_reference_arm_under_torchrun_prints_one_line():
     line = json.loads(lines[0])
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+    assert line["cpu_baseline"]["cpu_model"] is None or isinstance(line["cpu_baseline"]["cpu_model"], str)
     assert line["e2e"]["h2d_bytes_per_step"] == 0
 
 
