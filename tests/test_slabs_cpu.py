@@ -3,9 +3,10 @@ and the exchange protocol of parabiofvm_b200.slabs over gloo, checked against th
 whole z lines (src/solver/host/diffusion_solver.cpp:72-142, 416-480) and the central-difference z
 gradient (src/solver/host/gradient_solver.cpp:170-223).
 
-The slab arithmetic here is a float64 restatement of what the GPU passes do (the reduce pass, the
-combine recurrences, the solve pass with carries); the GPU passes themselves are checked against
-the single-solver step in tests/test_gpu_slabs.py.
+The slab arithmetic here is a float64 restatement of what the GPU passes do: the reduce pass as
+weighted sums with the library's weights (bfvm_slab_reduce_weights), the combine recurrences, and
+the solve pass with carries.  The GPU passes themselves are checked against the single-solver step
+in tests/test_gpu_slabs.py.
 """
 
 import os
@@ -149,12 +150,15 @@ class RestatedSlab:
     def __init__(self, d, bounds, index):
         import torch
 
-        from parabiofvm_b200.slabs import slab_coefficients
+        from parabiofvm_b200.slabs import slab_coefficients, slab_reduce_weights
 
         self.bounds, self.index, self.count = bounds, index, len(bounds) - 1
         self.i0, self.i1 = bounds[index], bounds[index + 1]
         self.bp, self.c = thomas_coefficients(MESH["n"], MESH["h"], MESH["dims"], MESH["dt"], MESH["D"], MESH["lam"])
         self.coef = slab_coefficients(MESH["n"], MESH["h"], MESH["D"], MESH["lam"], MESH["dt"], bounds)
+        # the reduce pass as the GPU runs it: sums over the planes whose weights the library keeps
+        self.a_first, self.wa, self.wb = slab_reduce_weights(MESH["n"], MESH["h"], MESH["D"], MESH["lam"], MESH["dt"],
+                                                             self.i0, self.i1)
         self.u = np.array(d[self.i0:self.i1], np.float64)
         self.lines = d.shape[1]
         self.exchange = torch.zeros(2 * self.lines, dtype=torch.float32)
@@ -164,8 +168,10 @@ class RestatedSlab:
     def diffusion_begin(self):
         import torch
 
-        x, f = slab_solve(self.u, self.bp, self.c, self.i0, self.i1)
-        self.exchange.copy_(torch.from_numpy(np.concatenate([f[-1], x[0]]).astype(np.float32)))
+        L = self.lines
+        A = np.einsum("kl,kl->l", expand(self.wa, L), self.u[self.a_first - self.i0:]) if len(self.wa) else np.zeros(L)
+        B = np.einsum("kl,kl->l", expand(self.wb, L), self.u[:len(self.wb)]) if len(self.wb) else np.zeros(L)
+        self.exchange.copy_(torch.from_numpy(np.concatenate([A, B]).astype(np.float32)))
 
     def diffusion_end(self, gathered):
         g = gathered.numpy().astype(np.float64).reshape(self.count, 2, self.lines)
