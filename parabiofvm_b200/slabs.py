@@ -89,6 +89,8 @@ class Slab(Solver):
     z sweep's reduced system) and `edges` [2][lines] (its first and last plane), lines = X*Y*S.
     Its work runs on the torch stream `stream` (a new one if None); `step` enqueues the exchanges
     there too, so the slabs that one process holds share one stream.
+    Agents added or removed on a slab (add_agents, remove_agents) must lie in its planes; the
+    slab's `agent_index` (set by make_slab) is the caller's to keep in step with such changes.
     """
 
     def __init__(self, bbox_min, bbox_max, voxel_shape, diffusion_coefficients, decay_rates, time_step, bounds, slab,
