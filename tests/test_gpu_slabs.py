@@ -147,6 +147,7 @@ def test_whole_mesh_calls_are_refused_on_a_split_mesh():
     (100, [0, 37, 70, 100], [50.0, 1e3, 1e5, 1e6]),  # slow decay: the sums keep every plane
     (300, [0, 150, 300], [50.0, 1e3, 5e3, 1e4]),      # fast decay: the sums keep the edge planes
     (300, [0, 100, 200, 300], [1e3, 3e4, 1e5, 2e5]),
+    (120, [0, 50, 120], [1e3, 1e5]),                  # 2 substrates: the one-line-per-thread kernel
 ])
 def test_reduce_pass_publishes_the_zero_carry_solve(planes, bounds, D):
     """The exchange that bfvm_slab_diffusion_begin writes, A = the forward value at the slab's last
@@ -156,7 +157,7 @@ def test_reduce_pass_publishes_the_zero_carry_solve(planes, bounds, D):
     from parabiofvm_b200 import slabs as sl
     from test_slabs_cpu import slab_solve, thomas_coefficients
 
-    w = synthetic(8, 4, 0, seed=planes + len(bounds), boundary_substrate0=False)
+    w = synthetic(8, len(D), 0, seed=planes + len(bounds), boundary_substrate0=False)
     w.diffusion_coefficients = list(D)
     w.bbox_max = (w.bbox_max[0], w.bbox_max[1], planes * w.voxel_shape[2])
     w.densities = np.random.default_rng(planes).uniform(0, 1, w.voxel_count * w.S).astype(np.float32)
