@@ -62,3 +62,25 @@ def test_an_index_beyond_the_count_at_its_turn_is_refused():
         plan_agent_removal(5, [-1])
     with pytest.raises(BfvmError):
         plan_agent_removal(0, [0])
+
+
+def test_any_removal_sequence_matches_sequential_removal():
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @st.composite
+    def removals(draw):
+        agents = draw(st.integers(min_value=0, max_value=400))
+        k = draw(st.integers(min_value=0, max_value=agents))
+        idx, c = [], agents
+        for _ in range(k):
+            idx.append(draw(st.integers(min_value=0, max_value=c - 1)))
+            c -= 1
+        return agents, idx
+
+    @settings(max_examples=300, deadline=None)
+    @given(removals())
+    def check(case):
+        _check(*case)
+
+    check()
