@@ -129,6 +129,12 @@ public:
 
 } // namespace solvers::b200
 
+// the names the reference's device backends use (include/BioFVM/solver.h of the reference), for
+// code written against solvers::device::solver directly
+namespace solvers {
+namespace device = b200;
+}
+
 using solver = solvers::b200::solver;
 using cell_solver = solvers::b200::cell_solver;
 

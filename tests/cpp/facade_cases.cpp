@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "BioFVM/microenvironment.h"
@@ -22,6 +23,10 @@
 #include "BioFVM/solver.h"
 
 using namespace biofvm;
+
+// the reference's spellings of the solver types name the same classes
+static_assert(std::is_same_v<solvers::device::solver, biofvm::solver>);
+static_assert(std::is_same_v<solvers::device::cell_solver, biofvm::cell_solver>);
 
 static void print_array(const char* name, const real_t* p, std::size_t n, bool last = false)
 {
