@@ -22,7 +22,8 @@ microenvironment::microenvironment(cartesian_mesh mesh, index_t substrates_count
 	  substrate_densities(std::make_unique<real_t[]>((std::size_t)substrates_count * mesh.voxel_count())),
 	  gradients(std::make_unique<real_t[]>((std::size_t)mesh.dims * substrates_count * mesh.voxel_count())),
 	  dirichlet_interior_voxels_count(0),
-	  compute_internalized_substrates(false)
+	  compute_internalized_substrates(false),
+	  data_residency(solvers::data_residency::host)
 {
 	// every voxel starts at the initial conditions: [voxel][s]
 	const std::size_t V = mesh.voxel_count();
@@ -59,7 +60,8 @@ microenvironment::microenvironment(microenvironment&& o)
 	  supply_rate_func(std::move(o.supply_rate_func)),
 	  uptake_rate_func(std::move(o.uptake_rate_func)),
 	  supply_target_densities_func(std::move(o.supply_target_densities_func)),
-	  compute_internalized_substrates(o.compute_internalized_substrates)
+	  compute_internalized_substrates(o.compute_internalized_substrates),
+	  data_residency(o.data_residency)
 {
 	if (o.agents && o.agents->agents_count() > 0)
 		throw std::logic_error("a microenvironment that holds agents cannot be moved");

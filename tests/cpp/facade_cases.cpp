@@ -18,6 +18,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "BioFVM/agent_container_base.h"
 #include "BioFVM/microenvironment.h"
 #include "BioFVM/microenvironment_builder.h"
 #include "BioFVM/solver.h"
@@ -110,7 +111,8 @@ static int mode_host()
 				agents.agents_count(), moved->id, moved->index(), moved->volume());
 	print_array("moved_secretion", moved->secretion_rates(), 2);
 	const auto vi = moved->voxel_index();
-	print_ints("moved_voxel", vi.data(), 3, true);
+	print_ints("moved_voxel", vi.data(), 3);
+	std::printf("\"host_resident\": %d", (int)(m.data_residency == solvers::data_residency::host));
 	std::printf("}\n");
 	return 0;
 }

@@ -60,6 +60,7 @@ def test_host_behaviour(program):
     assert out["agents"] == 3 and out["moved_id"] == 3 and out["moved_index"] == 1
     assert out["moved_volume"] == 103 and out["moved_secretion"] == [3, 13]
     assert out["moved_voxel"] == [1, 0, 0]
+    assert out["host_resident"] == 1  # microenvironment::data_residency starts at host
 
 
 @pytest.mark.gpu
