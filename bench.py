@@ -415,6 +415,10 @@ def run_reference(args):
 BATCH_INSTANCES = 256
 
 
+BATCH_TEXT = ("256 independent meshes, edge U{24..96}, 1..8 substrates, 100..20,000 clustered agents, "
+              "per-instance coefficients, recompute every 10th step")
+
+
 def make_batch(seed=20261204, count=BATCH_INSTANCES):
     """The ensemble of the batch-256 workload: per instance a cubic mesh of edge U{24..96},
     U{1..8} substrates and U{100..20000} clustered agents, each with its own coefficients."""
@@ -430,8 +434,12 @@ def make_batch(seed=20261204, count=BATCH_INSTANCES):
     return ws
 
 
-def run_batch(args):
-    """The batched-ensemble workload on one GPU: batched (one graph) and sequential (one stream)."""
+def measure_batch(steps, warmup, clocks=True):
+    """The batched-ensemble workload on one GPU.  Two copies of every instance are made: one set is
+    stepped as a batch (one graph per step), the other one instance after another on one stream
+    (bfvm_run_steps), over the same steps from the same state.  Returns the two device times, the
+    launches of the batched steps and the largest relative L2 distance between an instance's two
+    fields."""
     import torch
 
     from parabiofvm_b200 import Batch
@@ -442,8 +450,9 @@ def run_batch(args):
     units = sum(w.voxel_count * w.S for w in ws)
     log(f"batch: {len(ws)} instances, {units / 1e6:.1f} M voxel*substrates, built in "
         f"{time.perf_counter() - t_setup:.1f}s")
-    solvers = [make_solver(w) for w in ws]
     stream = torch.cuda.Stream()
+    batched = [make_solver(w) for w in ws]
+    alone = [make_solver(w) for w in ws]
 
     def timed(run):
         torch.cuda.synchronize()
@@ -455,49 +464,59 @@ def run_batch(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    # batched: the batch's own stream, ordered after / before `stream` through the solvers
-    for s in solvers:
+    for s in batched + alone:
         s.set_stream(stream.cuda_stream)
-    b = Batch(solvers)
-    b.run_steps(args.warmup, 0)
+    b = Batch(batched)
+    b.run_steps(warmup, 0)
     b.synchronize()
-    sampler = ClockSampler(physical_gpu_index(0))
-    sampler.start()
-    time.sleep(1.0)
-    launches0 = sum(s.launch_count for s in solvers)
-    ms_batch = timed(lambda: b.run_steps(args.steps, args.warmup))
-    launches = sum(s.launch_count for s in solvers) - launches0
-    clocks = sampler.stop()
+    sampler = ClockSampler(physical_gpu_index(0)) if clocks else None
+    if sampler:
+        sampler.start()
+        time.sleep(1.0)
+    launches0 = sum(s.launch_count for s in batched)
+    ms_batch = timed(lambda: b.run_steps(steps, warmup))
+    launches = sum(s.launch_count for s in batched) - launches0
+    clock_rec = sampler.stop() if sampler else None
     b.close()
 
-    # sequential: the same instances, one after another on one stream
+    # one instance after another: the same warm-up steps untimed, then the same steps timed
+    for k in range(warmup):
+        for s in alone:
+            s.run_steps(1, k)
+
     def sequential():
-        for k in range(args.steps):
-            for s in solvers:
-                s.run_steps(1, args.warmup + args.steps + k)
+        for k in range(steps):
+            for s in alone:
+                s.run_steps(1, warmup + k)
 
-    for s in solvers:
-        s.run_steps(1, 1)  # graphs of both step kinds exist before timing
-        s.run_steps(1, 10)
     ms_seq = timed(sequential)
-    for s in solvers:
+    worst = 0.0
+    for sb, sa in zip(batched, alone):
+        worst = max(worst, _rel_l2(sb.load_densities(), sa.load_densities()))
+    for s in batched + alone:
         s.close()
+    return {"instances": len(ws), "voxel_substrates": units, "ms_batch": ms_batch, "ms_sequential": ms_seq,
+            "launches": launches, "clocks": clock_rec, "max_rel_l2_vs_alone": worst}
 
-    value = units * args.steps / (ms_batch / 1e3)
-    seq = units * args.steps / (ms_seq / 1e3)
+
+def run_batch(args):
+    """The batched-ensemble workload on one GPU: batched (one graph) and sequential (one stream)."""
+    r = measure_batch(args.steps, args.warmup)
+    units = r["voxel_substrates"]
+    value = units * args.steps / (r["ms_batch"] / 1e3)
+    seq = units * args.steps / (r["ms_sequential"] / 1e3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_batch / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": r["ms_batch"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": f"batch-256: {len(ws)} independent meshes, edge U{{24..96}}, 1..8 substrates, "
-                               "100..20,000 clustered agents, per-instance coefficients, recompute every 10th step",
-                   "instances": len(ws), "voxel_substrates": units,
+        "config": {"workload": f"batch-256: {BATCH_TEXT}", "instances": r["instances"], "voxel_substrates": units,
                    "l2": "ensemble fields 4x the L2, no flush"},
-        "sequential": {"value": seq, "ms_per_step": ms_seq / args.steps,
+        "sequential": {"value": seq, "ms_per_step": r["ms_sequential"] / args.steps,
                        "what": "the same instances stepped one after another on one stream (bfvm_run_steps)"},
         "speedup_vs_sequential": value / seq,
-        "gpu_launches": launches,
-        "clocks": clocks,
+        "max_rel_l2_vs_alone": r["max_rel_l2_vs_alone"],
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -535,9 +554,17 @@ SURROGATE_TEXT = ("128^3 voxels (dx 20 um) x 4 FP32 substrates; network: 3x3x3 c
                   "steps, every 8th re-run plain, plain takes over above 1e-3 relative L2")
 
 
-def run_surrogate(args):
-    """The learned surrogate at 128^3 x 4: training throughput, one convolution against the tensor
-    peak, a macro-step against 16 plain steps, and the fallback controller over 1,600 steps."""
+def measure_surrogate(train_steps=10, warmup=3, fallback_macro_steps=100, fresh_train_steps=0):
+    """The learned surrogate at 128^3 x 4.
+
+    - Training throughput: Adam steps at batch 4 on one batch of pairs from the plain solver
+      (device-timed, no loss read-back), on a network of its own.
+    - One forward convolution at batch 4 against the tensor peak (the roofline numerator).
+    - One macro-step of the trained network (the committed parameters, trained by
+      parabiofvm_b200.surrogate_train) against 16 plain steps with 200,000 clustered agents.
+    - The fallback controller over 1,600 steps with the trained network, against plain stepping.
+    Without committed parameters the controller's network gets `fresh_train_steps` Adam steps on
+    fresh pairs instead."""
     import ctypes
 
     import torch
@@ -546,12 +573,8 @@ def run_surrogate(args):
     from parabiofvm_b200 import surrogate as su
 
     torch.cuda.set_device(0)
-    rng = np.random.default_rng(20261205)
-    S = 4
-    env = su.Microenvironment((128, 128, 128), 20, list(np.exp(rng.uniform(np.log(1e3), np.log(1e5), S))),
-                              list(rng.uniform(0.01, 1.0, S)), 0.01)
-    if args.conv_only:
-        return surrogate_conv_only(args, env)
+    env = su.standard_environment()
+    S = env.S
     B = 4
     net = su.Surrogate(env.grid, S, max_batch=B, seed=7)
     gen = su.PairGenerator(env, seed=11)
@@ -570,8 +593,7 @@ def run_surrogate(args):
 
     # training steps on that batch (device-timed; no loss read-back inside the timed region)
     net.stream.wait_stream(gen.stream)
-    train_steps = max(args.steps, 3)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         net.train_step(field, src, sink, target, pred, 1e-3, read_loss=False)
     net.synchronize()
     e0, e1 = events()
@@ -584,8 +606,18 @@ def run_surrogate(args):
     conv_flop = 2.0 * 27 * 32 * 32 * env.voxels * B
     train_flop = conv_flop * (10 + 9 + 10)  # forward, input gradients (not of layer 0), weight gradients
 
-    # a little training on fresh pairs, so the controller below runs a network that has learned
-    losses = su.train(net, gen, steps=args.surrogate_train_steps, batch=B, learning_rate=1e-3)
+    # the network the controller runs: the committed trained parameters, else a short training
+    run_net = su.Surrogate(env.grid, S, max_batch=1, seed=7, stream=net.stream)
+    trained = None
+    if os.path.exists(su.WEIGHTS_PATH):
+        rec = su.load_trained(run_net, env)
+        trained = {"parameters": os.path.relpath(su.WEIGHTS_PATH, ROOT), "best_epoch": rec["best_epoch"],
+                   "training_steps": rec["best_epoch"] * (rec["recipe"]["pairs"] // rec["recipe"]["batch"]),
+                   "pairs": rec["recipe"]["pairs"], "held_out_rel_l2": rec["held_out_rel_l2"],
+                   "held_out_rel_l2_without_net": rec["held_out_rel_l2_without_net"]}
+    else:
+        losses = su.train(run_net, gen, steps=fresh_train_steps, batch=1, learning_rate=1e-3)
+        trained = {"parameters": None, "training_steps": len(losses)}
 
     # one forward convolution at batch 4: the roofline numerator
     lib = _abi.load()
@@ -613,6 +645,7 @@ def run_surrogate(args):
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     ms_conv = e0.elapsed_time(e1) / reps
+    del xin, w, yout
     peak, peak_kind = measured_tensor_peak()
     achieved = conv_flop / (ms_conv / 1e3) / 1e12
 
@@ -636,52 +669,70 @@ def run_surrogate(args):
     with torch.cuda.stream(net.stream):
         out1 = torch.empty_like(f1)
     for _ in range(3):
-        net.infer(f1, src[0], sink[0], out1)
-    net.synchronize()
+        run_net.infer(f1, src[0], sink[0], out1)
+    run_net.synchronize()
     e0, e1 = events()
     e0.record(net.stream)
     for _ in range(10):
-        net.infer(f1, src[0], sink[0], out1)
+        run_net.infer(f1, src[0], sink[0], out1)
     e1.record(net.stream)
-    net.synchronize()
+    run_net.synchronize()
     ms_macro = e0.elapsed_time(e1) / 10
 
-    # the controller over 1,600 steps
+    # the controller over 1,600 steps, from a field of the training distribution
     run_field = f1.clone()
-    report = su.run_with_fallback(net, env, run_field, agents, macro_steps=100, check_every=8, tolerance=1e-3)
+    report = su.run_with_fallback(run_net, env, run_field, agents, macro_steps=fallback_macro_steps, check_every=8,
+                                  tolerance=1e-3)
     s = env.solver()
     s.store_agents(agents["sec"], agents["sat"], agents["upt"], agents["nex"], np.zeros_like(agents["sec"]), None,
                    agents["vol"], agents["pos"])
     s.store_densities_device(f1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s.run_steps(1600, 0)
+    s.run_steps(16 * fallback_macro_steps, 0)
     s.synchronize()
     plain_s = time.perf_counter() - t0
     plain_field = torch.empty_like(f1)
     s.load_densities_device(plain_field)
     s.synchronize()
     s.close()
+    run_net.close()
     net.close()
     gen.close()
-
-    line = {
-        "metric": METRIC, "value": VS * 16 / (ms_macro / 1e3), "unit": UNIT, "n_gpus": 1, "steps": 10,
-        "warmup": 3, "ms_per_step": ms_macro, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16 weights/activations, f32 accumulate", "data": "synthetic (seeded)",
-        "config": {"workload": f"surrogate-128: {SURROGATE_TEXT}", "l2": "activations 4x the L2 at batch 4"},
-        "macro_step": {"ms": ms_macro, "plain_16_steps_ms": ms_plain16, "speedup_vs_plain": ms_plain16 / ms_macro},
-        "training": {"ms_per_step_batch4": ms_train, "tflops": train_flop / (ms_train / 1e3) / 1e12,
-                     "pairs_per_s_generated": 1.0 / pair_s, "steps_on_fresh_pairs": len(losses),
-                     "loss_first": losses[0] if losses else None, "loss_last": losses[-1] if losses else None},
-        "roofline": {"bound": "tensor", "kernel": "sur_conv_kernel (forward, batch 4)", "achieved": achieved,
-                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": None, "ms": ms_conv},
+    return {
+        "VS": VS, "ms_macro": ms_macro, "ms_plain16": ms_plain16, "ms_train": ms_train,
+        "train_tflops": train_flop / (ms_train / 1e3) / 1e12, "pairs_per_s": 1.0 / pair_s, "trained": trained,
+        "ms_conv": ms_conv, "conv_tflops": achieved, "peak": peak, "peak_kind": peak_kind,
         "fallback_run": {"macro_steps": report.macro_steps, "surrogate_macro_steps": report.surrogate_steps,
                          "checks": [[m, e] for m, e in report.checks], "fell_back_at": report.fell_back_at,
                          "seconds": report.seconds, "plain_seconds": plain_s,
                          "speedup_vs_plain": plain_s / report.seconds,
                          "rel_l2_vs_plain": su.rel_l2(run_field, plain_field)},
+    }
+
+
+def run_surrogate(args):
+    """The learned surrogate at 128^3 x 4: training throughput, one convolution against the tensor
+    peak, a macro-step against 16 plain steps, and the fallback controller over 1,600 steps."""
+    if args.conv_only:
+        from parabiofvm_b200 import surrogate as su
+
+        return surrogate_conv_only(args, su.standard_environment())
+    r = measure_surrogate(train_steps=max(args.steps, 3), warmup=args.warmup,
+                          fresh_train_steps=args.surrogate_train_steps)
+    line = {
+        "metric": METRIC, "value": r["VS"] * 16 / (r["ms_macro"] / 1e3), "unit": UNIT, "n_gpus": 1, "steps": 10,
+        "warmup": 3, "ms_per_step": r["ms_macro"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 weights/activations, f32 accumulate", "data": "synthetic (seeded)",
+        "config": {"workload": f"surrogate-128: {SURROGATE_TEXT}", "l2": "activations 4x the L2 at batch 4"},
+        "macro_step": {"ms": r["ms_macro"], "plain_16_steps_ms": r["ms_plain16"],
+                       "speedup_vs_plain": r["ms_plain16"] / r["ms_macro"]},
+        "training": {"ms_per_step_batch4": r["ms_train"], "tflops": r["train_tflops"],
+                     "pairs_per_s_generated": r["pairs_per_s"], "network": r["trained"]},
+        "roofline": {"bound": "tensor", "kernel": "sur_conv_kernel (forward, batch 4)", "achieved": r["conv_tflops"],
+                     "peak": r["peak"], "unit": "TFLOP/s", "frac": r["conv_tflops"] / r["peak"],
+                     "peak_kind": r["peak_kind"], "traffic": None, "ms": r["ms_conv"]},
+        "fallback_run": r["fallback_run"],
         "gpu_launches": None,
     }
     print(json.dumps(line), flush=True)
@@ -1035,6 +1086,12 @@ def run_ours(args):
         parity = [parity_report(args.workload, 1, with_fp64=False), parity_report("plain-50", 100, with_fp64=True)]
         log(f"parity checks took {time.perf_counter() - t_par:.1f}s")
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.skip_extras:
+        t_ex = time.perf_counter()
+        extras = side_forms()
+        log(f"batch and surrogate measurements took {time.perf_counter() - t_ex:.1f}s")
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -1060,9 +1117,38 @@ def run_ours(args):
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks,
+        **extras,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def side_forms():
+    """The two forms that stand beside the plain step, measured briefly on the same GPU after it:
+    ``batch_256`` (10 batched steps against the same instances stepped alone) and ``surrogate_128``
+    (a macro-step of the trained network against 16 plain steps, the convolution against the tensor
+    peak, and the fallback controller over 1,600 steps)."""
+    out = {}
+    b = measure_batch(10, 3, clocks=False)
+    units = b["voxel_substrates"]
+    out["batch_256"] = {
+        "workload": f"batch-256: {BATCH_TEXT}", "steps": 10, "warmup": 3,
+        "ms_per_step": b["ms_batch"] / 10, "value": units * 10 / (b["ms_batch"] / 1e3), "unit": UNIT,
+        "sequential_ms_per_step": b["ms_sequential"] / 10,
+        "speedup_vs_sequential": b["ms_sequential"] / b["ms_batch"],
+        "max_rel_l2_vs_alone": b["max_rel_l2_vs_alone"], "gpu_launches": b["launches"]}
+    r = measure_surrogate(train_steps=5, warmup=3)
+    fb = r["fallback_run"]
+    out["surrogate_128"] = {
+        "workload": f"surrogate-128: {SURROGATE_TEXT}",
+        "macro_step_ms": r["ms_macro"], "plain_16_steps_ms": r["ms_plain16"],
+        "macro_step_speedup_vs_plain": r["ms_plain16"] / r["ms_macro"],
+        "conv_tflops": r["conv_tflops"], "conv_frac_of_peak": r["conv_tflops"] / r["peak"], "peak_kind": r["peak_kind"],
+        "train_step_ms_batch4": r["ms_train"], "network": r["trained"],
+        "controller": {"macro_steps": fb["macro_steps"], "surrogate_macro_steps": fb["surrogate_macro_steps"],
+                       "checked_rel_l2": fb["checks"], "fell_back_at": fb["fell_back_at"],
+                       "speedup_vs_plain": fb["speedup_vs_plain"], "rel_l2_vs_plain": fb["rel_l2_vs_plain"]}}
+    return out
 
 
 def main():
@@ -1093,6 +1179,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-parity", action="store_true",
                     help="leave out the oracle comparisons (one full-size step, 100 steps of plain-50)")
+    ap.add_argument("--skip-extras", action="store_true",
+                    help="leave out the brief batch-256 and surrogate-128 measurements of the default line")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     args = ap.parse_args()

@@ -378,14 +378,16 @@ int bfvm_sur_conv3d_wgrad(const int32_t shape[4], const void* input, const void*
  * [agent_count], positions [agent_count][dims].  The mesh is given as in bfvm_create by its
  * minimum corner and voxel shape, plus grid_shape (1 along unused axes).  Work is enqueued on
  * `stream` (a cudaStream_t; NULL is the legacy default stream) and the call returns without
- * waiting.  An agent outside the mesh is skipped and sets bit 1 of *error_flags (device int) when
- * error_flags is not NULL.
+ * waiting.  An agent outside the mesh is skipped and sets the value 1 (bit 0) in *error_flags
+ * (device int) when error_flags is not NULL.
  *
  * Its scratch memory is one static device array of BFVM_NOALLOC_SCRATCH_BYTES (about 8 MB), held
  * by every GPU that loads the library until the process exits; the call rejects more than
  * BFVM_NOALLOC_MAX_AGENTS agents or more than BFVM_NOALLOC_MAX_AGENT_SUBSTRATES agent x substrate
- * pairs with BFVM_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
+ * pairs with BFVM_ERR_INVALID_ARGUMENT.  A call outside stream capture looks up the array's device
+ * address (cudaGetSymbolAddress) and keeps it for calls made while `stream` is capturing, which
+ * reuse it: make the first call on each device before any capture (a call captured first returns
+ * BFVM_ERR_STATE), and after a device reset make one call outside capture again.  All calls share
  * the array, so calls that overlap on the GPU (other streams, other host threads) race: order
  * them on one stream.
  */

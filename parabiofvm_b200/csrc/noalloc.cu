@@ -39,9 +39,13 @@ static_assert(NA_TOTAL == BFVM_NOALLOC_SCRATCH_BYTES, "BFVM_NOALLOC_SCRATCH_BYTE
 
 static __device__ __align__(256) unsigned char noalloc_scratch[NA_TOTAL];
 
-// Device address of noalloc_scratch on the current device, looked up once per device.  In host
-// code the name noalloc_scratch is a host-side stand-in, not a device address.
-static int scratch_address(unsigned char** out)
+// Device address of noalloc_scratch on the current device.  In host code the name noalloc_scratch
+// is a host-side stand-in, not a device address.  Outside stream capture the address is looked up
+// on every call (cheap), so a device reset or a re-created primary context, which may move the
+// array, never leaves a stale address behind; the last address found on each device is kept for
+// calls made while `stream` is capturing, where the lookup (which may load the module) is not
+// allowed.  So the first call on a device must come before any capture.
+static int scratch_address(cudaStream_t stream, unsigned char** out)
 {
 	static std::mutex lock;
 	static void* addr[64] = {};
@@ -49,8 +53,14 @@ static int scratch_address(unsigned char** out)
 	BFVM_CUDA(cudaGetDevice(&dev));
 	if (dev < 0 || dev >= 64)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "device index beyond 63");
+	cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+	if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess)
+	{
+		(void)cudaGetLastError();
+		capture = cudaStreamCaptureStatusActive; // cannot tell: do not risk a lookup during a capture
+	}
 	std::lock_guard<std::mutex> guard(lock);
-	if (!addr[dev])
+	if (capture == cudaStreamCaptureStatusNone)
 	{
 		void* p = nullptr;
 		cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
@@ -58,6 +68,9 @@ static int scratch_address(unsigned char** out)
 			return cuda_fail(e, "cudaGetSymbolAddress(noalloc_scratch)");
 		addr[dev] = p;
 	}
+	else if (!addr[dev])
+		return fail(BFVM_ERR_STATE, "the first bfvm_secretion_solve_noalloc call on a device must come before any "
+									"stream capture");
 	*out = static_cast<unsigned char*>(addr[dev]);
 	return BFVM_OK;
 }
@@ -110,11 +123,11 @@ extern "C" int bfvm_secretion_solve_noalloc(float* densities, int dims, const in
 	if (!secretion_rates || !saturation_densities || !uptake_rates || !net_export_rates || !volumes || !positions)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "the agent arrays are required");
 
+	cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
 	unsigned char* base = nullptr;
-	int st = scratch_address(&base);
+	int st = scratch_address(stream, &base);
 	if (st)
 		return st;
-	cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
 	int* counts = reinterpret_cast<int*>(base + NA_COUNTS);
 	int* err = error_flags ? error_flags : reinterpret_cast<int*>(base + NA_FLAGWORD);
 	unsigned int* keys = reinterpret_cast<unsigned int*>(base + NA_KEYS);

@@ -18,6 +18,8 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import json
+import os
 import time
 
 import numpy as np
@@ -156,6 +158,37 @@ class Microenvironment:
                       self.diffusion_coefficients, self.decay_rates, self.time_step, device=device)
 
 
+STANDARD_SEED = 20261205
+WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "surrogate_128x4.npz")
+
+
+def standard_environment(seed=STANDARD_SEED):
+    """The 128^3 x 4 microenvironment the surrogate is trained and measured on: dx 20 um, dt 0.01
+    min, diffusion coefficients log-uniform in [1e3, 1e5] um^2/min and decay rates uniform in
+    [0.01, 1] /min, drawn from `seed`."""
+    rng = np.random.default_rng(seed)
+    S = 4
+    return Microenvironment((128, 128, 128), 20, [float(x) for x in np.exp(rng.uniform(np.log(1e3), np.log(1e5), S))],
+                            [float(x) for x in rng.uniform(0.01, 1.0, S)], 0.01)
+
+
+def load_trained(net, env, path=WEIGHTS_PATH):
+    """Load the trained parameters of `path` into `net` after checking that they were trained for
+    `env` (grid, voxel size, time step and coefficients).  Returns the file's training record."""
+    with np.load(path) as f:
+        params = f["parameters"]
+        record = json.loads(str(f["record"]))
+    want = {"grid": list(env.grid), "dx": env.dx, "time_step": env.time_step,
+            "diffusion_coefficients": env.diffusion_coefficients, "decay_rates": env.decay_rates}
+    got = record["environment"]
+    if (got["grid"] != want["grid"] or got["dx"] != want["dx"] or not np.isclose(got["time_step"], want["time_step"])
+            or not np.allclose(got["diffusion_coefficients"], want["diffusion_coefficients"], rtol=1e-6)
+            or not np.allclose(got["decay_rates"], want["decay_rates"], rtol=1e-6)):
+        raise ValueError(f"{path} was trained for another microenvironment: {got}")
+    net.load(params)
+    return record
+
+
 def random_agents(env, rng, count, clustered=False):
     """Agents with the plain workloads' distributions: volume 1000, secretion U(0,10), saturation
     U(0,1), uptake U(0,1), net export 0; uniform or in 16 Gaussian clusters."""
@@ -173,12 +206,18 @@ def random_agents(env, rng, count, clustered=False):
 
 
 class PairGenerator:
-    """Training pairs from the plain solver: (field, sources, sinks) -> the field 16 steps later."""
+    """Training pairs from the plain solver: (field, sources, sinks) -> the field 16 steps later.
+
+    ``fill`` draws a fresh pair from the generator's own sequence; ``fill(..., pair=k)`` makes pair
+    k of a fixed data set instead: its field and agents come from a generator seeded with
+    (seed, k), and the plain solver is deterministic, so the same k gives the same pair every time
+    (a data set of any size costs no memory, only the time to regenerate it)."""
 
     def __init__(self, env, seed=0, agents=(10_000, 100_000), device=0, stream=None):
         import torch
 
         self.env = env
+        self.seed = int(seed)
         self.rng = np.random.default_rng(seed)
         self.agents = agents
         self.stream = stream if stream is not None else torch.cuda.Stream()
@@ -189,15 +228,17 @@ class PairGenerator:
     def close(self):
         self.solver.close()
 
-    def fill(self, field, sources, sinks, target):
-        """One pair into views of [voxels][S] of device tensors."""
+    def fill(self, field, sources, sinks, target, pair=None):
+        """One pair into views of [voxels][S] of device tensors: pair `pair` of the fixed data set,
+        or the next fresh pair when `pair` is None."""
         import torch
 
         env = self.env
+        rng = self.rng if pair is None else np.random.default_rng((self.seed, int(pair)))
         with torch.cuda.stream(self.stream):
-            random_field(env.grid, env.S, self.rng, field, self.stream)
-            count = int(self.rng.integers(self.agents[0], self.agents[1] + 1))
-            a = random_agents(env, self.rng, count)
+            random_field(env.grid, env.S, rng, field, self.stream)
+            count = int(rng.integers(self.agents[0], self.agents[1] + 1))
+            a = random_agents(env, rng, count)
             dev = {k: torch.from_numpy(np.ascontiguousarray(v, np.float32)).to(self.device, non_blocking=False)
                    for k, v in a.items()}
             agent_rates((0, 0, 0), (env.dx,) * 3, env.grid, env.time_step, dev, sources, sinks, self.stream)
@@ -208,9 +249,9 @@ class PairGenerator:
             self.solver.load_densities_device(target)
             self._keep = dev  # the agent tensors stay alive until the stream has used them
 
-    def batch(self, field, sources, sinks, target):
+    def batch(self, field, sources, sinks, target, pairs=None):
         for b in range(field.shape[0]):
-            self.fill(field[b], sources[b], sinks[b], target[b])
+            self.fill(field[b], sources[b], sinks[b], target[b], None if pairs is None else pairs[b])
 
 
 def train(net, gen, steps, batch=4, learning_rate=1e-3, log_every=0, log=print):
@@ -231,6 +272,60 @@ def train(net, gen, steps, batch=4, learning_rate=1e-3, log_every=0, log=print):
         if log_every and (it + 1) % log_every == 0:
             log(f"surrogate step {it + 1}: loss {losses[-1]:.3e}")
     return losses
+
+
+def train_on_pairs(net, gen, pairs, epochs, batch=4, learning_rate=1e-3, held_out=(), seed=0, log=None):
+    """Adam on a fixed data set: pairs 0..pairs-1 of `gen`, `epochs` passes in a shuffled order,
+    `batch` pairs per step.  After every epoch the network is evaluated on the pairs listed in
+    `held_out` (indices outside the training set).  Returns a list of per-epoch dicts: mean loss,
+    and on the held-out pairs the network's mean relative L2 error against the plain solver next to
+    that of the field itself (the macro-step without a network)."""
+    import torch
+
+    env = gen.env
+    shape = (batch, env.voxels * env.S)
+    with torch.cuda.stream(net.stream):
+        field, src, sink, target, pred = [torch.empty(shape, dtype=torch.float32, device=gen.device)
+                                          for _ in range(5)]
+    order_rng = np.random.default_rng(seed)
+    curve = []
+    t0 = time.perf_counter()
+    for epoch in range(epochs):
+        order = order_rng.permutation(pairs)
+        losses = []
+        for i in range(0, pairs - batch + 1, batch):
+            gen.batch(field, src, sink, target, pairs=order[i:i + batch])
+            net.stream.wait_stream(gen.stream)
+            losses.append(net.train_step(field, src, sink, target, pred, learning_rate))
+            gen.stream.wait_stream(net.stream)
+        net_err, none_err = evaluate(net, gen, held_out) if len(held_out) else (None, None)
+        curve.append({"epoch": epoch + 1, "steps": (epoch + 1) * (pairs // batch), "loss_mean": float(np.mean(losses)),
+                      "loss_last": float(losses[-1]), "held_out_rel_l2": net_err, "held_out_rel_l2_without_net": none_err,
+                      "seconds": time.perf_counter() - t0})
+        if log:
+            log(json.dumps(curve[-1]))
+    return curve
+
+
+def evaluate(net, gen, pairs):
+    """Mean relative L2 error on the listed pairs of `gen`, of the network's prediction and of the
+    field itself, both against the plain solver's field 16 steps later."""
+    import torch
+
+    env = gen.env
+    with torch.cuda.stream(net.stream):
+        field, src, sink, target, pred = [torch.empty((1, env.voxels * env.S), dtype=torch.float32,
+                                                      device=gen.device) for _ in range(5)]
+    errs_net, errs_none = [], []
+    for k in pairs:
+        gen.batch(field, src, sink, target, pairs=[k])
+        net.stream.wait_stream(gen.stream)
+        net.infer(field, src, sink, pred)
+        net.synchronize()
+        errs_net.append(rel_l2(pred, target))
+        errs_none.append(rel_l2(field, target))
+        gen.stream.wait_stream(net.stream)
+    return float(np.mean(errs_net)), float(np.mean(errs_none))
 
 
 def rel_l2(a, b):

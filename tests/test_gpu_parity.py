@@ -48,7 +48,8 @@ def test_graph_steps_match_individual_calls():
 
 def test_cpu_runnable_config_100_steps():
     """50^3 voxels, 4 substrates, 5,000 uniform agents, Dirichlet 1.0 on substrate 0 at every
-    face, dt = 0.01, 100 steps: per-step and final error bounds against the FP32 oracle."""
+    face, dt = 0.01, 100 steps: the per-step bound (1e-5) after each of the first 10 steps and every
+    10th step after, and the final bound (1e-4) after step 100, against the FP32 oracle."""
     scn = synthetic(50, 4, 5000, seed=11, clustered=False)
     o32, g = _both(scn)
     o64 = make_oracle(scn, np.float64)
@@ -57,11 +58,11 @@ def test_cpu_runnable_config_100_steps():
         o32.run_steps(1, k)
         o64.run_steps(1, k)
         g.run_steps(1, k)
-        if k < 5 or k % 10 == 9:
+        if k < 10 or k % 10 == 9:
             e = rel_err(g.densities(), o32.densities())
             worst = max(worst, e)
-            if k == 0:
-                assert e < 1e-5, f"step 0 max rel err {e}"
+            # the per-step bar holds at every sampled step, not only the first
+            assert e < 1e-5, f"step {k} max rel err {e}"
     d = g.densities()
     e32 = rel_err(d, o32.densities())
     e64 = rel_err(d, o64.densities())

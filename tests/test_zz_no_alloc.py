@@ -4,8 +4,10 @@ Such callers (a host framework that owns every device allocation, a memory budge
 of time, code running while another library captures a stream) hand over their own device buffers;
 the entry point keeps its binning scratch in a static device array instead of allocating.  It runs
 the same kernels in the same order as bfvm_secretion_solve with recompute, so the checks below ask
-for the same bits as that entry point, on two calls in a row (the second call finds the first
-call's leftovers in the shared scratch array).
+for the same bits as that entry point and as the FP32 oracle, on calls in a row (each call finds
+the previous call's leftovers in the shared scratch array); they also check that a call changes
+the device's free memory by nothing and that a call can be captured in a CUDA graph in global
+capture mode, where an allocation would fail the capture.
 
 This file is named to be collected last: a failure here comes after every other test has run.
 """
@@ -37,18 +39,31 @@ def _call(lib, dens_ptr, w, grid, agents, dev, err_ptr, stream_ptr):
 @pytest.mark.gpu
 @pytest.mark.parametrize("edge,S,agents,internalized", [(40, 4, 6000, True), (24, 3, 2000, False)])
 def test_noalloc_matches_secretion_solve(edge, S, agents, internalized):
+    """Three recompute calls in a row on the caller's buffers, each checked bit for bit against
+    bfvm_secretion_solve and the first two against the FP32 oracle too.  The second call must leave
+    the device's free memory unchanged, and the third is captured in a CUDA graph in global capture
+    mode, where any allocation would end the capture with an error, then replayed."""
     import torch
+
+    from scenarios import make_oracle
 
     w = synthetic(edge, S, agents, seed=77 + edge, clustered=True, sigma=60.0, internalized=internalized)
     a = w.agents
 
-    # the existing entry point, two recompute calls in a row
+    # the existing entry point, three recompute calls in a row
     ref = make_solver(w)
     expect = []
-    for _ in range(2):
+    for _ in range(3):
         ref.secretion(True)
         expect.append((ref.load_densities().copy(), ref.load_internalized().copy() if internalized else None))
     ref.close()
+    # the oracle, two calls
+    o = make_oracle(w, np.float32)
+    oracle_expect = []
+    for _ in range(2):
+        o.secretion(True)
+        oracle_expect.append((o.densities().copy(), o.internalized().copy() if internalized else None))
+    o.close()
 
     # the no-alloc entry point on caller-owned buffers: the field of a second solver (no agents
     # stored there) and agent arrays the test allocates
@@ -70,17 +85,43 @@ def test_noalloc_matches_secretion_solve(edge, S, agents, internalized):
     }
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     torch.cuda.synchronize()
-
     lib = _abi.load()
-    for call in range(2):
-        _abi.check(_call(lib, dens_ptr, w, own.grid, a, dev, err.data_ptr(), stream.cuda_stream))
-        stream.synchronize()
+
+    def check(call):
         d = own.load_densities()
         np.testing.assert_array_equal(d, expect[call][0], err_msg=f"densities after call {call + 1}")
+        if call < 2:
+            np.testing.assert_array_equal(d, oracle_expect[call][0], err_msg=f"oracle densities, call {call + 1}")
         if internalized:
-            np.testing.assert_array_equal(dev["intern"].cpu().numpy().reshape(-1), expect[call][1].reshape(-1),
-                                          err_msg=f"internalized after call {call + 1}")
+            got = dev["intern"].cpu().numpy().reshape(-1)
+            np.testing.assert_array_equal(got, expect[call][1].reshape(-1), err_msg=f"internalized, call {call + 1}")
+            if call < 2:
+                np.testing.assert_array_equal(got, oracle_expect[call][1].reshape(-1),
+                                              err_msg=f"oracle internalized, call {call + 1}")
+
+    # call 1: eager
+    _abi.check(_call(lib, dens_ptr, w, own.grid, a, dev, err.data_ptr(), stream.cuda_stream))
+    stream.synchronize()
+    check(0)
+    # call 2: eager, with the device's free memory read on both sides
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    _abi.check(_call(lib, dens_ptr, w, own.grid, a, dev, err.data_ptr(), stream.cuda_stream))
+    stream.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert free_after == free_before, (free_before, free_after)
+    check(1)
+    # call 3: captured in global mode, then replayed once
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, capture_error_mode="global"):
+        _abi.check(_call(lib, dens_ptr, w, own.grid, a, dev, err.data_ptr(), torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    check(1)  # capturing ran nothing
+    graph.replay()
+    torch.cuda.synchronize()
+    check(2)
     assert int(err.item()) == 0
+    del graph
     own.close()
 
 
