@@ -184,9 +184,16 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step);
 int bfvm_synchronize(bfvm_solver* s);
 
 /*
- * Tuning options (no counterpart in the reference): "tma_sweeps" 0/1 stages sweep tiles through
- * shared memory with the TMA (default 1; 0 selects the kernels that read the field directly).
- * Results agree to rounding either way.
+ * Tuning options (no counterpart in the reference; they replace the reference's abort() on a
+ * device error, src/solver/device/CUDA/device_context.h:12-21, with a bounded wait and a status):
+ * - "tma_sweeps" 0/1 stages sweep tiles through shared memory with the TMA (default 1; 0 selects
+ *   the kernels that read the field directly).  Results agree to rounding either way.
+ * - "wait_limit_cycles" bounds every wait of the staged sweeps on a tile copy, in GPU clock cycles
+ *   (default 4e9, about two seconds; accepted range [1e4, 4e10]).  A wait that runs out makes the
+ *   kernel give up its tile, let its copies in flight land and return; the next synchronising call
+ *   returns BFVM_ERR_TIMEOUT, and the field is then not valid until it is stored again.
+ * - "test_drop_tile_copy" (tests of that bound only) names a staged-sweep tile whose stage barrier
+ *   is armed but whose copies are never issued, so its wait runs out; -1 (the default) turns it off.
  */
 int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value);
 

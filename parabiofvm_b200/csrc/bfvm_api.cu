@@ -1000,6 +1000,18 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 	const std::string n(name);
 	if (n == "tma_sweeps")
 		s->use_tma = value != 0;
+	else if (n == "wait_limit_cycles")
+	{
+		if (value < 10000 || value > 40000000000LL)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "wait_limit_cycles must lie in [1e4, 4e10]");
+		s->wait_limit_cycles = value;
+	}
+	else if (n == "test_drop_tile_copy")
+	{
+		if (value < -1)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "test_drop_tile_copy takes a tile index or -1");
+		s->drop_tile_copy = value;
+	}
 	else
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "unknown option " + n);
 	free_graphs(s);

@@ -145,6 +145,9 @@ struct bfvm_solver
 
 	long long launches = 0;
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
+	long long wait_limit_cycles = 4000000000LL; // bound of the staged sweeps' waits on tile copies (clock64 cycles;
+												// the default is the kernels' WAIT_LIMIT_CYCLES)
+	long long drop_tile_copy = -1;				// tests only: a staged-sweep tile whose copies are never issued
 	bfvm::sweep_tuning tune[3];	 // staged sweep launch shape per axis
 
 	// graphs for run_steps: [recompute]

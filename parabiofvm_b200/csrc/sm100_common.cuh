@@ -37,11 +37,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 	return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// Wait for the phase of `bar` with the given parity for at most `limit` cycles of clock64; false
+// when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = WAIT_LIMIT_CYCLES)
 {
 	const long long t0 = clock64();
 	while (!mbar_try_wait(bar, parity))
-		if (clock64() - t0 > WAIT_LIMIT_CYCLES)
+		if (clock64() - t0 > limit)
 			return false;
 	return true;
 }

@@ -206,6 +206,8 @@ static sweep_args make_args(bfvm_solver* st, int axis)
 	a.err = st->dev_error;
 	a.slab_carry = nullptr;
 	a.slab_lines = 0;
+	a.wait_limit = st->wait_limit_cycles;
+	a.drop_tile_copy = st->drop_tile_copy;
 	return a;
 }
 

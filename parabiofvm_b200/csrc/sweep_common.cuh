@@ -25,6 +25,11 @@ struct sweep_args
 	// for every other sweep
 	const float* slab_carry;
 	long long slab_lines;
+	// staged sweeps (sweep_tma.cu): the bound of every wait on a tile copy, in clock64 cycles; and,
+	// for tests of that bound only, a tile whose stage barrier is armed but whose copies are never
+	// issued (-1: none), so that the wait on it runs out
+	long long wait_limit;
+	long long drop_tile_copy;
 };
 
 __device__ __forceinline__ void block_range(int j, int base_len, int extra, int& p, int& L)
