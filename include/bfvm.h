@@ -188,6 +188,9 @@ int bfvm_synchronize(bfvm_solver* s);
  * device error, src/solver/device/CUDA/device_context.h:12-21, with a bounded wait and a status):
  * - "tma_sweeps" 0/1 stages sweep tiles through shared memory with the TMA (default 1; 0 selects
  *   the kernels that read the field directly).  Results agree to rounding either way.
+ * - "fused_dirichlet" 0/1: in the LOD step (bfvm_diffusion_solve, bfvm_run_steps) a staged sweep
+ *   writes the Dirichlet overwrite that follows it, tile by tile (default 1; 0 runs it as a
+ *   separate scatter).  Results are identical either way.
  * - "wait_limit_cycles" bounds every wait of the staged sweeps on a tile copy, in GPU clock cycles
  *   (default 4e9, about two seconds; accepted range [1e4, 4e10]).  A wait that runs out makes the
  *   kernel give up its tile, let its copies in flight land and return; the next synchronising call

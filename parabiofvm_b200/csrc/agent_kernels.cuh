@@ -47,7 +47,10 @@ __global__ void secrete_kernel(long long total, int S, float* __restrict__ dens,
 							   float voxel_volume);
 
 // One (voxel segment, substrate) pair of the secretion update; t < segments * S (secrete_kernel of
-// cell.cu, and the ensemble update of batch_kernels.cu).  See cell.cu for the formulas.
+// cell.cu, and the ensemble update of batch_kernels.cu).  See cell.cu for the formulas.  SORTED:
+// the per-agent rows num/den/fac/intern are in the binning's sorted order (row p is the agent at
+// sorted position p), otherwise in agent order (row order[p]).
+template <bool SORTED = false>
 __device__ __forceinline__ void secrete_element(long long t, int S, float* __restrict__ dens,
 												const int* __restrict__ counts, const int* __restrict__ seg_start,
 												const int* __restrict__ order, const unsigned int* __restrict__ keys,
@@ -70,7 +73,7 @@ __device__ __forceinline__ void secrete_element(long long t, int S, float* __res
 		if (!counts[2])
 		{
 			// compute_fused: the voxel holds this one agent
-			const size_t k = (size_t)order[b] * S + s;
+			const size_t k = (size_t)(SORTED ? b : order[b]) * S + s;
 			const float term = __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(__fsub_rn(1.f, rd), D), rn), rd), rf);
 			intern[k] = __fsub_rn(intern[k], __fmul_rn(voxel_volume, term));
 		}
@@ -80,7 +83,7 @@ __device__ __forceinline__ void secrete_element(long long t, int S, float* __res
 			const int e = seg_start[seg + 1];
 			for (int p = b; p < e; p++)
 			{
-				const size_t k = (size_t)order[p] * S + s;
+				const size_t k = (size_t)(SORTED ? p : order[p]) * S + s;
 				const float dk = den[k];
 				const float term =
 					__fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(-dk, D), num[k]), __fadd_rn(1.f, dk)), fac[k]);
@@ -94,7 +97,9 @@ __device__ __forceinline__ void secrete_element(long long t, int S, float* __res
 __global__ void __launch_bounds__(SCAN_THREADS) scan_tile_kernel(const int* in, int* out, long long n, int* tile_sums);
 __global__ void scan_add_kernel(int* out, long long n, const int* tile_offsets);
 
-int rebuild_bins(bfvm_solver* s); // cell.cu: keys, sort, segments, intermediates, reductions
+// cell.cu: keys, sort, segments, intermediates, reductions; `sorted`: also the sorted copies of the
+// per-agent terms (agent_state::snum ...), from which the reductions are then summed
+int rebuild_bins(bfvm_solver* s, bool sorted = false);
 
 // number of 8-bit radix passes for keys in [0, V] (V marks agents outside the mesh)
 inline int sort_passes(long long V)

@@ -30,6 +30,7 @@ struct bfvm_batch
 	std::vector<long long> epochs[2];	 // instance graph epochs when graph[rc] was captured
 	bfvm::ensemble_plan ens[2];			 // descriptors of the ensemble meshes captured in graph[rc]
 	long long ens_kernels[2] = { 0, 0 }; // ensemble launches in graph[rc] (counted on the first mesh)
+	bool holds_refs = false;			 // the instances count this batch in batch_refs
 };
 
 namespace bfvm {
@@ -225,6 +226,21 @@ int bfvm_batch_create(bfvm_batch** out, int32_t count, bfvm_solver* const* solve
 	}
 	if (e != cudaSuccess)
 		st = cuda_fail(e, "batch stream and events");
+	// the ensemble kernels use the agent terms in agent order: the instances hand back any sorted
+	// internalized amounts, and their own step graphs (which may use sorted terms) are dropped
+	for (int32_t i = 0; i < count && !st; i++)
+	{
+		bfvm_solver* s = b->inst[i];
+		st = agents_unsort(s, false);
+		if (!st)
+			st = solver_drop_graphs(s);
+	}
+	if (!st)
+	{
+		for (bfvm_solver* s : b->inst)
+			s->batch_refs++;
+		b->holds_refs = true;
+	}
 	if (st)
 	{
 		bfvm_batch_destroy(b);
@@ -243,6 +259,12 @@ int bfvm_batch_destroy(bfvm_batch* b)
 		cudaStreamSynchronize(b->stream);
 	batch_free_graph(b, 0);
 	batch_free_graph(b, 1);
+	if (b->holds_refs)
+		for (bfvm_solver* s : b->inst)
+		{
+			s->batch_refs--;
+			solver_drop_graphs(s); // stepping alone again may sort the agent terms
+		}
 	ensemble_free(b->ens[0]);
 	ensemble_free(b->ens[1]);
 	for (cudaEvent_t ev : b->join)

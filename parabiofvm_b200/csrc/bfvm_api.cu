@@ -94,6 +94,14 @@ static void free_graphs(bfvm_solver* s)
 	s->graph_epoch++; // graphs that captured this solver's buffers (its own, a batch's) are stale
 }
 
+int solver_drop_graphs(bfvm_solver* s)
+{
+	BFVM_CUDA(cudaSetDevice(s->device));
+	BFVM_CUDA(cudaStreamSynchronize(s->stream));
+	free_graphs(s);
+	return BFVM_OK;
+}
+
 static void destroy_all(bfvm_solver* s)
 {
 	if (s->device >= 0)
@@ -147,14 +155,7 @@ int check_device_errors(bfvm_solver* s)
 	return BFVM_OK;
 }
 
-static int diffusion(bfvm_solver* s)
-{
-	int st;
-	for (int axis = 0; axis < s->dims; axis++)
-		if ((st = launch_sweep(s, axis, axis == s->dims - 1)))
-			return st;
-	return BFVM_OK;
-}
+static int diffusion(bfvm_solver* s) { return launch_diffusion(s); }
 
 int order_after_copies(bfvm_solver* s)
 {
@@ -679,7 +680,12 @@ int bfvm_store_agents(bfvm_solver* s, int32_t count, const float* secretion_rate
 	BFVM_CUDA(cudaMemcpyAsync(a.pos, positions, (size_t)count * s->dims * sizeof(float), cudaMemcpyHostToDevice,
 							  s->stream));
 	if (resized)
+	{
 		a.binned = false;
+		a.sorted = false; // the stored amounts are the master until the next binning sorts them
+	}
+	else if ((st = agents_resort_internalized(s)))
+		return st;
 	return BFVM_OK;
 }
 
@@ -727,6 +733,9 @@ int bfvm_load_internalized_async(bfvm_solver* s, float* host)
 	if (!host)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
 	int rc;
+	// amounts held in sorted order are written to agent order first, after earlier copies read it
+	if (s->ag.sorted && ((rc = order_after_copies(s)) || (rc = agents_unsort(s, true))))
+		return rc;
 	if ((rc = begin_async_copy(s)))
 		return rc;
 	BFVM_CUDA(cudaMemcpyAsync(host, s->ag.intern, (size_t)s->ag.count * s->S * sizeof(float), cudaMemcpyDeviceToHost,
@@ -742,7 +751,7 @@ int bfvm_load_internalized(bfvm_solver* s, float* host)
 	if (!host)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "null host buffer");
 	int rc;
-	if ((rc = order_after_copies(s)))
+	if ((rc = order_after_copies(s)) || (rc = agents_unsort(s, true)))
 		return rc;
 	BFVM_CUDA(cudaMemcpyAsync(host, s->ag.intern, (size_t)s->ag.count * s->S * sizeof(float), cudaMemcpyDeviceToHost,
 							  s->stream));
@@ -827,7 +836,7 @@ int bfvm_add_agents(bfvm_solver* s, int32_t count, const float* secretion_rates,
 	if ((long long)s->ag.count + count > INT32_MAX)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "more than 2^31 - 1 agents");
 	int st;
-	if ((st = order_after_copies(s)))
+	if ((st = order_after_copies(s)) || (st = agents_unsort(s, false)))
 		return st;
 	BFVM_CUDA(cudaStreamSynchronize(s->stream));
 	free_graphs(s);
@@ -920,7 +929,7 @@ int bfvm_remove_agents(bfvm_solver* s, int32_t count, const int32_t* indices)
 		return st;
 	if (count == 0)
 		return BFVM_OK;
-	if ((st = order_after_copies(s)))
+	if ((st = order_after_copies(s)) || (st = agents_unsort(s, false)))
 		return st;
 	BFVM_CUDA(cudaStreamSynchronize(s->stream));
 	free_graphs(s);
@@ -951,9 +960,15 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
 				return st;
 			continue;
 		}
-		if (!s->step_graph[rc])
+		// what a step launches depends on whether the agent terms are sorted when it starts (a
+		// recompute step writes sorted amounts back first; a step after a batch sorts them), so
+		// there is a graph per (recompute, sorted before) and the host state advances as the
+		// captured step did
+		const int gi = 2 * rc + (s->ag.sorted ? 1 : 0);
+		if (!s->step_graph[gi])
 		{
 			cudaGraph_t g = nullptr;
+			const bool sorted_before = s->ag.sorted;
 			BFVM_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
 			const long long before = s->launches;
 			int st = one_step(s, rc == 1);
@@ -966,18 +981,25 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
 			}
 			if (ce != cudaSuccess)
 				return cuda_fail(ce, "cudaStreamEndCapture");
-			s->graph_kernels[rc] = s->launches - before;
+			s->graph_kernels[gi] = s->launches - before;
+			s->graph_sorted_after[gi] = s->ag.sorted;
 			s->launches = before;
-			ce = cudaGraphInstantiate(&s->step_graph[rc], g, 0);
+			s->ag.sorted = sorted_before; // set again below, as after every launch of the graph
+			ce = cudaGraphInstantiate(&s->step_graph[gi], g, 0);
 			cudaGraphDestroy(g);
 			if (ce != cudaSuccess)
 			{
-				s->step_graph[rc] = nullptr;
+				s->step_graph[gi] = nullptr;
 				return cuda_fail(ce, "cudaGraphInstantiate");
 			}
 		}
-		BFVM_CUDA(cudaGraphLaunch(s->step_graph[rc], s->stream));
-		s->launches += s->graph_kernels[rc];
+		BFVM_CUDA(cudaGraphLaunch(s->step_graph[gi], s->stream));
+		s->launches += s->graph_kernels[gi];
+		if (s->ag.count > 0)
+		{
+			s->ag.binned = true;
+			s->ag.sorted = s->graph_sorted_after[gi];
+		}
 	}
 	return BFVM_OK;
 }
@@ -1000,6 +1022,8 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 	const std::string n(name);
 	if (n == "tma_sweeps")
 		s->use_tma = value != 0;
+	else if (n == "fused_dirichlet")
+		s->dir_fused = value != 0;
 	else if (n == "wait_limit_cycles")
 	{
 		if (value < 10000 || value > 40000000000LL)

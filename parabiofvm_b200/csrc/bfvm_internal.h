@@ -71,6 +71,19 @@ struct scan_plan
 	std::vector<int*> level_sums;		// block sums per level (device)
 };
 
+// A Dirichlet overwrite list grouped by the tiles of one axis's staged sweep (dirichlet.cu): the
+// runs of four and single elements of tile w are [qoff[w], qoff[w + 1]) and [soff[w], soff[w + 1]).
+struct dirichlet_tiles
+{
+	long long items = 0; // tiles of the sweep; 0 when the axis has no grouped list
+	int* qoff = nullptr;
+	long long* qidx = nullptr;
+	float4* qval = nullptr;
+	int* soff = nullptr;
+	long long* sidx = nullptr;
+	float* sval = nullptr;
+};
+
 struct agent_state
 {
 	int count = 0;
@@ -91,6 +104,15 @@ struct agent_state
 	int tiles = 0;
 	scan_plan hist_scan, flag_scan;
 	bool binned = false;		 // a recompute has run since the last store
+
+	// A solver stepping alone with internalized substrates keeps its per-agent terms in the
+	// binning's sorted order (cell.cu): row p of snum/sden/sfac/sintern is row vals[p] of
+	// num/den/fac/intern, and rank[i] is agent i's row there, so the per-step update reads and
+	// writes contiguous rows.  While `sorted` is set, sintern holds the internalized amounts and
+	// intern is only a copy, refreshed when they are loaded.
+	float *snum = nullptr, *sden = nullptr, *sfac = nullptr, *sintern = nullptr; // [A][S] sorted
+	int* rank = nullptr;																// [A]
+	bool sorted = false;
 
 	int* move_idx = nullptr; // [2][moves]: destinations, then sources of bfvm_remove_agents
 	int move_capacity = 0;
@@ -132,6 +154,9 @@ struct bfvm_solver
 	long long* dir_idx = nullptr; // element index vid * S + s
 	float* dir_val = nullptr;
 	long long dir_count = 0;
+	// the same list grouped by the tiles of each axis's staged sweep, which applies a tile's entries
+	// right after storing the tile (the overwrite that follows the sweep in the LOD step)
+	bfvm::dirichlet_tiles dir_tiles[3];
 
 	bfvm::agent_state ag;
 
@@ -145,14 +170,17 @@ struct bfvm_solver
 
 	long long launches = 0;
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
+	bool dir_fused = true;		 // staged sweeps of the LOD step write the overwrite that follows them
 	long long wait_limit_cycles = 4000000000LL; // bound of the staged sweeps' waits on tile copies (clock64 cycles;
 												// the default is the kernels' WAIT_LIMIT_CYCLES)
 	long long drop_tile_copy = -1;				// tests only: a staged-sweep tile whose copies are never issued
 	bfvm::sweep_tuning tune[3];	 // staged sweep launch shape per axis
 
-	// graphs for run_steps: [recompute]
-	cudaGraphExec_t step_graph[2] = { nullptr, nullptr };
-	long long graph_kernels[2] = { 0, 0 }; // kernel nodes per step graph
+	// graphs for run_steps: [2 * recompute + agent terms sorted before the step]
+	cudaGraphExec_t step_graph[4] = { nullptr, nullptr, nullptr, nullptr };
+	long long graph_kernels[4] = { 0, 0, 0, 0 }; // kernel nodes per step graph
+	bool graph_sorted_after[4] = { false, false, false, false }; // agent terms sorted after the step
+	int batch_refs = 0; // batches holding this solver: their ensemble kernels use agent order
 	bool graphs_dirty = true;
 	long long graph_epoch = 0; // advances whenever captured buffers or launch shapes may have changed
 
@@ -210,6 +238,7 @@ int check_device_errors(bfvm_solver* s);	  // waits for the stream, reports devi
 
 // sweep.cu
 int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);
+int launch_diffusion(bfvm_solver* s); // the LOD step, overwrites fused into the staged sweeps
 // the staged sweep of one axis alone, with launch shape `tune` (groups 0: built-in choice);
 // `handled` is false when the staged path does not take the shape
 int launch_staged_sweep(bfvm_solver* s, int axis, const sweep_tuning& tune, bool& handled);
@@ -236,6 +265,9 @@ void free_bulk(bfvm_solver* s);
 int cell_alloc(bfvm_solver* s, int count);
 void cell_free(bfvm_solver* s);
 int launch_secretion(bfvm_solver* s, bool recompute);
+int agents_unsort(bfvm_solver* s, bool keep_sorted); // internalized amounts back to agent order (cell.cu)
+int solver_drop_graphs(bfvm_solver* s);			  // after queued work, drop the step graphs (bfvm_api.cu)
+int agents_resort_internalized(bfvm_solver* s);	  // stored internalized amounts into sorted order
 int launch_release(bfvm_solver* s, int index);
 // storage for `count` agents keeping the stored rows; the moves dst[k] <- src[k] of every agent row
 int cell_grow(bfvm_solver* s, int count);

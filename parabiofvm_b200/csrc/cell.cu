@@ -218,6 +218,76 @@ __global__ void reduce_kernel(long long total, int S, const int* __restrict__ co
 	red_fac[t] = rf;
 }
 
+// The same sums over rows in the binning's sorted order (row p is the agent at sorted position p).
+__global__ void reduce_sorted_kernel(long long total, int S, const int* __restrict__ counts,
+									 const int* __restrict__ seg_start, const float* __restrict__ num,
+									 const float* __restrict__ den, const float* __restrict__ fac,
+									 float* __restrict__ red_num, float* __restrict__ red_den,
+									 float* __restrict__ red_fac)
+{
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= total)
+		return;
+	const int seg = (int)(t / S);
+	const int s = (int)(t % S);
+	if (seg >= counts[0])
+		return;
+	const int b = seg_start[seg], e = seg_start[seg + 1];
+	const size_t w = (size_t)b * S + s;
+	float rn = __fadd_rn(0.f, num[w]);
+	float rd = __fadd_rn(0.f, __fadd_rn(den[w], 1.f));
+	float rf = __fadd_rn(0.f, fac[w]);
+	for (int p = b + 1; p < e; p++)
+	{
+		const size_t k = (size_t)p * S + s;
+		rn = __fadd_rn(rn, num[k]);
+		rd = __fadd_rn(rd, den[k]);
+		rf = __fadd_rn(rf, fac[k]);
+	}
+	red_num[t] = rn;
+	red_den[t] = rd;
+	red_fac[t] = rf;
+}
+
+// Row p of the sorted copies takes row order[p] of the agent-order arrays, and rank[order[p]] = p
+// (t over A * S; every agent, those outside the mesh included, has a row).
+__global__ void sort_agent_terms_kernel(long long total, int S, const int* __restrict__ order,
+										const float* __restrict__ num, const float* __restrict__ den,
+										const float* __restrict__ fac, const float* __restrict__ intern,
+										float* __restrict__ snum, float* __restrict__ sden, float* __restrict__ sfac,
+										float* __restrict__ sintern, int* __restrict__ rank)
+{
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= total)
+		return;
+	const int p = (int)(t / S);
+	const int s = (int)(t - (long long)p * S);
+	const int i = order[p];
+	const size_t k = (size_t)i * S + s;
+	snum[t] = num[k];
+	sden[t] = den[k];
+	sfac[t] = fac[k];
+	sintern[t] = intern[k];
+	if (s == 0)
+		rank[i] = p;
+}
+
+// One array between the two orders: to_sorted, row p of `sorted` takes row order[p] of `agent`;
+// otherwise row order[p] of `agent` takes row p of `sorted`.
+__global__ void permute_rows_kernel(long long total, int S, const int* __restrict__ order, float* __restrict__ agent,
+									float* __restrict__ sorted, int to_sorted)
+{
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= total)
+		return;
+	const int p = (int)(t / S);
+	const size_t k = (size_t)order[p] * S + (t - (long long)p * S);
+	if (to_sorted)
+		sorted[t] = agent[k];
+	else
+		agent[k] = sorted[t];
+}
+
 // ---------------------------------------------------------------------------------------------
 // the per-step update (compute_result)
 
@@ -234,6 +304,22 @@ __global__ void secrete_kernel(long long total, int S, float* __restrict__ dens,
 		return;
 	secrete_element(t, S, dens, counts, seg_start, order, keys, num, den, fac, red_num, red_den, red_fac, intern,
 					internalized, voxel_volume);
+}
+
+// The same update with the per-agent rows in the binning's sorted order: an agent's rows are read
+// and written where its voxel's segment lies, so a warp touches contiguous memory.
+__global__ void secrete_sorted_kernel(long long total, int S, float* __restrict__ dens, const int* __restrict__ counts,
+									  const int* __restrict__ seg_start, const unsigned int* __restrict__ keys,
+									  const float* __restrict__ snum, const float* __restrict__ sden,
+									  const float* __restrict__ sfac, const float* __restrict__ red_num,
+									  const float* __restrict__ red_den, const float* __restrict__ red_fac,
+									  float* __restrict__ sintern, float voxel_volume)
+{
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= total)
+		return;
+	secrete_element<true>(t, S, dens, counts, seg_start, nullptr, keys, snum, sden, sfac, red_num, red_den, red_fac,
+						  sintern, 1, voxel_volume);
 }
 
 // release_internalized_substrates (:301-346): D += I*F/Vv at the agent's current voxel, I = 0
@@ -257,6 +343,29 @@ __global__ void release_kernel(int index, int S, int dims, const float* __restri
 	intern[k] = 0.f;
 }
 
+// The same release with the internalized amounts in sorted order: agent `index` is at row rank[index].
+__global__ void release_sorted_kernel(int index, int S, int dims, const float* __restrict__ pos, int3 bmin, int3 vox,
+									  int3 grid, float* __restrict__ dens, float* __restrict__ sintern,
+									  const int* __restrict__ rank, const float* __restrict__ frac, float voxel_volume,
+									  int* err)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= S)
+		return;
+	int3 c;
+	if (!voxel_of(pos + (size_t)index * dims, dims, bmin, vox, grid, c))
+	{
+		if (s == 0)
+			atomicOr(err, DEVERR_AGENT_OUTSIDE);
+		return;
+	}
+	const size_t v = (size_t)c.x + (size_t)grid.x * ((size_t)c.y + (size_t)grid.y * c.z);
+	const size_t k = (size_t)rank[index] * S + s;
+	const float f = frac[(size_t)index * S + s];
+	dens[v * S + s] = __fadd_rn(dens[v * S + s], __fdiv_rn(__fmul_rn(sintern[k], f), voxel_volume));
+	sintern[k] = 0.f;
+}
+
 // ---------------------------------------------------------------------------------------------
 // host side
 
@@ -264,8 +373,10 @@ void cell_free(bfvm_solver* s)
 {
 	agent_state& a = s->ag;
 	for (float** p : { &a.sec, &a.sat, &a.upt, &a.nex, &a.intern, &a.frac, &a.vol, &a.pos, &a.num, &a.den, &a.fac,
-					   &a.red_num, &a.red_den, &a.red_fac })
+					   &a.red_num, &a.red_den, &a.red_fac, &a.snum, &a.sden, &a.sfac, &a.sintern })
 		device_free(*p);
+	device_free(a.rank);
+	a.sorted = false;
 	device_free(a.keys);
 	device_free(a.keys_alt);
 	device_free(a.vals);
@@ -301,6 +412,14 @@ int cell_alloc(bfvm_solver* s, int count)
 			return st;
 	if ((st = device_alloc(&a.vol, (size_t)count)) || (st = device_alloc(&a.pos, (size_t)count * s->dims)))
 		return st;
+	if (s->internalized)
+	{
+		for (float** p : { &a.snum, &a.sden, &a.sfac, &a.sintern })
+			if ((st = device_alloc(p, AS)))
+				return st;
+		if ((st = device_alloc(&a.rank, (size_t)count)))
+			return st;
+	}
 	a.tiles = (int)((count + SORT_TILE - 1) / SORT_TILE);
 	if ((st = device_alloc(&a.keys, (size_t)count)) || (st = device_alloc(&a.keys_alt, (size_t)count))
 		|| (st = device_alloc(&a.vals, (size_t)count)) || (st = device_alloc(&a.vals_alt, (size_t)count))
@@ -315,7 +434,7 @@ int cell_alloc(bfvm_solver* s, int count)
 	return BFVM_OK;
 }
 
-int rebuild_bins(bfvm_solver* s)
+int rebuild_bins(bfvm_solver* s, bool sorted)
 {
 	agent_state& a = s->ag;
 	const int A = a.count;
@@ -372,27 +491,103 @@ int rebuild_bins(bfvm_solver* s)
 														 a.num, a.den, a.fac);
 	if ((st = check_launch(s, "intermediates_kernel")))
 		return st;
-	reduce_kernel<<<blocks, 256, 0, s->stream>>>(AS, s->S, a.seg_count_dev, a.seg_start, a.vals, a.num, a.den, a.fac,
-												 a.red_num, a.red_den, a.red_fac);
-	if ((st = check_launch(s, "reduce_kernel")))
-		return st;
+	if (sorted)
+	{
+		sort_agent_terms_kernel<<<blocks, 256, 0, s->stream>>>(AS, s->S, a.vals, a.num, a.den, a.fac, a.intern, a.snum,
+																a.sden, a.sfac, a.sintern, a.rank);
+		if ((st = check_launch(s, "sort_agent_terms_kernel")))
+			return st;
+		reduce_sorted_kernel<<<blocks, 256, 0, s->stream>>>(AS, s->S, a.seg_count_dev, a.seg_start, a.snum, a.sden,
+															 a.sfac, a.red_num, a.red_den, a.red_fac);
+		if ((st = check_launch(s, "reduce_sorted_kernel")))
+			return st;
+	}
+	else
+	{
+		reduce_kernel<<<blocks, 256, 0, s->stream>>>(AS, s->S, a.seg_count_dev, a.seg_start, a.vals, a.num, a.den,
+													 a.fac, a.red_num, a.red_den, a.red_fac);
+		if ((st = check_launch(s, "reduce_kernel")))
+			return st;
+	}
 	a.binned = true;
 	return BFVM_OK;
 }
 
+// One per-agent array between agent order and the binning's sorted order.
+static int permute_rows(bfvm_solver* s, float* agent, float* sorted, bool to_sorted)
+{
+	const long long AS = (long long)s->ag.count * s->S;
+	permute_rows_kernel<<<(unsigned)((AS + 255) / 256), 256, 0, s->stream>>>(AS, s->S, s->ag.vals, agent, sorted,
+																			  to_sorted ? 1 : 0);
+	return check_launch(s, "permute_rows_kernel");
+}
+
+// While the agent terms are sorted, the internalized amounts live in sintern: write them back to
+// agent order (intern).  keep_sorted: as a copy for a load (sintern stays the master); otherwise
+// agent order becomes the master.
+int agents_unsort(bfvm_solver* s, bool keep_sorted)
+{
+	agent_state& a = s->ag;
+	if (!a.sorted || a.count == 0)
+		return BFVM_OK;
+	const int st = permute_rows(s, a.intern, a.sintern, false);
+	if (!st && !keep_sorted)
+		a.sorted = false;
+	return st;
+}
+
+// Internalized amounts just stored in agent order: into sorted order, when the terms are sorted.
+int agents_resort_internalized(bfvm_solver* s)
+{
+	agent_state& a = s->ag;
+	if (!a.sorted || a.count == 0)
+		return BFVM_OK;
+	return permute_rows(s, a.intern, a.sintern, true);
+}
+
+// A solver stepping alone with internalized substrates runs secretion on sorted agent terms: a
+// rebinning sorts them (after writing the internalized amounts back to agent order with the old
+// order), and a solver binned but not sorted (a batch stepped it) sorts them once.  Solvers held
+// by a batch, and solvers without internalized substrates, keep agent order.
 int launch_secretion(bfvm_solver* s, bool recompute)
 {
 	agent_state& a = s->ag;
 	if (a.count == 0)
 		return BFVM_OK;
+	const bool use_sorted = s->internalized && s->batch_refs == 0;
 	int st;
-	if (recompute || !a.binned)
-		if ((st = rebuild_bins(s)))
+	if (recompute || !a.binned || (a.sorted && !use_sorted))
+	{
+		if ((st = agents_unsort(s, false)))
 			return st;
+	}
+	if (recompute || !a.binned)
+	{
+		if ((st = rebuild_bins(s, use_sorted)))
+			return st;
+		a.sorted = use_sorted;
+	}
+	else if (use_sorted && !a.sorted)
+	{
+		const long long AS = (long long)a.count * s->S;
+		sort_agent_terms_kernel<<<(unsigned)((AS + 255) / 256), 256, 0, s->stream>>>(
+			AS, s->S, a.vals, a.num, a.den, a.fac, a.intern, a.snum, a.sden, a.sfac, a.sintern, a.rank);
+		if ((st = check_launch(s, "sort_agent_terms_kernel")))
+			return st;
+		a.sorted = true;
+	}
 	const long long AS = (long long)a.count * s->S;
+	const float vv = (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]);
+	if (a.sorted)
+	{
+		secrete_sorted_kernel<<<(unsigned)((AS + 255) / 256), 256, 0, s->stream>>>(
+			AS, s->S, s->dens, a.seg_count_dev, a.seg_start, a.keys, a.snum, a.sden, a.sfac, a.red_num, a.red_den,
+			a.red_fac, a.sintern, vv);
+		return check_launch(s, "secrete_sorted_kernel");
+	}
 	secrete_kernel<<<(unsigned)((AS + 255) / 256), 256, 0, s->stream>>>(
 		AS, s->S, s->dens, a.seg_count_dev, a.seg_start, a.vals, a.keys, a.num, a.den, a.fac, a.red_num, a.red_den,
-		a.red_fac, a.intern, s->internalized ? 1 : 0, (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]));
+		a.red_fac, a.intern, s->internalized ? 1 : 0, vv);
 	return check_launch(s, "secrete_kernel");
 }
 
@@ -404,10 +599,16 @@ int launch_release(bfvm_solver* s, int index)
 	const int3 bmin = make_int3(s->bbox_min[0], s->bbox_min[1], s->bbox_min[2]);
 	const int3 vox = make_int3(s->voxel[0], s->voxel[1], s->voxel[2]);
 	const int3 grid = make_int3(s->grid[0], s->grid[1], s->grid[2]);
+	const float vv = (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]);
+	if (a.sorted)
+	{
+		release_sorted_kernel<<<(s->S + 127) / 128, 128, 0, s->stream>>>(index, s->S, s->dims, a.pos, bmin, vox, grid,
+																		  s->dens, a.sintern, a.rank, a.frac, vv,
+																		  s->dev_error);
+		return check_launch(s, "release_sorted_kernel");
+	}
 	release_kernel<<<(s->S + 127) / 128, 128, 0, s->stream>>>(index, s->S, s->dims, a.pos, bmin, vox, grid, s->dens,
-															  a.intern, a.frac,
-															  (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]),
-															  s->dev_error);
+															  a.intern, a.frac, vv, s->dev_error);
 	return check_launch(s, "release_kernel");
 }
 

@@ -44,6 +44,17 @@ int launch_dirichlet(bfvm_solver* st)
 	return check_launch(st, "dirichlet_scatter_kernel");
 }
 
+static void free_tiles(dirichlet_tiles& t)
+{
+	device_free(t.qoff);
+	device_free(t.qidx);
+	device_free(t.qval);
+	device_free(t.soff);
+	device_free(t.sidx);
+	device_free(t.sval);
+	t.items = 0;
+}
+
 void free_dirichlet(bfvm_solver* s)
 {
 	device_free(s->dir_qidx);
@@ -52,6 +63,115 @@ void free_dirichlet(bfvm_solver* s)
 	device_free(s->dir_val);
 	s->dir_qcount = 0;
 	s->dir_count = 0;
+	for (auto& t : s->dir_tiles)
+		free_tiles(t);
+}
+
+// The tiles of the staged sweep along `axis` (sweep_tma.cu): x, R = 32 / S whole rows; y, 32
+// columns of the x*s plane of one z plane; z, 32 columns of the y*x*s plane.  Returns the tile
+// count (0 when the staged sweep cannot take the axis) and sets tile(e) for element e.
+struct staged_tiling
+{
+	int axis = 0;
+	long long XS = 0, YXS = 0, R = 1, col_tiles = 0, items = 0;
+
+	long long tile(long long e) const
+	{
+		if (axis == 0)
+			return (e / XS) / R;
+		if (axis == 1)
+			return (e / YXS) * col_tiles + (e % XS) / 32;
+		return (e % YXS) / 32;
+	}
+};
+
+static staged_tiling staged_tiles(const bfvm_solver* s, int axis)
+{
+	staged_tiling t;
+	t.axis = axis;
+	const long long X = s->grid[0], Y = s->grid[1], Z = s->grid[2], S = s->S;
+	t.XS = X * S;
+	t.YXS = Y * X * S;
+	if (axis >= s->dims || t.XS % 4 != 0 || (axis == 0 && S > 32))
+		return t;
+	if (axis == 0)
+	{
+		t.R = 32 / S;
+		t.items = (Y * Z + t.R - 1) / t.R;
+	}
+	else if (axis == 1)
+	{
+		t.col_tiles = (t.XS + 31) / 32;
+		t.items = Z * t.col_tiles;
+	}
+	else
+		t.items = (t.YXS + 31) / 32;
+	return t;
+}
+
+// Group the sorted runs and singles by the tiles of each axis (a counting sort keeps each tile's
+// entries in ascending element order) and upload them.
+static int build_tile_lists(bfvm_solver* s, const std::vector<long long>& qidx, const std::vector<float4>& qval,
+							const std::vector<long long>& sidx, const std::vector<float>& sval)
+{
+	for (int axis = 0; axis < s->dims; axis++)
+	{
+		const staged_tiling tl = staged_tiles(s, axis);
+		if (tl.items == 0 || tl.items > INT32_MAX || qidx.size() + sidx.size() > (size_t)INT32_MAX)
+			continue;
+		dirichlet_tiles& t = s->dir_tiles[axis];
+		std::vector<int> qoff(tl.items + 1, 0), soff(tl.items + 1, 0);
+		for (long long e : qidx)
+			qoff[tl.tile(e) + 1]++;
+		for (long long e : sidx)
+			soff[tl.tile(e) + 1]++;
+		for (long long w = 0; w < tl.items; w++)
+		{
+			qoff[w + 1] += qoff[w];
+			soff[w + 1] += soff[w];
+		}
+		std::vector<long long> qi(qidx.size()), si(sidx.size());
+		std::vector<float4> qv(qval.size());
+		std::vector<float> sv(sval.size());
+		{
+			std::vector<int> at(qoff.begin(), qoff.end() - 1);
+			for (size_t k = 0; k < qidx.size(); k++)
+			{
+				const int p = at[tl.tile(qidx[k])]++;
+				qi[p] = qidx[k];
+				qv[p] = qval[k];
+			}
+			std::vector<int> as(soff.begin(), soff.end() - 1);
+			for (size_t k = 0; k < sidx.size(); k++)
+			{
+				const int p = as[tl.tile(sidx[k])]++;
+				si[p] = sidx[k];
+				sv[p] = sval[k];
+			}
+		}
+		int st;
+		if ((st = device_alloc(&t.qoff, qoff.size())) || (st = device_alloc(&t.soff, soff.size()))
+			|| (st = device_alloc(&t.qidx, qi.size())) || (st = device_alloc(&t.qval, qv.size()))
+			|| (st = device_alloc(&t.sidx, si.size())) || (st = device_alloc(&t.sval, sv.size())))
+		{
+			free_tiles(t);
+			return st;
+		}
+		BFVM_CUDA(cudaMemcpy(t.qoff, qoff.data(), qoff.size() * sizeof(int), cudaMemcpyHostToDevice));
+		BFVM_CUDA(cudaMemcpy(t.soff, soff.data(), soff.size() * sizeof(int), cudaMemcpyHostToDevice));
+		if (!qi.empty())
+		{
+			BFVM_CUDA(cudaMemcpy(t.qidx, qi.data(), qi.size() * sizeof(long long), cudaMemcpyHostToDevice));
+			BFVM_CUDA(cudaMemcpy(t.qval, qv.data(), qv.size() * sizeof(float4), cudaMemcpyHostToDevice));
+		}
+		if (!si.empty())
+		{
+			BFVM_CUDA(cudaMemcpy(t.sidx, si.data(), si.size() * sizeof(long long), cudaMemcpyHostToDevice));
+			BFVM_CUDA(cudaMemcpy(t.sval, sv.data(), sv.size() * sizeof(float), cudaMemcpyHostToDevice));
+		}
+		t.items = tl.items;
+	}
+	return BFVM_OK;
 }
 
 // Resolve the faces and interior voxels into the overwrite list and upload it.
@@ -173,7 +293,12 @@ int rebuild_dirichlet(bfvm_solver* s)
 	}
 	s->dir_qcount = (long long)qidx.size();
 	s->dir_count = (long long)sidx.size();
-	return BFVM_OK;
+	if (s->slab_count > 1 || qidx.size() + sidx.size() == 0)
+		return BFVM_OK; // slabs step axis by axis through the unfused calls
+	const int st2 = build_tile_lists(s, qidx, qval, sidx, sval);
+	if (st2)
+		free_dirichlet(s);
+	return st2;
 }
 
 } // namespace bfvm

@@ -208,6 +208,7 @@ static sweep_args make_args(bfvm_solver* st, int axis)
 	a.slab_lines = 0;
 	a.wait_limit = st->wait_limit_cycles;
 	a.drop_tile_copy = st->drop_tile_copy;
+	a.dir = dirichlet_tiles();
 	return a;
 }
 
@@ -242,18 +243,17 @@ int launch_slab_z(bfvm_solver* st)
 	return rc;
 }
 
-// One axis of the LOD step: the Dirichlet overwrite that precedes the sweep, the sweep, and after
-// the last axis the closing overwrite.
-int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
+// The sweep of one axis by the first kernel that takes its shape: the TMA-staged sweep (which sets
+// `staged`), the ensemble sweep on this mesh alone, or the direct kernels.
+static int sweep_axis(bfvm_solver* st, int axis, const sweep_args& a, bool& staged)
 {
-	int rc = launch_dirichlet(st);
-	if (rc)
-		return rc;
 	const sweep_plan& pl = st->plan[axis];
-	const sweep_args a = make_args(st, axis);
+	int rc = BFVM_OK;
 	bool handled = false;
+	staged = false;
 	if (st->use_tma)
 		rc = launch_sweep_tma(st, axis, a, handled, &st->tune[axis]);
+	staged = handled;
 	// the same front-padded block algebra without TMA staging, where the lines fit 16 blocks
 	if (!rc && !handled && st->self_plan && pl.vtab && pl.vP <= ENS_MAX_P && (axis > 0 || st->S <= 32))
 	{
@@ -264,8 +264,40 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 	}
 	if (!rc && !handled)
 		rc = pl.M == 32 ? launch_sweep_m<32>(st, axis, a) : launch_sweep_m<64>(st, axis, a);
+	return rc;
+}
+
+// One axis on its own (bfvm_diffusion_sweep): the Dirichlet overwrite that precedes the sweep,
+// the sweep, and after the last axis the closing overwrite.
+int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
+{
+	int rc = launch_dirichlet(st);
+	if (rc)
+		return rc;
+	bool staged = false;
+	rc = sweep_axis(st, axis, make_args(st, axis), staged);
 	if (!rc && final_dirichlet)
 		rc = launch_dirichlet(st);
+	return rc;
+}
+
+// The whole LOD step (src/solver/host/diffusion_solver.cpp:512-544): overwrite, then per axis the
+// sweep and the overwrite after it.  A staged sweep writes that overwrite itself, tile by tile
+// right after storing the tile, from the list grouped by its tiles; other sweeps are followed by
+// the scatter kernel.
+int launch_diffusion(bfvm_solver* st)
+{
+	int rc = launch_dirichlet(st);
+	for (int axis = 0; axis < st->dims && !rc; axis++)
+	{
+		sweep_args a = make_args(st, axis);
+		if (st->dir_fused)
+			a.dir = st->dir_tiles[axis];
+		bool staged = false;
+		rc = sweep_axis(st, axis, a, staged);
+		if (!rc && !(staged && a.dir.items > 0))
+			rc = launch_dirichlet(st);
+	}
 	return rc;
 }
 

@@ -30,6 +30,9 @@ struct sweep_args
 	// issued (-1: none), so that the wait on it runs out
 	long long wait_limit;
 	long long drop_tile_copy;
+	// staged sweeps of the LOD step: the Dirichlet overwrite that follows this sweep, grouped by its
+	// tiles; each tile's entries are written right after the tile (items 0: no overwrite here)
+	dirichlet_tiles dir;
 };
 
 __device__ __forceinline__ void block_range(int j, int base_len, int extra, int& p, int& L)

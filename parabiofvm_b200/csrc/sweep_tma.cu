@@ -179,6 +179,19 @@ __device__ __forceinline__ void store_element(float* p, float v)
 		*p = v;
 }
 
+// The Dirichlet entries of tile w (sweep_args::dir), written by the gthr threads of a warp group.
+// The caller has ordered them after every store of the tile with a barrier of the group, so an
+// entry's value replaces the solved one, as the overwrite after the sweep does.
+__device__ __forceinline__ void overwrite_tile(const dirichlet_tiles& d, float* data, long long w, int gtid, int gthr)
+{
+	const int q1 = __ldg(&d.qoff[w + 1]);
+	for (int e = __ldg(&d.qoff[w]) + gtid; e < q1; e += gthr)
+		*reinterpret_cast<float4*>(data + __ldg(&d.qidx[e])) = __ldg(&d.qval[e]);
+	const int s1 = __ldg(&d.soff[w + 1]);
+	for (int e = __ldg(&d.soff[w]) + gtid; e < s1; e += gthr)
+		data[__ldg(&d.sidx[e])] = __ldg(&d.sval[e]);
+}
+
 // SLAB (y/z tiles only): 0 a plain sweep; 1 the solve pass of a z-slab, which enters every line
 // with the carries C (left) and X (right) of slab_carry: it always runs the carry folds, from C and
 // X instead of zero, with the tables of precompute_padded_range.
@@ -315,6 +328,9 @@ __global__ void __launch_bounds__(640, 1)
 		// ahead, so NST tiles stay in flight through the rest of this tile's solve
 		if (leader)
 			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st]);
+		// the barrier also ordered the previous tile's stores: its Dirichlet entries go on top
+		if (a.dir.items > 0 && it > 0)
+			overwrite_tile(a.dir, a.data, w - wstride, lane + 32 * j, gthr);
 
 		if (SLAB != 0)
 		{
@@ -408,6 +424,11 @@ __global__ void __launch_bounds__(640, 1)
 		}
 	}
 
+	if (!failed && a.dir.items > 0 && it > 0)
+	{
+		group_sync(bar_id, gthr); // the last tile's stores, then its entries
+		overwrite_tile(a.dir, a.data, w - wstride, lane + 32 * j, gthr);
+	}
 	if (failed && leader)
 	{
 		atomicOr(a.err, DEVERR_TIMEOUT);

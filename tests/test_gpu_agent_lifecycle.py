@@ -155,3 +155,29 @@ def test_all_agents_leave_then_new_ones_arrive():
     _same(a, b)
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_store_with_same_count_keeps_binning_and_takes_new_amounts():
+    """Storing agents with an unchanged count keeps the binning until the next recompute step (as
+    the reference's store does) and takes the stored internalized amounts, also while the solver
+    holds them in the binning's sorted order: the same as a fresh solver given that state."""
+    w = synthetic(30, 4, 2500, seed=17, clustered=True, sigma=80.0)
+    a = w.agents
+    s = make_solver(w)
+    s.run_steps(5, 0)
+    field = s.load_densities().copy()
+    intern = (s.load_internalized().reshape(a.count, w.S) * 0.5).astype(np.float32)
+    s.store_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates, intern,
+                   a.fraction_released, a.volumes, a.positions)
+    s.run_steps(4, 5)
+    w2 = synthetic(30, 4, 2500, seed=17, clustered=True, sigma=80.0)
+    w2.densities = field
+    w2.agents.internalized = intern
+    fresh = make_solver(w2)
+    fresh.run_steps(4, 5)
+    np.testing.assert_array_equal(s.load_densities(), fresh.load_densities())
+    np.testing.assert_array_equal(s.load_gradients(), fresh.load_gradients())
+    np.testing.assert_array_equal(s.load_internalized(), fresh.load_internalized())
+    s.close()
+    fresh.close()

@@ -81,3 +81,26 @@ def test_batch_follows_changes_to_an_instance():
     b.close()
     for s in solvers + ref:
         s.close()
+
+
+def test_solver_alone_then_batched_then_alone():
+    """A solver stepping alone keeps its agent terms in the binning's sorted order; joining a batch
+    hands them back in agent order for the ensemble kernels, and leaving it sorts them again.  Every
+    hand-over keeps the results bit for bit those of a solver that only ever stepped alone."""
+    ws = _ensemble()[:3]
+    solvers = [make_solver(w) for w in ws]
+    ref = make_solver(ws[0])
+    solvers[0].run_steps(12, 0)
+    b = Batch(solvers)
+    b.run_steps(12, 12)
+    b.synchronize()
+    b.close()
+    solvers[0].release(5)
+    solvers[0].run_steps(12, 24)
+    ref.run_steps(24, 0)
+    ref.release(5)
+    ref.run_steps(12, 24)
+    for g, e in zip(_state(solvers[0]), _state(ref)):
+        np.testing.assert_array_equal(g, e)
+    for s in solvers + [ref]:
+        s.close()
