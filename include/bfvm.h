@@ -137,6 +137,12 @@ int bfvm_diffusion_sweep(bfvm_solver* s, int axis);
 int bfvm_dirichlet_solve(bfvm_solver* s);
 /* Central-difference gradients of the current field (gradient_solver::solve). */
 int bfvm_gradient_solve(bfvm_solver* s);
+/* bfvm_diffusion_solve followed by bfvm_gradient_solve (diffusion_solver::solve then
+ * gradient_solver::solve, as src/main.cpp:76-90 calls them), with the gradient computed inside the
+ * z sweep where the staged sweep takes the mesh: each tile's gradient is computed from the planes
+ * the sweep just wrote, while they are still in L2, instead of re-reading the field from memory.
+ * The results are the same bits as the two calls. */
+int bfvm_diffusion_gradient_solve(bfvm_solver* s);
 /* Secretion and uptake (cell_solver::simulate_secretion_and_uptake); recompute != 0 rebuilds the
  * per-voxel reductions from the current agent data and positions. */
 int bfvm_secretion_solve(bfvm_solver* s, int recompute);

@@ -189,6 +189,10 @@ class Solver:
     def gradient(self):
         check(self._lib.bfvm_gradient_solve(self._h))
 
+    def diffusion_gradient(self):
+        """diffusion() then gradient(), the gradient computed inside the z sweep where it can be."""
+        check(self._lib.bfvm_diffusion_gradient_solve(self._h))
+
     def secretion(self, recompute):
         check(self._lib.bfvm_secretion_solve(self._h, int(bool(recompute))))
 

@@ -47,6 +47,7 @@ SIGNATURES = {
     "bfvm_diffusion_sweep": (c_int, [c_void_p, c_int]),
     "bfvm_dirichlet_solve": (c_int, [c_void_p]),
     "bfvm_gradient_solve": (c_int, [c_void_p]),
+    "bfvm_diffusion_gradient_solve": (c_int, [c_void_p]),
     "bfvm_secretion_solve": (c_int, [c_void_p, c_int]),
     "bfvm_release_internalized": (c_int, [c_void_p, c_int32]),
     "bfvm_add_agents": (c_int, [c_void_p, c_int32] + [P(c_float)] * 8),

@@ -111,6 +111,9 @@ static void destroy_all(bfvm_solver* s)
 		free_plan(p);
 	cell_free(s);
 	free_dirichlet(s);
+	device_free(s->grad_tile_done);
+	device_free(s->grad_deferred);
+	s->grad_tiles = 0;
 	free_bulk(s);
 	if (s->self_plan)
 	{
@@ -166,8 +169,7 @@ int order_after_copies(bfvm_solver* s)
 	return BFVM_OK;
 }
 
-// the copy stream starts after everything queued on the solver's stream so far
-static int begin_async_copy(bfvm_solver* s)
+static int ensure_copy_stream(bfvm_solver* s)
 {
 	if (!s->copy_stream)
 	{
@@ -175,6 +177,15 @@ static int begin_async_copy(bfvm_solver* s)
 		BFVM_CUDA(cudaEventCreateWithFlags(&s->copy_ready, cudaEventDisableTiming));
 		BFVM_CUDA(cudaEventCreateWithFlags(&s->copy_done, cudaEventDisableTiming));
 	}
+	return BFVM_OK;
+}
+
+// the copy stream starts after everything queued on the solver's stream so far
+static int begin_async_copy(bfvm_solver* s)
+{
+	int st;
+	if ((st = ensure_copy_stream(s)))
+		return st;
 	BFVM_CUDA(cudaEventRecord(s->copy_ready, s->stream));
 	BFVM_CUDA(cudaStreamWaitEvent(s->copy_stream, s->copy_ready, 0));
 	return BFVM_OK;
@@ -187,12 +198,26 @@ static int end_async_copy(bfvm_solver* s)
 	return BFVM_OK;
 }
 
+// diffusion, gradient (inside the z sweep where it can be), secretion.  Only secretion touches
+// agent data, so the wait for the asynchronous agent copies (the copy stream's last event; inside
+// a capture, an external event node that waits for the copies issued before each launch of the
+// graph) comes right before it, and the diffusion overlaps the copies.
 int one_step(bfvm_solver* s, bool recompute)
 {
 	int st;
-	if ((st = diffusion(s)) || (st = launch_gradient(s)) || (st = launch_secretion(s, recompute)))
+	bool gradient_done = false;
+	if ((st = launch_diffusion(s, true, &gradient_done)))
 		return st;
-	return BFVM_OK;
+	if (!gradient_done && (st = launch_gradient(s)))
+		return st;
+	if (s->copy_stream && s->ag.count > 0)
+	{
+		cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+		BFVM_CUDA(cudaStreamIsCapturing(s->stream, &cs));
+		BFVM_CUDA(cudaStreamWaitEvent(s->stream, s->copy_done,
+									  cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0));
+	}
+	return launch_secretion(s, recompute);
 }
 
 } // namespace bfvm
@@ -781,6 +806,17 @@ int bfvm_dirichlet_solve(bfvm_solver* s)
 	return launch_dirichlet(s);
 }
 
+int bfvm_diffusion_gradient_solve(bfvm_solver* s)
+{
+	CHECK_SOLVER(s);
+	REFUSE_SLABS(s, "bfvm_diffusion_gradient_solve");
+	bool done = false;
+	int st = launch_diffusion(s, true, &done);
+	if (st)
+		return st;
+	return done ? BFVM_OK : launch_gradient(s);
+}
+
 int bfvm_gradient_solve(bfvm_solver* s)
 {
 	CHECK_SOLVER(s);
@@ -946,8 +982,11 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
 	if (steps < 0)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "steps must not be negative");
 	REFUSE_SLABS(s, "bfvm_run_steps");
+	// agent copies issued on the copy stream are waited for inside each step, right before its
+	// secretion (one_step); the events exist before any graph is captured, so every graph holds
+	// that wait
 	int oc;
-	if ((oc = order_after_copies(s)))
+	if (s->ag.count > 0 && (oc = ensure_copy_stream(s)))
 		return oc;
 	for (int i = 0; i < steps; i++)
 	{
@@ -1024,6 +1063,8 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 		s->use_tma = value != 0;
 	else if (n == "fused_dirichlet")
 		s->dir_fused = value != 0;
+	else if (n == "fused_gradient")
+		s->grad_fused = value != 0;
 	else if (n == "wait_limit_cycles")
 	{
 		if (value < 10000 || value > 40000000000LL)

@@ -171,6 +171,10 @@ struct bfvm_solver
 	long long launches = 0;
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
 	bool dir_fused = true;		 // staged sweeps of the LOD step write the overwrite that follows them
+	bool grad_fused = true;		 // the z sweep of a step computes the gradient (sweep_tma.cu)
+	int* grad_tile_done = nullptr; // [z tiles] and [1 + z tiles] of the gradient inside the z sweep
+	int* grad_deferred = nullptr;
+	long long grad_tiles = 0;
 	long long wait_limit_cycles = 4000000000LL; // bound of the staged sweeps' waits on tile copies (clock64 cycles;
 												// the default is the kernels' WAIT_LIMIT_CYCLES)
 	long long drop_tile_copy = -1;				// tests only: a staged-sweep tile whose copies are never issued
@@ -238,7 +242,9 @@ int check_device_errors(bfvm_solver* s);	  // waits for the stream, reports devi
 
 // sweep.cu
 int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);
-int launch_diffusion(bfvm_solver* s); // the LOD step, overwrites fused into the staged sweeps
+// the LOD step, overwrites fused into the staged sweeps; with `gradient`, the z sweep also
+// computes the gradient where it can, and *gradient_done tells whether it did
+int launch_diffusion(bfvm_solver* s, bool gradient = false, bool* gradient_done = nullptr);
 // the staged sweep of one axis alone, with launch shape `tune` (groups 0: built-in choice);
 // `handled` is false when the staged path does not take the shape
 int launch_staged_sweep(bfvm_solver* s, int axis, const sweep_tuning& tune, bool& handled);

@@ -244,15 +244,18 @@ int launch_slab_z(bfvm_solver* st)
 }
 
 // The sweep of one axis by the first kernel that takes its shape: the TMA-staged sweep (which sets
-// `staged`), the ensemble sweep on this mesh alone, or the direct kernels.
-static int sweep_axis(bfvm_solver* st, int axis, const sweep_args& a, bool& staged)
+// `staged`; with gf, only if it also computes the gradient), the ensemble sweep on this mesh alone,
+// or the direct kernels.
+static int sweep_axis(bfvm_solver* st, int axis, const sweep_args& a, bool& staged, const grad_fuse* gf = nullptr)
 {
 	const sweep_plan& pl = st->plan[axis];
 	int rc = BFVM_OK;
 	bool handled = false;
 	staged = false;
 	if (st->use_tma)
-		rc = launch_sweep_tma(st, axis, a, handled, &st->tune[axis]);
+		rc = launch_sweep_tma(st, axis, a, handled, &st->tune[axis], nullptr, false, gf);
+	if (!rc && !handled && gf)
+		return sweep_axis(st, axis, a, staged); // the shape cannot take the gradient: sweep alone
 	staged = handled;
 	// the same front-padded block algebra without TMA staging, where the lines fit 16 blocks
 	if (!rc && !handled && st->self_plan && pl.vtab && pl.vP <= ENS_MAX_P && (axis > 0 || st->S <= 32))
@@ -285,16 +288,57 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 // sweep and the overwrite after it.  A staged sweep writes that overwrite itself, tile by tile
 // right after storing the tile, from the list grouped by its tiles; other sweeps are followed by
 // the scatter kernel.
-int launch_diffusion(bfvm_solver* st)
+int launch_diffusion(bfvm_solver* st, bool gradient, bool* gradient_done)
 {
+	if (gradient_done)
+		*gradient_done = false;
 	int rc = launch_dirichlet(st);
 	for (int axis = 0; axis < st->dims && !rc; axis++)
 	{
 		sweep_args a = make_args(st, axis);
 		if (st->dir_fused)
 			a.dir = st->dir_tiles[axis];
+		// the gradient inside the z sweep needs the final field there: no overwrite after it, or
+		// the overwrite written by the sweep itself
+		const bool overwrite_after = st->dir_qcount + st->dir_count > 0;
+		grad_fuse gf;
+		const bool fuse_grad = gradient && axis == 2 && st->grad_fused && st->batch_refs == 0 && st->slab_count == 1
+							   && st->plan[2].vP > 1 && (!overwrite_after || a.dir.items > 0);
+		if (fuse_grad)
+		{
+			const long long items = ((long long)st->grid[1] * st->grid[0] * st->S + 31) / 32; // z tiles
+			if (st->grad_tiles < items)
+			{
+				device_free(st->grad_tile_done);
+				device_free(st->grad_deferred);
+				st->grad_tiles = 0;
+				if ((rc = device_alloc(&st->grad_tile_done, (size_t)items))
+					|| (rc = device_alloc(&st->grad_deferred, (size_t)items + 1)))
+					return rc;
+				st->grad_tiles = items;
+			}
+			gf.g = st->grad;
+			gf.tile_done = st->grad_tile_done;
+			gf.deferred = st->grad_deferred;
+			gf.lag = 0;
+			gf.total = st->V * st->S;
+			gf.X = st->grid[0];
+			gf.Y = st->grid[1];
+			gf.Z = st->grid[2];
+			gf.S = st->S;
+			// the factors of gradient.cu: 1/h at the ends, 1/(2h) inside, rounded to float
+			gf.bx = 1.f / st->voxel[0];
+			gf.cx = 1.f / (st->voxel[0] * 2);
+			gf.by = 1.f / st->voxel[1];
+			gf.cy = 1.f / (st->voxel[1] * 2);
+			gf.bz = 1.f / st->voxel[2];
+			gf.cz = 1.f / (st->voxel[2] * 2);
+			gf.spin_limit = 200000; // about 0.1 ms, then the tile is deferred
+		}
 		bool staged = false;
-		rc = sweep_axis(st, axis, a, staged);
+		rc = sweep_axis(st, axis, a, staged, fuse_grad ? &gf : nullptr);
+		if (!rc && fuse_grad && staged && gradient_done)
+			*gradient_done = true;
 		if (!rc && !(staged && a.dir.items > 0))
 			rc = launch_dirichlet(st);
 	}

@@ -197,9 +197,28 @@ inline int set_smem(K kernel, size_t smem)
 	return BFVM_OK;
 }
 
-// slab_solve (z axis only): the solve pass of a z-slab's sweep
+// The gradient computed inside the z sweep of the step (sweep_tma.cu).  Tile w's final values (its
+// stores and the Dirichlet entries written after them) are published in tile_done[w]; the group
+// that swept tile w then computes the gradient of tile w - lag from the field, whose planes are
+// still in L2, once the tiles holding that tile's x and y neighbours are published.  A group that
+// finds a neighbour unpublished after spin_limit cycles leaves the tile to grad_deferred_kernel,
+// which runs after the sweep (deferred[0] counts the tiles, deferred[1 ...] lists them).
+struct grad_fuse
+{
+	float* g;		 // [3][Z][Y][X][S]
+	int* tile_done;	 // [z tiles], zero before the sweep
+	int* deferred;	 // [1 + z tiles], deferred[0] zero before the sweep
+	long long lag;	 // in tiles
+	long long total; // V * S
+	int X, Y, Z, S;
+	float bx, cx, by, cy, bz, cz;
+	long long spin_limit;
+};
+
+// slab_solve (z axis only): the solve pass of a z-slab's sweep.  gf (z axis only): compute the
+// gradient inside the sweep; `handled` then also means the gradient is (being) computed.
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled,
 					 const sweep_tuning* tune = nullptr, std::vector<sweep_tuning>* shapes = nullptr,
-					 bool slab_solve = false);
+					 bool slab_solve = false, const grad_fuse* gf = nullptr);
 
 } // namespace bfvm

@@ -192,13 +192,139 @@ __device__ __forceinline__ void overwrite_tile(const dirichlet_tiles& d, float* 
 		data[__ldg(&d.sidx[e])] = __ldg(&d.sval[e]);
 }
 
+// ------------------------------------------------------------------------------------------------
+// the gradient inside the z sweep (grad_fuse in sweep_common.cuh)
+
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+	int v;
+	asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+
+// Tile t holds its final values: called by one thread after a barrier of its group that ordered
+// every store of the tile (and the Dirichlet entries written over them).
+__device__ __forceinline__ void publish_tile(const grad_fuse& f, long long t)
+{
+	__threadfence();
+	asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(f.tile_done + t), "r"(1) : "memory");
+}
+
+// The gradient of z tile g: columns 32g .. 32g + 31 of the y*x*s plane over every plane, the same
+// arithmetic as gradient.cu (bit for bit).  Thread (lane, j) of a group of P warps marches column
+// 32g + lane over planes [j c, (j + 1) c), c = ceil(Z / P), keeping u(z-1), u(z), u(z+1) in
+// registers; x and y neighbours are read through L2 (coherent loads: other CTAs wrote them in this
+// kernel), the three components are stored streaming.
+__device__ __forceinline__ void gradient_tile(const grad_fuse& f, const float* u, long long g, int lane, int j, int P)
+{
+	const long long plane = (long long)f.Y * f.X * f.S;
+	const long long q = g * 32 + lane;
+	if (q >= plane)
+		return;
+	const int XS = f.X * f.S;
+	const int y = (int)(q / XS);
+	const int x = (int)(q - (long long)y * XS) / f.S;
+	const int chunk = (f.Z + P - 1) / P;
+	const int z0 = j * chunk;
+	const int z1 = min(f.Z, z0 + chunk);
+	if (z0 >= z1)
+		return;
+	const int xo_hi = x == f.X - 1 ? 0 : f.S, xo_lo = x == 0 ? 0 : f.S;
+	const float fx = (x == 0 || x == f.X - 1) ? f.bx : f.cx;
+	const int yo_hi = y == f.Y - 1 ? 0 : XS, yo_lo = y == 0 ? 0 : XS;
+	const float fy = (y == 0 || y == f.Y - 1) ? f.by : f.cy;
+	const float* p = u + (long long)z0 * plane + q;
+	float* gp = f.g + (long long)z0 * plane + q;
+	float prev = z0 > 0 ? __ldcg(p - plane) : 0.f;
+	float cur = __ldcg(p);
+	for (int z = z0; z < z1; z++, p += plane, gp += plane)
+	{
+		const float next = z + 1 < f.Z ? __ldcg(p + plane) : cur;
+		const float gx = f.X == 1 ? 0.f : __fmul_rn(__fsub_rn(__ldcg(p + xo_hi), __ldcg(p - xo_lo)), fx);
+		const float gy = f.Y == 1 ? 0.f : __fmul_rn(__fsub_rn(__ldcg(p + yo_hi), __ldcg(p - yo_lo)), fy);
+		float gz;
+		if (z == 0)
+			gz = __fmul_rn(__fsub_rn(next, cur), f.bz);
+		else if (z == f.Z - 1)
+			gz = __fmul_rn(__fsub_rn(cur, prev), f.bz);
+		else
+			gz = __fmul_rn(__fsub_rn(next, prev), f.cz);
+		__stcs(gp, gx);
+		__stcs(gp + f.total, gy);
+		__stcs(gp + 2 * f.total, gz);
+		prev = cur;
+		cur = next;
+	}
+}
+
+// Whether the tiles holding the x and y neighbours of tile g (and g itself) are published: the
+// group's threads each watch some of them, for at most spin_limit cycles.
+__device__ __forceinline__ bool neighbours_ready(const grad_fuse& f, long long g, int gtid, int gthr, int bar_id)
+{
+	const long long plane = (long long)f.Y * f.X * f.S;
+	const long long XS = (long long)f.X * f.S;
+	const long long c0 = g * 32, c1 = min(c0 + 31, plane - 1);
+	const long long lo[3] = { c0 - f.S, c0 - XS, c0 + XS }, hi[3] = { c1 + f.S, c1 - XS, c1 + XS };
+	long long first[3];
+	int count[3], total = 0;
+	for (int r = 0; r < 3; r++)
+	{
+		const long long a = max(lo[r], 0LL), b = min(hi[r], plane - 1);
+		first[r] = a >> 5;
+		count[r] = a > b ? 0 : (int)((b >> 5) - (a >> 5) + 1);
+		total += count[r];
+	}
+	bool ok = true;
+	for (int k = gtid; k < total; k += gthr)
+	{
+		const long long t = k < count[0] ? first[0] + k
+										 : (k < count[0] + count[1] ? first[1] + (k - count[0])
+																	: first[2] + (k - count[0] - count[1]));
+		const long long start = clock64();
+		while (ld_acquire(f.tile_done + t) == 0)
+		{
+			if (clock64() - start > f.spin_limit)
+			{
+				ok = false;
+				break;
+			}
+			__nanosleep(100);
+		}
+	}
+	return group_sync_and(bar_id, gthr, ok);
+}
+
+// The gradient of tile g by a group: now if its neighbours are published, else left to
+// grad_deferred_kernel.
+__device__ __forceinline__ void gradient_work(const grad_fuse& f, const float* u, long long g, int lane, int j, int P,
+											  int bar_id)
+{
+	const int gtid = lane + 32 * j, gthr = 32 * P;
+	if (neighbours_ready(f, g, gtid, gthr, bar_id))
+		gradient_tile(f, u, g, lane, j, P);
+	else if (gtid == 0)
+	{
+		const int k = atomicAdd(f.deferred, 1);
+		f.deferred[1 + k] = (int)g;
+	}
+}
+
+// The tiles whose gradient the sweep left behind, after the sweep: CTAs of (32, P) threads.
+__global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constant__ grad_fuse f, const float* u)
+{
+	const int n = *(volatile int*)f.deferred;
+	for (int k = blockIdx.x; k < n; k += gridDim.x)
+		gradient_tile(f, u, f.deferred[1 + k], threadIdx.x, threadIdx.y, blockDim.y);
+}
+
 // SLAB (y/z tiles only): 0 a plain sweep; 1 the solve pass of a z-slab, which enters every line
 // with the carries C (left) and X (right) of slab_carry: it always runs the carry folds, from C and
 // X instead of zero, with the tables of precompute_padded_range.
-template <bool ROWS, bool NOALLOC, int SLAB>
+// GRAD (z sweep, P > 1): the gradient of the step inside the sweep (grad_fuse).
+template <bool ROWS, bool NOALLOC, int SLAB, bool GRAD>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
-					 const __grid_constant__ tma_tile tt)
+					 const __grid_constant__ tma_tile tt, const __grid_constant__ grad_fuse gf)
 {
 	constexpr int M = 32;
 	extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -372,6 +498,10 @@ __global__ void __launch_bounds__(640, 1)
 			// this block's first solution element without the right carry
 			carry_t[j * 32 + lane] = fmaf(C, __ldg(&tgptab[j * S + s]), d[0]);
 			group_sync(bar_id, gthr);
+			// the previous tile's stores (before the first barrier) and its Dirichlet entries
+			// (before this one) are all done
+			if (GRAD && leader && it > 0)
+				publish_tile(gf, w - wstride);
 			// right carry X = x_{q+1}: fold the blocks to the right, X_k = x^k_p + Gp_k X_{k+1}
 			float Xc = 0.f;
 			if (j < P - 1)
@@ -422,12 +552,27 @@ __global__ void __launch_bounds__(640, 1)
 				}
 			}
 		}
+		if (GRAD && w >= gf.lag)
+			gradient_work(gf, a.data, w - gf.lag, lane, j, P, bar_id);
 	}
 
 	if (!failed && a.dir.items > 0 && it > 0)
 	{
 		group_sync(bar_id, gthr); // the last tile's stores, then its entries
 		overwrite_tile(a.dir, a.data, w - wstride, lane + 32 * j, gthr);
+	}
+	if (GRAD && !failed)
+	{
+		if (it > 0)
+		{
+			group_sync(bar_id, gthr);
+			if (leader)
+				publish_tile(gf, w - wstride);
+		}
+		// the gradients still owed: tiles w - lag of this group's stride past the last tile
+		for (; w - gf.lag < tt.items; w += wstride)
+			if (w >= gf.lag)
+				gradient_work(gf, a.data, w - gf.lag, lane, j, P, bar_id);
 	}
 	if (failed && leader)
 	{
@@ -466,25 +611,42 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 
 static constexpr int TMA_MAX_P = 16;
 
-template <bool ROWS, bool NOALLOC, int SLAB = 0>
+template <bool ROWS, bool NOALLOC, int SLAB = 0, bool GRAD = false>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
-							  size_t smem)
+							  size_t smem, const grad_fuse* gfp = nullptr)
 {
-	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB>;
+	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
 	const int threads = 32 * a.vP * tt.groups;
 	const int grid = persistent_grid(kernel, threads, smem, (tt.items + tt.groups - 1) / tt.groups, st->device);
-	kernel<<<grid, dim3(32, a.vP, tt.groups), smem, st->stream>>>(a, map, tt);
-	return check_launch(st, tt.axis == 0 ? "sweep_tma<x>"
-										 : (tt.axis == 1 ? "sweep_tma<y>" : (SLAB ? "sweep_tma<z slab>" : "sweep_tma<z>")));
+	grad_fuse gf;
+	std::memset(&gf, 0, sizeof(gf));
+	if (GRAD)
+	{
+		gf = *gfp;
+		// lag: the widest neighbour reach in tiles (a row of the y*x*s plane, plus S) and two
+		// strides of the persistent groups, so the neighbours are normally published in time
+		const long long XS = (long long)gf.X * gf.S;
+		const long long reach = (XS + gf.S + 31) / 32 + 1;
+		gf.lag = reach + 2LL * grid * tt.groups + 32;
+		BFVM_CUDA(cudaMemsetAsync(gf.tile_done, 0, (size_t)tt.items * sizeof(int), st->stream));
+		BFVM_CUDA(cudaMemsetAsync(gf.deferred, 0, sizeof(int), st->stream));
+	}
+	kernel<<<grid, dim3(32, a.vP, tt.groups), smem, st->stream>>>(a, map, tt, gf);
+	rc = check_launch(st, tt.axis == 0 ? "sweep_tma<x>"
+									   : (tt.axis == 1 ? "sweep_tma<y>" : (SLAB ? "sweep_tma<z slab>" : "sweep_tma<z>")));
+	if (rc || !GRAD)
+		return rc;
+	grad_deferred_kernel<<<sm_count_impl(st->device) * 2, dim3(32, a.vP), 0, st->stream>>>(gf, a.data);
+	return check_launch(st, "grad_deferred_kernel");
 }
 
 // tune: launch shape to use (groups 0: the built-in choice).  shapes: when given, nothing is
 // launched; the launch shapes that fit are listed instead.
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled, const sweep_tuning* tune,
-					 std::vector<sweep_tuning>* shapes, bool slab_solve)
+					 std::vector<sweep_tuning>* shapes, bool slab_solve, const grad_fuse* gf)
 {
 	if (slab_solve && axis != 2)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab passes exist for the z sweep only");
@@ -615,6 +777,11 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		return launch_tma_variant<false, true>(st, a, map, tt, smem);
 	if (slab_solve)
 		return launch_tma_variant<false, false, 1>(st, a, map, tt, smem);
+	if (gf && a.vP > 1)
+		return launch_tma_variant<false, false, 0, true>(st, a, map, tt, smem, gf);
+	handled = !gf; // a gradient was asked for and this shape cannot compute it: the caller sweeps
+	if (!handled)
+		return BFVM_OK;
 	return launch_tma_variant<false, false>(st, a, map, tt, smem);
 }
 

@@ -174,3 +174,23 @@ def test_fused_dirichlet_identical_to_scatter(edge, S, dims):
     fused.diffusion()
     plain.diffusion()
     np.testing.assert_array_equal(fused.densities(), plain.densities())
+
+
+@pytest.mark.parametrize("edge,S,dirichlet", [(96, 16, True), (70, 4, True), (54, 2, False), (40, 8, True),
+                                              (100, 5, False)])
+def test_gradient_inside_z_sweep_identical(edge, S, dirichlet):
+    """Within a step the z sweep computes the gradient itself, tile by tile once the neighbouring
+    tiles hold their final values (option fused_gradient; 0 runs the gradient kernel after the
+    sweep).  The gradients and fields must be the same bits.  The cases cover tiles that straddle
+    rows of the y*x*s plane (54 x 2), meshes smaller than the lag (every gradient after the sweep
+    loop), and steps with and without the Dirichlet overwrite written by the sweep."""
+    scn = synthetic(edge, S, 1200, seed=3 * edge + S, clustered=True, sigma=60.0,
+                    interior_fraction=0.02 if dirichlet else 0.0, boundary_substrate0=dirichlet)
+    fused = gpu_runner(scn)
+    plain = gpu_runner(scn)
+    plain.s.set_option("fused_gradient", 0)
+    for first, n in ((0, 3), (3, 9)):
+        fused.run_steps(n, first)
+        plain.run_steps(n, first)
+        np.testing.assert_array_equal(fused.gradients(), plain.gradients())
+        np.testing.assert_array_equal(fused.densities(), plain.densities())
