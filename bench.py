@@ -467,6 +467,7 @@ def measure_batch(steps, warmup, clocks=True):
     for s in batched + alone:
         s.set_stream(stream.cuda_stream)
     b = Batch(batched)
+    tuned = b.autotune()
     b.run_steps(warmup, 0)
     b.synchronize()
     sampler = ClockSampler(physical_gpu_index(0)) if clocks else None
@@ -496,7 +497,7 @@ def measure_batch(steps, warmup, clocks=True):
     for s in batched + alone:
         s.close()
     return {"instances": len(ws), "voxel_substrates": units, "ms_batch": ms_batch, "ms_sequential": ms_seq,
-            "launches": launches, "clocks": clock_rec, "max_rel_l2_vs_alone": worst}
+            "launches": launches, "clocks": clock_rec, "max_rel_l2_vs_alone": worst, "autotuned": tuned}
 
 
 def run_batch(args):
@@ -515,6 +516,7 @@ def run_batch(args):
                        "what": "the same instances stepped one after another on one stream (bfvm_run_steps)"},
         "speedup_vs_sequential": value / seq,
         "max_rel_l2_vs_alone": r["max_rel_l2_vs_alone"],
+        "autotuned": r["autotuned"],
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
@@ -1161,7 +1163,7 @@ def side_forms():
         "ms_per_step": b["ms_batch"] / 10, "value": units * 10 / (b["ms_batch"] / 1e3), "unit": UNIT,
         "sequential_ms_per_step": b["ms_sequential"] / 10,
         "speedup_vs_sequential": b["ms_sequential"] / b["ms_batch"],
-        "max_rel_l2_vs_alone": b["max_rel_l2_vs_alone"], "gpu_launches": b["launches"]}
+        "max_rel_l2_vs_alone": b["max_rel_l2_vs_alone"], "autotuned": b["autotuned"], "gpu_launches": b["launches"]}
     r = measure_surrogate(train_steps=5, warmup=3)
     fb = r["fallback_run"]
     out["surrogate_128"] = {

@@ -197,6 +197,10 @@ int bfvm_synchronize(bfvm_solver* s);
  * - "fused_dirichlet" 0/1: in the LOD step (bfvm_diffusion_solve, bfvm_run_steps) a staged sweep
  *   writes the Dirichlet overwrite that follows it, tile by tile (default 1; 0 runs it as a
  *   separate scatter).  Results are identical either way.
+ * - "fused_gradient" 0/1: in bfvm_run_steps and bfvm_diffusion_gradient_solve the z sweep computes
+ *   the gradient from the planes it has just written (default 1; 0 runs the gradient kernel after
+ *   the sweep).  Results are identical either way.  "fused_gradient_evict_first" 0/1 (default 1):
+ *   that sweep reads its tiles with an L2 evict-first policy, keeping the written planes in L2.
  * - "wait_limit_cycles" bounds every wait of the staged sweeps on a tile copy, in GPU clock cycles
  *   (default 4e9, about two seconds; accepted range [1e4, 4e10]).  A wait that runs out makes the
  *   kernel give up its tile, let its copies in flight land and return; the next synchronising call
@@ -250,6 +254,17 @@ int bfvm_batch_create(bfvm_batch** out, int32_t count, bfvm_solver* const* solve
 int bfvm_batch_destroy(bfvm_batch* b);
 int bfvm_batch_run_steps(bfvm_batch* b, int32_t steps, int32_t first_step);
 int bfvm_batch_synchronize(bfvm_batch* b);
+/*
+ * Autotuning of a batch (no counterpart in the reference): time each launch choice of the
+ * ensemble kernels on scratch copies of the instances' fields and gradients, phase by phase, and
+ * keep the fastest for this batch and, for the rest of the process, for batches of the same
+ * meshes.  The choices: per sweep axis the register cap (1 or 2 CTAs of up to 512 threads per SM)
+ * and CTAs per slot of tiles (1, 2, 4); for the gradient the planes per work unit (32, 64, 128)
+ * and per batch of loads (4, 8).  choices, if not NULL, receives [8] = minb x/y/z, split x/y/z,
+ * gradient planes, gradient load batch.  Results do not depend on the choices.  Needs one
+ * field-and-gradient's worth of scratch for every instance.
+ */
+int bfvm_batch_autotune(bfvm_batch* b, int32_t* choices);
 
 /*
  * z-slabs (no counterpart in the reference, whose solvers hold a whole mesh on one device): one 3D

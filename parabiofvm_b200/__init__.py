@@ -288,6 +288,14 @@ class Batch:
     def synchronize(self):
         check(self._lib.bfvm_batch_synchronize(self._h))
 
+    def autotune(self):
+        """Time the ensemble kernels' launch choices (bfvm_batch_autotune) and keep the fastest;
+        returns them."""
+        c = (ctypes.c_int32 * 8)()
+        check(self._lib.bfvm_batch_autotune(self._h, c))
+        return {"sweep_ctas_per_sm": list(c[0:3]), "sweep_ctas_per_slot": list(c[3:6]), "gradient_planes": c[6],
+                "gradient_load_batch": c[7]}
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             self._lib.bfvm_batch_destroy(self._h)

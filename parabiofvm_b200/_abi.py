@@ -67,6 +67,7 @@ SIGNATURES = {
     "bfvm_batch_destroy": (c_int, [c_void_p]),
     "bfvm_batch_run_steps": (c_int, [c_void_p, c_int32, c_int32]),
     "bfvm_batch_synchronize": (c_int, [c_void_p]),
+    "bfvm_batch_autotune": (c_int, [c_void_p, P(c_int32)]),
     "bfvm_create_slab": (c_int, [P(c_void_p), c_int, P(c_int32), P(c_int32), P(c_int32), c_int32, c_float,
                                  P(c_float), P(c_float), c_int, c_int32, P(c_int32), c_int32]),
     "bfvm_slab_info": (c_int, [c_void_p, P(c_int32), P(c_int32), P(c_int32), P(c_int32)]),

@@ -12,6 +12,9 @@
 // (its graph epoch advances).
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "agent_kernels.cuh"
@@ -31,6 +34,8 @@ struct bfvm_batch
 	bfvm::ensemble_plan ens[2];			 // descriptors of the ensemble meshes captured in graph[rc]
 	long long ens_kernels[2] = { 0, 0 }; // ensemble launches in graph[rc] (counted on the first mesh)
 	bool holds_refs = false;			 // the instances count this batch in batch_refs
+	bool tuned = false;					 // bfvm_batch_autotune chose `tune`
+	bfvm::ens_tuning tune;
 };
 
 namespace bfvm {
@@ -52,6 +57,43 @@ static bool batch_graph_current(const bfvm_batch* b, int rc)
 	return true;
 }
 
+// The autotuner's choices for batches of the same meshes, for the rest of the process.
+static std::mutex g_tune_lock;
+static std::map<std::string, ens_tuning> g_tune_cache;
+
+static std::vector<bfvm_solver*> ensemble_members(const bfvm_batch* b)
+{
+	std::vector<bfvm_solver*> m;
+	for (bfvm_solver* s : b->inst)
+		if (ensemble_eligible(s))
+			m.push_back(s);
+	return m;
+}
+
+// the shapes the ensemble kernels see: per member dims, grid, substrates and blocks per line
+static std::string ensemble_signature(const std::vector<bfvm_solver*>& members)
+{
+	std::string sig;
+	for (const bfvm_solver* s : members)
+	{
+		sig += std::to_string(s->dims) + ":" + std::to_string(s->grid[0]) + "," + std::to_string(s->grid[1]) + ","
+			   + std::to_string(s->grid[2]) + "x" + std::to_string(s->S);
+		for (int d = 0; d < s->dims; d++)
+			sig += "/" + std::to_string(s->plan[d].vP);
+		sig += ";";
+	}
+	return sig;
+}
+
+static ens_tuning batch_tuning(const bfvm_batch* b, const std::vector<bfvm_solver*>& members)
+{
+	if (b->tuned)
+		return b->tune;
+	std::lock_guard<std::mutex> g(g_tune_lock);
+	const auto it = g_tune_cache.find(ensemble_signature(members));
+	return it == g_tune_cache.end() ? ens_tuning() : it->second;
+}
+
 static int batch_capture(bfvm_batch* b, int rc)
 {
 	batch_free_graph(b, rc);
@@ -66,7 +108,7 @@ static int batch_capture(bfvm_batch* b, int rc)
 			members.push_back(b->inst[i]);
 			in_ens[i] = 1;
 		}
-	int st = ensemble_build(b->ens[rc], members);
+	int st = ensemble_build(b->ens[rc], members, batch_tuning(b, members));
 	if (st)
 		return st;
 	const ensemble_plan& plan = b->ens[rc];
@@ -317,6 +359,140 @@ int bfvm_batch_run_steps(bfvm_batch* b, int32_t steps, int32_t first_step)
 		b->inst[0]->launches += b->ens_kernels[rc];
 	}
 	return instances_wait_batch(b);
+}
+
+// Time each launch choice of the ensemble kernels on scratch copies of the members' fields and
+// gradients (so the instances' state is untouched), phase by phase, and keep the fastest.
+int bfvm_batch_autotune(bfvm_batch* b, int32_t* choices)
+{
+	if (!b)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "null batch");
+	BFVM_CUDA(cudaSetDevice(b->device));
+	const std::vector<bfvm_solver*> members = ensemble_members(b);
+	ens_tuning best;
+	int st = BFVM_OK;
+	if (!members.empty())
+	{
+		if ((st = batch_wait_instances(b)))
+			return st;
+		// one scratch block: each member's field then its gradient
+		std::vector<std::pair<float*, float*>> bufs(members.size());
+		size_t total = 0;
+		for (const bfvm_solver* s : members)
+			total += (size_t)s->V * s->S * (1 + s->dims);
+		float* scratch = nullptr;
+		if ((st = device_alloc(&scratch, total)))
+			return st;
+		size_t at = 0;
+		for (size_t i = 0; i < members.size() && !st; i++)
+		{
+			const bfvm_solver* s = members[i];
+			const size_t vs = (size_t)s->V * s->S;
+			bufs[i] = { scratch + at, scratch + at + vs };
+			at += vs * (1 + s->dims);
+			const cudaError_t e = cudaMemcpyAsync(bufs[i].first, s->dens, vs * sizeof(float), cudaMemcpyDeviceToDevice,
+												  b->stream);
+			if (e != cudaSuccess)
+				st = cuda_fail(e, "cudaMemcpyAsync(autotune scratch)");
+		}
+		cudaEvent_t e0 = nullptr, e1 = nullptr;
+		if (!st && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+			st = cuda_fail(cudaGetLastError(), "cudaEventCreate");
+		ensemble_plan plan;
+		// device time of `phase` under tuning t: one launch to warm up, the mean of three
+		auto time_phase = [&](const ens_tuning& t, auto phase, float& ms) -> int {
+			int r = ensemble_build(plan, members, t, &bufs);
+			if (!r)
+				r = phase(plan);
+			for (int k = 0; k < 3 && !r; k++)
+			{
+				if (k == 0)
+					BFVM_CUDA(cudaEventRecord(e0, b->stream));
+				r = phase(plan);
+			}
+			if (r)
+				return r;
+			BFVM_CUDA(cudaEventRecord(e1, b->stream));
+			BFVM_CUDA(cudaEventSynchronize(e1));
+			BFVM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+			return BFVM_OK;
+		};
+		int maxdims = 0;
+		for (const bfvm_solver* s : members)
+			maxdims = std::max(maxdims, s->dims);
+		for (int axis = 0; axis < maxdims && !st; axis++)
+		{
+			float best_ms = 0.f;
+			ens_tuning keep = best;
+			bool first = true;
+			for (int minb : { 2, 1 })
+				for (int split : { 1, 2, 4 })
+				{
+					ens_tuning t = best;
+					t.sweep_minb[axis] = minb;
+					t.sweep_split[axis] = split;
+					float ms = 0.f;
+					if ((st = time_phase(t, [&](const ensemble_plan& p) { return ensemble_sweep(p, axis, b->stream); }, ms)))
+						break;
+					if (first || ms < best_ms)
+					{
+						best_ms = ms;
+						keep = t;
+						first = false;
+					}
+				}
+			best = keep;
+		}
+		if (!st)
+		{
+			float best_ms = 0.f;
+			ens_tuning keep = best;
+			bool first = true;
+			for (int zc : { 64, 32, 128 })
+				for (int zu : { 8, 4 })
+				{
+					ens_tuning t = best;
+					t.grad_zc = zc;
+					t.grad_zu = zu;
+					float ms = 0.f;
+					if ((st = time_phase(t, [&](const ensemble_plan& p) { return ensemble_gradient(p, b->stream); }, ms)))
+						break;
+					if (first || ms < best_ms)
+					{
+						best_ms = ms;
+						keep = t;
+						first = false;
+					}
+				}
+			best = keep;
+		}
+		cudaStreamSynchronize(b->stream);
+		ensemble_free(plan);
+		if (e0)
+			cudaEventDestroy(e0);
+		if (e1)
+			cudaEventDestroy(e1);
+		device_free(scratch);
+		if (st)
+			return st;
+		std::lock_guard<std::mutex> g(g_tune_lock);
+		g_tune_cache[ensemble_signature(members)] = best;
+	}
+	b->tune = best;
+	b->tuned = true;
+	batch_free_graph(b, 0);
+	batch_free_graph(b, 1);
+	if (choices)
+	{
+		for (int d = 0; d < 3; d++)
+		{
+			choices[d] = best.sweep_minb[d];
+			choices[3 + d] = best.sweep_split[d];
+		}
+		choices[6] = best.grad_zc;
+		choices[7] = best.grad_zu;
+	}
+	return BFVM_OK;
 }
 
 int bfvm_batch_synchronize(bfvm_batch* b)

@@ -55,14 +55,13 @@ __global__ void __launch_bounds__(256) ens_dirichlet_kernel(const ens_inst* __re
 }
 
 // central differences (gradient.cu); output layouts 1D [x][s][1], 2D [y][x][s][2], 3D [3][z][y][x][s].
-// One unit is 256 consecutive columns of the (y, x, s) plane over up to ENS_GRAD_ZC planes: each
-// thread marches z keeping u(z-1), u(z), u(z+1) in registers (gradient3d_vec4_kernel of gradient.cu
-// for any S), reading x and y neighbours from L1/L2.  A thread's x and y never change along z, so
-// the one-sided or central form of each axis is fixed once as two neighbour offsets and a factor;
-// z advances ENS_GRAD_ZU planes at a time with every load of those planes issued before their
-// arithmetic, which keeps enough loads in flight for small meshes to stream at HBM rate.
-static constexpr int ENS_GRAD_ZC = 64;
-static constexpr int ENS_GRAD_ZU = 8;
+// One unit is 256 consecutive columns of the (y, x, s) plane over up to ZC planes: each thread
+// marches z keeping u(z-1), u(z), u(z+1) in registers (gradient3d_vec4_kernel of gradient.cu for
+// any S), reading x and y neighbours from L1/L2.  A thread's x and y never change along z, so the
+// one-sided or central form of each axis is fixed once as two neighbour offsets and a factor; z
+// advances ZU planes at a time with every load of those planes issued before their arithmetic,
+// which keeps enough loads in flight for small meshes to stream at HBM rate.  ZC and ZU are launch
+// choices (ens_tuning).
 
 // neighbour offsets lo, hi and factor of an axis at position pos of n: (u[1] - u[0]) / h at the
 // first voxel, (u[n-1] - u[n-2]) / h at the last, (u[i+1] - u[i-1]) / (2h) inside; an axis of one
@@ -97,13 +96,13 @@ __device__ __forceinline__ void axis_form(int pos, int n, long long stride, floa
 
 // The z march of one column of a 3-D mesh over planes [z0, z1): p and g point at plane z0 of the
 // column in the field and in the x component of the gradient.  Planes that have a next plane run
-// ENS_GRAD_ZU at a time without guards, through pointers that advance a plane per step; the rest
-// (up to ENS_GRAD_ZU - 1 planes, and the mesh's last plane) run one at a time.
+// U at a time without guards, through pointers that advance a plane per step; the rest (up to
+// U - 1 planes, and the mesh's last plane) run one at a time.
+template <int U>
 __device__ __forceinline__ void ens_gradient_3d(const ens_inst& m, const float* __restrict__ p, float* __restrict__ g,
 												long long plane, int z0, int z1, long long xlo, long long xhi,
 												float fx, long long ylo, long long yhi, float fy)
 {
-	constexpr int U = ENS_GRAD_ZU;
 	const int Z = m.Z;
 	const long long total = plane * Z;
 	const bool hasx = m.X > 1, hasy = m.Y > 1;
@@ -169,10 +168,10 @@ __device__ __forceinline__ void ens_gradient_3d(const ens_inst& m, const float* 
 // ALL3D: every mesh is 3-D.  The kernel then holds the 3-D march alone, which fits 64 registers, so
 // four CTAs share an SM: twice the loads in flight of the kernel that also holds the 1-D and 2-D
 // forms (held to 128 registers, two CTAs).
-template <bool ALL3D>
+template <bool ALL3D, int ZU>
 __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const ens_inst* __restrict__ inst,
 																		   const long long* __restrict__ first,
-																		   int count, long long units)
+																		   int count, long long units, int ZC)
 {
 	for (long long u = blockIdx.x; u < units; u += gridDim.x)
 	{
@@ -184,8 +183,8 @@ __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const 
 		const int ncx = (plane_cols + 255) / 256;
 		const int local = (int)(u - first[i]);
 		const int cx = local % ncx;
-		const int z0 = (local / ncx) * ENS_GRAD_ZC;
-		const int z1 = min(Z, z0 + ENS_GRAD_ZC);
+		const int z0 = (local / ncx) * ZC;
+		const int z1 = min(Z, z0 + ZC);
 		const int c = cx * 256 + threadIdx.x; // column of the plane: y * XS + q
 		if (c >= plane_cols)
 			continue;
@@ -205,17 +204,17 @@ __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const 
 		if (ALL3D || dims == 3)
 		{
 			const long long e0 = (long long)z0 * plane + row;
-			ens_gradient_3d(m, d + e0, g + e0, plane, z0, z1, xlo, xhi, fx, ylo, yhi, fy);
+			ens_gradient_3d<ZU>(m, d + e0, g + e0, plane, z0, z1, xlo, xhi, fx, ylo, yhi, fy);
 			continue;
 		}
 		float prev = z0 > 0 ? __ldg(&d[(long long)(z0 - 1) * plane + row]) : 0.f;
 		float cur = __ldg(&d[(long long)z0 * plane + row]);
-		for (int z = z0; z < z1; z += ENS_GRAD_ZU)
+		for (int z = z0; z < z1; z += ZU)
 		{
 			// every load of these planes first
-			float nx[ENS_GRAD_ZU], xa[ENS_GRAD_ZU], xb[ENS_GRAD_ZU], ya[ENS_GRAD_ZU], yb[ENS_GRAD_ZU];
+			float nx[ZU], xa[ZU], xb[ZU], ya[ZU], yb[ZU];
 #pragma unroll
-			for (int k = 0; k < ENS_GRAD_ZU; k++)
+			for (int k = 0; k < ZU; k++)
 			{
 				const int zz = z + k;
 				const long long e = (long long)zz * plane + row;
@@ -227,7 +226,7 @@ __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const 
 				yb[k] = (in && dims >= 2) ? __ldg(&d[e + ylo]) : 0.f;
 			}
 #pragma unroll
-			for (int k = 0; k < ENS_GRAD_ZU; k++)
+			for (int k = 0; k < ZU; k++)
 			{
 				const int zz = z + k;
 				if (zz >= z1)
@@ -322,8 +321,8 @@ __device__ __forceinline__ void x_tile_rows(const ens_inst& m, long long local, 
 // double-buffered, measured 8% slower over a 256-mesh ensemble.)
 // Two CTAs of 512 threads per SM (64 registers): at 114 registers a mesh of 3 blocks per line ran 5
 // CTAs of 3 warps per SM, too few warps to hide the loads and barriers.
-template <int AXIS>
-__global__ void __launch_bounds__(512, 2) ens_sweep_kernel(const ens_inst* __restrict__ inst,
+template <int AXIS, int MINB>
+__global__ void __launch_bounds__(512, MINB) ens_sweep_kernel(const ens_inst* __restrict__ inst,
 														 const long long* __restrict__ first, int count,
 														 long long units, long long chunk, int maxP)
 {
@@ -490,9 +489,11 @@ void ensemble_free(ensemble_plan& plan)
 	plan.count = 0;
 }
 
-int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
+int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes, const ens_tuning& tune,
+				   const std::vector<std::pair<float*, float*>>* buffers)
 {
 	ensemble_free(plan);
+	plan.tune = tune;
 	const int n = (int)meshes.size();
 	if (n == 0)
 		return BFVM_OK;
@@ -507,8 +508,8 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
 	{
 		const bfvm_solver* s = meshes[i];
 		ens_inst& m = h[i];
-		m.dens = s->dens;
-		m.grad = s->grad;
+		m.dens = buffers ? (*buffers)[i].first : s->dens;
+		m.grad = buffers ? (*buffers)[i].second : s->grad;
 		m.dims = s->dims;
 		plan.all3d = plan.all3d && s->dims == 3;
 		m.S = s->S;
@@ -552,7 +553,7 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes)
 		units[ENS_SWEEP_X] = R > 0 ? (Y * Z + R - 1) / R : 0;
 		units[ENS_SWEEP_Y] = s->dims >= 2 ? Z * ((XS + 31) / 32) : 0;
 		units[ENS_SWEEP_Z] = s->dims >= 3 ? (Y * XS + 31) / 32 : 0;
-		units[ENS_GRADIENT] = ((XS * Y + 255) / 256) * ((Z + ENS_GRAD_ZC - 1) / ENS_GRAD_ZC);
+		units[ENS_GRADIENT] = ((XS * Y + 255) / 256) * ((Z + tune.grad_zc - 1) / tune.grad_zc);
 		units[ENS_SECRETION] = (m.AS + 255) / 256;
 		for (int ph = 0; ph < ENS_PHASES; ph++)
 			plan.first_h[ph][i + 1] = plan.first_h[ph][i] + units[ph];
@@ -606,17 +607,26 @@ int ensemble_dirichlet(const ensemble_plan& plan, int phase, cudaStream_t stream
 	return launched("ens_dirichlet_kernel");
 }
 
+template <int ZU>
+static void launch_ens_gradient(const ensemble_plan& plan, long long units, cudaStream_t stream)
+{
+	if (plan.all3d)
+		ens_gradient_kernel<true, ZU><<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT],
+																			   plan.count, units, plan.tune.grad_zc);
+	else
+		ens_gradient_kernel<false, ZU><<<element_grid(units), 256, 0, stream>>>(
+			plan.inst, plan.first[ENS_GRADIENT], plan.count, units, plan.tune.grad_zc);
+}
+
 int ensemble_gradient(const ensemble_plan& plan, cudaStream_t stream)
 {
 	const long long units = plan.count ? plan.first_h[ENS_GRADIENT][plan.count] : 0;
 	if (units == 0)
 		return BFVM_OK;
-	if (plan.all3d)
-		ens_gradient_kernel<true><<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT],
-																		   plan.count, units);
+	if (plan.tune.grad_zu == 4)
+		launch_ens_gradient<4>(plan, units, stream);
 	else
-		ens_gradient_kernel<false><<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT],
-																			plan.count, units);
+		launch_ens_gradient<8>(plan, units, stream);
 	return launched("ens_gradient_kernel");
 }
 
@@ -630,10 +640,10 @@ int ensemble_secretion(const ensemble_plan& plan, cudaStream_t stream)
 	return launched("ens_secretion_kernel");
 }
 
-template <int AXIS>
+template <int AXIS, int MINB>
 static int launch_ens_sweep(const ensemble_plan& plan, long long units, cudaStream_t stream)
 {
-	auto kernel = ens_sweep_kernel<AXIS>;
+	auto kernel = ens_sweep_kernel<AXIS, MINB>;
 	const int P = plan.maxP[AXIS];
 	const size_t smem = (2 * (size_t)P * 32 + plan.table_floats[AXIS]) * sizeof(float);
 	int rc = set_smem(kernel, smem);
@@ -641,7 +651,7 @@ static int launch_ens_sweep(const ensemble_plan& plan, long long units, cudaStre
 		return rc;
 	int per_sm = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * P, smem);
-	const long long slots = (long long)std::max(per_sm, 1) * current_device_sms();
+	const long long slots = (long long)std::max(per_sm, 1) * current_device_sms() * plan.tune.sweep_split[AXIS];
 	const long long chunk = std::max<long long>(1, (units + slots - 1) / slots);
 	const unsigned grid = (unsigned)((units + chunk - 1) / chunk);
 	kernel<<<grid, dim3(32, P), smem, stream>>>(plan.inst, plan.first[ENS_SWEEP_X + AXIS], plan.count, units, chunk, P);
@@ -653,11 +663,12 @@ int ensemble_sweep(const ensemble_plan& plan, int axis, cudaStream_t stream)
 	const long long units = plan.count ? plan.first_h[ENS_SWEEP_X + axis][plan.count] : 0;
 	if (units == 0)
 		return BFVM_OK;
+	const bool one = plan.tune.sweep_minb[axis] == 1;
 	if (axis == 0)
-		return launch_ens_sweep<0>(plan, units, stream);
+		return one ? launch_ens_sweep<0, 1>(plan, units, stream) : launch_ens_sweep<0, 2>(plan, units, stream);
 	if (axis == 1)
-		return launch_ens_sweep<1>(plan, units, stream);
-	return launch_ens_sweep<2>(plan, units, stream);
+		return one ? launch_ens_sweep<1, 1>(plan, units, stream) : launch_ens_sweep<1, 2>(plan, units, stream);
+	return one ? launch_ens_sweep<2, 1>(plan, units, stream) : launch_ens_sweep<2, 2>(plan, units, stream);
 }
 
 } // namespace bfvm

@@ -1065,6 +1065,8 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 		s->dir_fused = value != 0;
 	else if (n == "fused_gradient")
 		s->grad_fused = value != 0;
+	else if (n == "fused_gradient_evict_first")
+		s->grad_evict_first = value != 0;
 	else if (n == "wait_limit_cycles")
 	{
 		if (value < 10000 || value > 40000000000LL)

@@ -172,6 +172,7 @@ struct bfvm_solver
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
 	bool dir_fused = true;		 // staged sweeps of the LOD step write the overwrite that follows them
 	bool grad_fused = true;		 // the z sweep of a step computes the gradient (sweep_tma.cu)
+	bool grad_evict_first = true; // ... reading its tiles with an L2 evict-first policy
 	int* grad_tile_done = nullptr; // [z tiles] and [1 + z tiles] of the gradient inside the z sweep
 	int* grad_deferred = nullptr;
 	long long grad_tiles = 0;

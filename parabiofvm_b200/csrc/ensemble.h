@@ -52,6 +52,19 @@ enum ens_phase : int
 	ENS_PHASES = 6
 };
 
+// Launch choices of the ensemble kernels (batch_kernels.cu), picked by bfvm_batch_autotune:
+// per sweep axis, the register cap (CTAs of up to 512 threads resident per SM: 1 or 2) and how many
+// CTAs share a slot's run of tiles (1, 2 or 4: shorter runs balance better, longer runs restage
+// the coefficient tables less often); for the gradient, the planes per work unit and the planes
+// whose loads are issued together.
+struct ens_tuning
+{
+	int sweep_minb[3] = { 2, 2, 2 };
+	int sweep_split[3] = { 1, 1, 1 };
+	int grad_zc = 64;
+	int grad_zu = 8;
+};
+
 struct ensemble_plan
 {
 	int count = 0;					 // meshes in the ensemble
@@ -62,12 +75,16 @@ struct ensemble_plan
 	int maxS = 1;
 	size_t table_floats[3] = { 0, 0, 0 }; // largest staged table per axis
 	bool all3d = true;					  // every mesh is 3-D (the gradient kernel without the 1-D/2-D forms)
+	ens_tuning tune;					  // launch choices (the gradient units follow tune.grad_zc)
 };
 
 // Which meshes the ensemble kernels cover: every axis with n >= 2 and at most ENS_MAX_P blocks,
 // at most 32 substrates.
 bool ensemble_eligible(const bfvm_solver* s);
-int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes);
+// buffers: when given, the field and gradient buffers of each mesh instead of the solvers' own
+// (the autotuner times candidates on scratch copies)
+int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes, const ens_tuning& tune = ens_tuning(),
+				   const std::vector<std::pair<float*, float*>>* buffers = nullptr);
 void ensemble_free(ensemble_plan& plan);
 // One phase for every mesh of the plan, on `stream`.  `dirichlet_phase` k applies the overwrite to
 // meshes with k <= dims (before sweep k, or after the last sweep).

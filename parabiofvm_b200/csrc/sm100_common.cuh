@@ -55,6 +55,23 @@ __device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, 
 				 : "memory");
 }
 
+// An L2 policy that marks lines as the first to evict (for data read once).
+__device__ __forceinline__ uint64_t l2_evict_first_policy()
+{
+	uint64_t p;
+	asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+	return p;
+}
+
+__device__ __forceinline__ void tma_load_2d_hint(float* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar,
+												 uint64_t policy)
+{
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, "
+				 "{%2, %3}], [%4], %5;" ::"r"(smem_addr(dst)),
+				 "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_addr(bar)), "l"(policy)
+				 : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar)
 {
 	asm volatile(

@@ -52,6 +52,9 @@ struct tma_tile
 	int stages; // pipeline depth of each group
 	// zero-filled virtual fronts of a stage: `front_count` runs of `front_floats`, `front_pitch` apart
 	int front_floats, front_count, front_pitch;
+	// z tiles read with an L2 evict-first policy, so that the planes the sweep writes (which the
+	// gradient inside it reads back) are the lines L2 keeps
+	int evict_first;
 };
 
 // Issue the copies of tile w into `dst`, completing on `bar` (one thread).  The line elements land
@@ -82,6 +85,8 @@ __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMa
 	{
 		if (tt.axis == 1)
 			tma_load_3d(base + b * tt.box_h * 32, map, c0, b * tt.box_h, (int)outer, bar);
+		else if (tt.evict_first)
+			tma_load_2d_hint(base + b * tt.box_h * 32, map, c0, b * tt.box_h, bar, l2_evict_first_policy());
 		else
 			tma_load_2d(base + b * tt.box_h * 32, map, c0, b * tt.box_h, bar);
 	}
@@ -778,7 +783,10 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	if (slab_solve)
 		return launch_tma_variant<false, false, 1>(st, a, map, tt, smem);
 	if (gf && a.vP > 1)
+	{
+		tt.evict_first = st->grad_evict_first ? 1 : 0;
 		return launch_tma_variant<false, false, 0, true>(st, a, map, tt, smem, gf);
+	}
 	handled = !gf; // a gradient was asked for and this shape cannot compute it: the caller sweeps
 	if (!handled)
 		return BFVM_OK;

@@ -104,3 +104,30 @@ def test_solver_alone_then_batched_then_alone():
         np.testing.assert_array_equal(g, e)
     for s in solvers + [ref]:
         s.close()
+
+
+def test_autotuned_batch_matches_each_solver_alone():
+    """bfvm_batch_autotune times the ensemble kernels' launch choices on scratch copies: it leaves
+    the instances' state as it was, and the batch stepped with the chosen launches still ends
+    exactly where each solver stepped alone ends."""
+    ws = _ensemble()
+    alone = []
+    for w in ws:
+        s = make_solver(w)
+        s.run_steps(11, 0)
+        alone.append(_state(s))
+        s.close()
+    solvers = [make_solver(w) for w in ws]
+    b = Batch(solvers)
+    b.run_steps(1, 0)
+    choices = b.autotune()
+    assert set(choices["sweep_ctas_per_sm"]) <= {1, 2} and set(choices["sweep_ctas_per_slot"]) <= {1, 2, 4}
+    assert choices["gradient_planes"] in (32, 64, 128) and choices["gradient_load_batch"] in (4, 8)
+    b.run_steps(10, 1)
+    b.synchronize()
+    for i, s in enumerate(solvers):
+        for g, a in zip(_state(s), alone[i]):
+            np.testing.assert_array_equal(g, a, err_msg=f"instance {i}")
+    b.close()
+    for s in solvers:
+        s.close()
