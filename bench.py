@@ -1062,10 +1062,12 @@ def run_ours(args):
         intern_out = pinned(A * w.S)
         pos_step = pinned(A * w.dims)
         pos_step[:] = np.asarray(a.positions, np.float32).reshape(-1)
-        # once: the state in and out (as the reference driver stores before its loop and loads after);
-        # every step: the agents' positions in and their internalized substrates out
+        # once: the state in and out, as the reference's device solver stores it before its loop and
+        # loads it after (densities and internalized substrates: src/solver/device/CUDA/
+        # device_context.cpp:99-116); every step: the agents' positions in and their internalized
+        # substrates out.  The gradients stay on the device; loading them too is timed after.
         h2d = field_in.nbytes + sum(v.nbytes for v in ag.values()) + args.steps * pos_step.nbytes
-        d2h = field_out.nbytes + grad_out.nbytes + args.steps * intern_out.nbytes
+        d2h = field_out.nbytes + args.steps * intern_out.nbytes
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -1081,19 +1083,30 @@ def run_ours(args):
             s.run_steps(1, k)
             s.load_internalized_async(intern_out)
         s.load_densities(field_out)
-        s.load_gradients(grad_out)
         s.synchronize()
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        # the gradients loaded as well (6.3 GB at plain-320), for comparison
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        s.load_gradients(grad_out)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        grad_ms = max_over_ranks(g0.elapsed_time(g1))
         e2e = {"value": whole_job_rate(world, VS, args.steps, e2e_ms), "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
                "ms_total": e2e_ms,
+               "with_gradients_loaded": {"value": whole_job_rate(world, VS, args.steps, e2e_ms + grad_ms),
+                                         "gradient_load_ms": grad_ms,
+                                         "d2h_bytes_per_step": (d2h + grad_out.nbytes) // args.steps},
                "what": "through the C ABI from pinned host memory: field and agents stored before the steps, "
                        "every step the agents' positions stored, the step run (bfvm_run_steps: diffusion, gradient, "
                        "secretion) and the internalized substrates loaded (the per-step copies asynchronous, "
-                       "overlapping the step's diffusion), field and gradients loaded after the steps"}
+                       "overlapping the step's diffusion), the field loaded after the steps (the reference device "
+                       "solver's store/load set); with_gradients_loaded adds loading the gradients"}
         del field_in, field_out, grad_out, intern_out, ag
 
     s.close()

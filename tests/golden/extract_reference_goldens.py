@@ -109,7 +109,9 @@ def extract(ref_root: str) -> dict:
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_reference_goldens.py <paraBioFVM source root>")
+    ref_root = sys.argv[1]
     data = extract(ref_root)
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_goldens.json")
     with open(out, "w") as f:
