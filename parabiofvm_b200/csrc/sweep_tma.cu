@@ -197,6 +197,30 @@ __device__ __forceinline__ void overwrite_tile(const dirichlet_tiles& d, float* 
 		data[__ldg(&d.sidx[e])] = __ldg(&d.sval[e]);
 }
 
+// The Dirichlet entries of x tile w written into its staged rows (the overwrite that precedes the
+// x sweep), by the gthr threads of a warp group after the tile's copies landed.  Element e of the
+// field is row e / XS, column e % XS; row rl of the tile sits at rl * row_pitch + front.
+__device__ __forceinline__ void overwrite_stage(const dirichlet_tiles& d, float* stage, const tma_tile& tt, long long w,
+												int gtid, int gthr)
+{
+	const long long row0 = w * tt.R;
+	const int q1 = __ldg(&d.qoff[w + 1]);
+	for (int e = __ldg(&d.qoff[w]) + gtid; e < q1; e += gthr)
+	{
+		const long long el = __ldg(&d.qidx[e]);
+		const long long row = el / tt.XS;
+		const int col = (int)(el - row * tt.XS);
+		*reinterpret_cast<float4*>(stage + (row - row0) * tt.row_pitch + tt.front + col) = __ldg(&d.qval[e]);
+	}
+	const int s1 = __ldg(&d.soff[w + 1]);
+	for (int e = __ldg(&d.soff[w]) + gtid; e < s1; e += gthr)
+	{
+		const long long el = __ldg(&d.sidx[e]);
+		const long long row = el / tt.XS;
+		stage[(row - row0) * tt.row_pitch + tt.front + (int)(el - row * tt.XS)] = __ldg(&d.sval[e]);
+	}
+}
+
 // ------------------------------------------------------------------------------------------------
 // the gradient inside the z sweep (grad_fuse in sweep_common.cuh)
 
@@ -427,6 +451,13 @@ __global__ void __launch_bounds__(640, 1)
 			sstride = ROWS ? tl.sstride : 32;
 		}
 		const bool ok = mbar_wait(&bars[st], parity, a.wait_limit);
+		if (ROWS && a.dir_in.items > 0)
+		{
+			// the overwrite that precedes the sweep, into the staged rows, before any thread reads them
+			if (ok)
+				overwrite_stage(a.dir_in, stages + (size_t)st * tt.stage_floats, tt, w, lane + 32 * j, gthr);
+			group_sync(bar_id, gthr);
+		}
 
 		const float cs = ctab[s];
 		const float* bcol = btab + s * NP + p; // b' of this block: bcol[k]
