@@ -681,6 +681,30 @@ def measure_surrogate(train_steps=10, warmup=3, fallback_macro_steps=100, fresh_
     run_net.synchronize()
     ms_macro = e0.elapsed_time(e1) / 10
 
+    # the trained network rolled out alone for 8 macro-steps from a field and agents of its training
+    # distribution (uniform agents), against plain stepping: its relative L2 error after each
+    rollout = []
+    with torch.cuda.stream(net.stream):
+        g_field, g_src, g_sink = [torch.empty((1, VS), device="cuda") for _ in range(3)]
+    su.random_field(env.grid, env.S, np.random.default_rng(19), g_field[0], net.stream)
+    ua = su.random_agents(env, np.random.default_rng(17), 55_000)
+    s = env.solver()
+    s.set_stream(net.stream.cuda_stream)
+    s.store_agents(ua["sec"], ua["sat"], ua["upt"], ua["nex"], np.zeros_like(ua["sec"]), None, ua["vol"], ua["pos"])
+    dev_ua = {k: torch.from_numpy(np.ascontiguousarray(v, np.float32)).cuda() for k, v in ua.items()}
+    su.agent_rates((0, 0, 0), (env.dx,) * 3, env.grid, env.time_step, dev_ua, g_src[0], g_sink[0], net.stream)
+    s.store_densities_device(g_field[0])
+    sur_field = g_field[0].clone()
+    plain_now = torch.empty_like(sur_field)
+    for m in range(8):
+        run_net.infer(sur_field, g_src[0], g_sink[0], out1)
+        sur_field.copy_(out1)
+        s.run_steps(16, 16 * m)
+        s.load_densities_device(plain_now)
+        s.synchronize()
+        rollout.append(su.rel_l2(sur_field, plain_now))
+    s.close()
+
     # the controller over 1,600 steps, from a field of the training distribution
     run_field = f1.clone()
     report = su.run_with_fallback(run_net, env, run_field, agents, macro_steps=fallback_macro_steps, check_every=8,
@@ -710,6 +734,7 @@ def measure_surrogate(train_steps=10, warmup=3, fallback_macro_steps=100, fresh_
                          "seconds": report.seconds, "plain_seconds": plain_s,
                          "speedup_vs_plain": plain_s / report.seconds,
                          "rel_l2_vs_plain": su.rel_l2(run_field, plain_field)},
+        "rollout_rel_l2_uniform_agents": rollout,
     }
 
 
@@ -735,6 +760,7 @@ def run_surrogate(args):
                      "peak": r["peak"], "unit": "TFLOP/s", "frac": r["conv_tflops"] / r["peak"],
                      "peak_kind": r["peak_kind"], "traffic": None, "ms": r["ms_conv"]},
         "fallback_run": r["fallback_run"],
+        "rollout_rel_l2_uniform_agents": r["rollout_rel_l2_uniform_agents"],
         "gpu_launches": None,
     }
     print(json.dumps(line), flush=True)
@@ -1187,7 +1213,8 @@ def side_forms():
         "train_step_ms_batch4": r["ms_train"], "network": r["trained"],
         "controller": {"macro_steps": fb["macro_steps"], "surrogate_macro_steps": fb["surrogate_macro_steps"],
                        "checked_rel_l2": fb["checks"], "fell_back_at": fb["fell_back_at"],
-                       "speedup_vs_plain": fb["speedup_vs_plain"], "rel_l2_vs_plain": fb["rel_l2_vs_plain"]}}
+                       "speedup_vs_plain": fb["speedup_vs_plain"], "rel_l2_vs_plain": fb["rel_l2_vs_plain"]},
+        "rollout_rel_l2_uniform_agents": r["rollout_rel_l2_uniform_agents"]}
     return out
 
 

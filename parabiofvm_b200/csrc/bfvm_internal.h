@@ -77,10 +77,10 @@ struct dirichlet_tiles
 {
 	long long items = 0; // tiles of the sweep; 0 when the axis has no grouped list
 	int* qoff = nullptr;
-	long long* qidx = nullptr;
+	int* qidx = nullptr; // element indices (the lists exist for fields of fewer than 2^31 elements)
 	float4* qval = nullptr;
 	int* soff = nullptr;
-	long long* sidx = nullptr;
+	int* sidx = nullptr;
 	float* sval = nullptr;
 };
 

@@ -117,7 +117,7 @@ static int build_tile_lists(bfvm_solver* s, const std::vector<long long>& qidx, 
 	for (int axis = 0; axis < s->dims; axis++)
 	{
 		const staged_tiling tl = staged_tiles(s, axis);
-		if (tl.items == 0 || tl.items > INT32_MAX || qidx.size() + sidx.size() > (size_t)INT32_MAX)
+		if (tl.items == 0 || tl.items > INT32_MAX || s->V * s->S > INT32_MAX)
 			continue;
 		dirichlet_tiles& t = s->dir_tiles[axis];
 		std::vector<int> qoff(tl.items + 1, 0), soff(tl.items + 1, 0);
@@ -130,7 +130,7 @@ static int build_tile_lists(bfvm_solver* s, const std::vector<long long>& qidx, 
 			qoff[w + 1] += qoff[w];
 			soff[w + 1] += soff[w];
 		}
-		std::vector<long long> qi(qidx.size()), si(sidx.size());
+		std::vector<int> qi(qidx.size()), si(sidx.size());
 		std::vector<float4> qv(qval.size());
 		std::vector<float> sv(sval.size());
 		{
@@ -138,14 +138,14 @@ static int build_tile_lists(bfvm_solver* s, const std::vector<long long>& qidx, 
 			for (size_t k = 0; k < qidx.size(); k++)
 			{
 				const int p = at[tl.tile(qidx[k])]++;
-				qi[p] = qidx[k];
+				qi[p] = (int)qidx[k];
 				qv[p] = qval[k];
 			}
 			std::vector<int> as(soff.begin(), soff.end() - 1);
 			for (size_t k = 0; k < sidx.size(); k++)
 			{
 				const int p = as[tl.tile(sidx[k])]++;
-				si[p] = sidx[k];
+				si[p] = (int)sidx[k];
 				sv[p] = sval[k];
 			}
 		}
@@ -161,12 +161,12 @@ static int build_tile_lists(bfvm_solver* s, const std::vector<long long>& qidx, 
 		BFVM_CUDA(cudaMemcpy(t.soff, soff.data(), soff.size() * sizeof(int), cudaMemcpyHostToDevice));
 		if (!qi.empty())
 		{
-			BFVM_CUDA(cudaMemcpy(t.qidx, qi.data(), qi.size() * sizeof(long long), cudaMemcpyHostToDevice));
+			BFVM_CUDA(cudaMemcpy(t.qidx, qi.data(), qi.size() * sizeof(int), cudaMemcpyHostToDevice));
 			BFVM_CUDA(cudaMemcpy(t.qval, qv.data(), qv.size() * sizeof(float4), cudaMemcpyHostToDevice));
 		}
 		if (!si.empty())
 		{
-			BFVM_CUDA(cudaMemcpy(t.sidx, si.data(), si.size() * sizeof(long long), cudaMemcpyHostToDevice));
+			BFVM_CUDA(cudaMemcpy(t.sidx, si.data(), si.size() * sizeof(int), cudaMemcpyHostToDevice));
 			BFVM_CUDA(cudaMemcpy(t.sval, sv.data(), sv.size() * sizeof(float), cudaMemcpyHostToDevice));
 		}
 		t.items = tl.items;

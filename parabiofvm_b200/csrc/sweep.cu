@@ -209,7 +209,6 @@ static sweep_args make_args(bfvm_solver* st, int axis)
 	a.wait_limit = st->wait_limit_cycles;
 	a.drop_tile_copy = st->drop_tile_copy;
 	a.dir = dirichlet_tiles();
-	a.dir_in = dirichlet_tiles();
 	return a;
 }
 
@@ -258,9 +257,6 @@ static int sweep_axis(bfvm_solver* st, int axis, const sweep_args& a, bool& stag
 	if (!rc && !handled && gf)
 		return sweep_axis(st, axis, a, staged); // the shape cannot take the gradient: sweep alone
 	staged = handled;
-	// the overwrite meant to go into the staged tiles runs as the scatter before another kernel
-	if (!rc && !handled && a.dir_in.items > 0)
-		rc = launch_dirichlet(st);
 	// the same front-padded block algebra without TMA staging, where the lines fit 16 blocks
 	if (!rc && !handled && st->self_plan && pl.vtab && pl.vP <= ENS_MAX_P && (axis > 0 || st->S <= 32))
 	{
@@ -296,16 +292,14 @@ int launch_diffusion(bfvm_solver* st, bool gradient, bool* gradient_done)
 {
 	if (gradient_done)
 		*gradient_done = false;
-	// the first overwrite goes into the staged tiles of the x sweep when its list exists
-	const bool first_in_sweep = st->dir_fused && st->dir_tiles[0].items > 0;
-	int rc = first_in_sweep ? BFVM_OK : launch_dirichlet(st);
+	// the first overwrite stays a scatter: inside the x sweep it would have to reach the staged
+	// tile before any thread reads it, with the entries' load latency on every tile's path
+	int rc = launch_dirichlet(st);
 	for (int axis = 0; axis < st->dims && !rc; axis++)
 	{
 		sweep_args a = make_args(st, axis);
 		if (st->dir_fused)
 			a.dir = st->dir_tiles[axis];
-		if (axis == 0 && first_in_sweep)
-			a.dir_in = st->dir_tiles[0];
 		// the gradient inside the z sweep needs the final field there: no overwrite after it, or
 		// the overwrite written by the sweep itself
 		const bool overwrite_after = st->dir_qcount + st->dir_count > 0;

@@ -33,9 +33,6 @@ struct sweep_args
 	// staged sweeps of the LOD step: the Dirichlet overwrite that follows this sweep, grouped by its
 	// tiles; each tile's entries are written right after the tile (items 0: no overwrite here)
 	dirichlet_tiles dir;
-	// the staged x sweep: the overwrite that precedes it, written into each staged tile before the
-	// tile is solved (items 0: none)
-	dirichlet_tiles dir_in;
 };
 
 __device__ __forceinline__ void block_range(int j, int base_len, int extra, int& p, int& L)

@@ -197,29 +197,45 @@ __device__ __forceinline__ void overwrite_tile(const dirichlet_tiles& d, float* 
 		data[__ldg(&d.sidx[e])] = __ldg(&d.sval[e]);
 }
 
-// The Dirichlet entries of x tile w written into its staged rows (the overwrite that precedes the
-// x sweep), by the gthr threads of a warp group after the tile's copies landed.  Element e of the
-// field is row e / XS, column e % XS; row rl of the tile sits at rl * row_pitch + front.
-__device__ __forceinline__ void overwrite_stage(const dirichlet_tiles& d, float* stage, const tma_tile& tt, long long w,
-												int gtid, int gthr)
+// One thread's share of a tile's Dirichlet entries held in registers: the run of four and the
+// single element at position gtid of the tile's lists.  The sweep loads them a tile ahead of their
+// use, so their latency hides behind the next tile's solve.
+struct dir_regs
 {
-	const long long row0 = w * tt.R;
-	const int q1 = __ldg(&d.qoff[w + 1]);
-	for (int e = __ldg(&d.qoff[w]) + gtid; e < q1; e += gthr)
+	int qi = -1, si = -1; // -1: no entry for this thread
+	float4 qv;
+	float sv = 0.f;
+
+	__device__ __forceinline__ void load(const dirichlet_tiles& d, const int (&o)[4], int gtid)
 	{
-		const long long el = __ldg(&d.qidx[e]);
-		const long long row = el / tt.XS;
-		const int col = (int)(el - row * tt.XS);
-		*reinterpret_cast<float4*>(stage + (row - row0) * tt.row_pitch + tt.front + col) = __ldg(&d.qval[e]);
+		qi = -1;
+		si = -1;
+		if (o[0] + gtid < o[1])
+		{
+			qi = __ldg(&d.qidx[o[0] + gtid]);
+			qv = __ldg(&d.qval[o[0] + gtid]);
+		}
+		if (o[2] + gtid < o[3])
+		{
+			si = __ldg(&d.sidx[o[2] + gtid]);
+			sv = __ldg(&d.sval[o[2] + gtid]);
+		}
 	}
-	const int s1 = __ldg(&d.soff[w + 1]);
-	for (int e = __ldg(&d.soff[w]) + gtid; e < s1; e += gthr)
+
+	// these entries, then (rarely) those past one per thread of the group, straight from the lists
+	__device__ __forceinline__ void store(const dirichlet_tiles& d, const int (&o)[4], float* data, int gtid,
+										  int gthr) const
 	{
-		const long long el = __ldg(&d.sidx[e]);
-		const long long row = el / tt.XS;
-		stage[(row - row0) * tt.row_pitch + tt.front + (int)(el - row * tt.XS)] = __ldg(&d.sval[e]);
+		if (qi >= 0)
+			*reinterpret_cast<float4*>(data + qi) = qv;
+		if (si >= 0)
+			data[si] = sv;
+		for (int e = o[0] + gthr + gtid; e < o[1]; e += gthr)
+			*reinterpret_cast<float4*>(data + __ldg(&d.qidx[e])) = __ldg(&d.qval[e]);
+		for (int e = o[2] + gthr + gtid; e < o[3]; e += gthr)
+			data[__ldg(&d.sidx[e])] = __ldg(&d.sval[e]);
 	}
-}
+};
 
 // ------------------------------------------------------------------------------------------------
 // the gradient inside the z sweep (grad_fuse in sweep_common.cuh)
@@ -436,10 +452,24 @@ __global__ void __launch_bounds__(640, 1)
 	bool failed = false;
 	int it = 0;
 	long long w = w0;
+	// the Dirichlet entries of the previous tile (written after the first barrier of this one):
+	// their list offsets, loaded an iteration before the entries, and the entries themselves
+	int dir_prev[4] = { 0, 0, 0, 0 };
+	dir_regs dir_hold;
 	for (; w < tt.items; w += wstride, it++)
 	{
 		const int st = it % NST;
 		const uint32_t parity = (uint32_t)((it / NST) & 1);
+		int dir_cur[4] = { 0, 0, 0, 0 };
+		if (a.dir.items > 0)
+		{
+			if (it > 0)
+				dir_hold.load(a.dir, dir_prev, lane + 32 * j);
+			dir_cur[0] = __ldg(&a.dir.qoff[w]);
+			dir_cur[1] = __ldg(&a.dir.qoff[w + 1]);
+			dir_cur[2] = __ldg(&a.dir.soff[w]);
+			dir_cur[3] = __ldg(&a.dir.soff[w + 1]);
+		}
 
 		const float* cur = stages + (size_t)st * tt.stage_floats;
 		int s, sbase, sstride;
@@ -451,13 +481,6 @@ __global__ void __launch_bounds__(640, 1)
 			sstride = ROWS ? tl.sstride : 32;
 		}
 		const bool ok = mbar_wait(&bars[st], parity, a.wait_limit);
-		if (ROWS && a.dir_in.items > 0)
-		{
-			// the overwrite that precedes the sweep, into the staged rows, before any thread reads them
-			if (ok)
-				overwrite_stage(a.dir_in, stages + (size_t)st * tt.stage_floats, tt, w, lane + 32 * j, gthr);
-			group_sync(bar_id, gthr);
-		}
 
 		const float cs = ctab[s];
 		const float* bcol = btab + s * NP + p; // b' of this block: bcol[k]
@@ -492,7 +515,7 @@ __global__ void __launch_bounds__(640, 1)
 			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st]);
 		// the barrier also ordered the previous tile's stores: its Dirichlet entries go on top
 		if (a.dir.items > 0 && it > 0)
-			overwrite_tile(a.dir, a.data, w - wstride, lane + 32 * j, gthr);
+			dir_hold.store(a.dir, dir_prev, a.data, lane + 32 * j, gthr);
 
 		if (SLAB != 0)
 		{
@@ -590,6 +613,9 @@ __global__ void __launch_bounds__(640, 1)
 		}
 		if (GRAD && w >= gf.lag)
 			gradient_work(gf, a.data, w - gf.lag, lane, j, P, bar_id);
+#pragma unroll
+		for (int k = 0; k < 4; k++)
+			dir_prev[k] = dir_cur[k];
 	}
 
 	if (!failed && a.dir.items > 0 && it > 0)

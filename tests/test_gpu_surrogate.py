@@ -189,33 +189,47 @@ def _env():
     return Microenvironment((128, 16, 16), 20, [2000.0, 20000.0], [0.1, 0.5], 0.01)
 
 
-def test_training_beats_the_method_without_the_network():
-    """Trained on pairs from the plain solver, the network predicts the field 16 steps ahead better
-    than the field itself does (what a macro-step would be without the network), on pairs it has
-    not seen."""
-    import torch
-
-    from parabiofvm_b200.surrogate import PairGenerator, Surrogate, rel_l2, train
+def test_training_reduces_the_loss():
+    """Adam steps of the project's own kernels on fresh pairs from the plain solver lower the loss
+    (a small mesh, so the test stays short; the full training is parabiofvm_b200.surrogate_train)."""
+    from parabiofvm_b200.surrogate import PairGenerator, Surrogate, train
 
     env = _env()
     net = Surrogate(env.grid, env.S, max_batch=2, seed=1)
     gen = PairGenerator(env, seed=2, agents=(500, 3000))
     losses = train(net, gen, steps=300, batch=2, learning_rate=2e-3)
     assert np.mean(losses[-10:]) < 0.5 * np.mean(losses[:3]), losses[:3] + losses[-10:]
-    held = PairGenerator(env, seed=99, agents=(500, 3000))
-    shape = (1, env.voxels * env.S)
-    field, src, sink, target, pred = [torch.empty(shape, device="cuda") for _ in range(5)]
-    errs_net, errs_none = [], []
-    for _ in range(4):
-        held.batch(field, src, sink, target)
-        net.stream.wait_stream(held.stream)
-        net.infer(field, src, sink, pred)
-        net.synchronize()
-        errs_net.append(rel_l2(pred, target))
-        errs_none.append(rel_l2(field, target))
-    assert np.mean(errs_net) < 0.6 * np.mean(errs_none), (errs_net, errs_none)
     gen.close()
-    held.close()
+    net.close()
+
+
+# the trained network's error on pairs outside its training set, as the training run measured it
+# (parabiofvm_b200/data/surrogate_128x4.npz: 2,000 pairs, batch 4, Adam lr 1e-3, best of 11 epochs)
+TRAINED_HELD_OUT_REL_L2 = 0.0077
+
+
+def test_trained_network_on_unseen_pairs():
+    """The committed network (trained on 2,000 pairs of the standard 128^3 x 4 microenvironment)
+    predicts the field 16 plain steps ahead on pairs it has never seen with the relative L2 error
+    its training reached, about 13x below the macro-step without a network (the field itself).
+    The 1e-3 at which the controller lets it keep control is not reached: the error plateaued near
+    8e-3 over the training epochs."""
+    import torch
+
+    from parabiofvm_b200 import surrogate as su
+
+    env = su.standard_environment()
+    net = su.Surrogate(env.grid, env.S, max_batch=1, seed=0)
+    rec = su.load_trained(net, env)
+    assert rec["held_out_rel_l2"] < 0.01
+    # pairs of the training data set's generator far beyond its 2,000 training pairs
+    gen = su.PairGenerator(env, seed=rec["recipe"]["data_seed"])
+    err_net, err_none = su.evaluate(net, gen, range(10_000, 10_006))
+    print(f"unseen pairs: rel-L2 {err_net:.4e} with the network, {err_none:.4e} without")
+    assert err_net < 1.5 * TRAINED_HELD_OUT_REL_L2, err_net
+    assert err_net < 0.15 * err_none, (err_net, err_none)
+    torch.cuda.synchronize()
+    gen.close()
     net.close()
 
 
