@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "agent_kernels.cuh"
+#include "sweep_common.cuh"
 
 namespace bfvm {
 
@@ -343,6 +344,80 @@ __global__ void release_kernel(int index, int S, int dims, const float* __restri
 	intern[k] = 0.f;
 }
 
+// The sorted update four substrates at a time (S % 4 == 0): one thread owns a (segment, four
+// substrates) pair and moves every row as 16-byte accesses.  Its threads stride over the segments
+// the binning found (counts[0], read on the device), so no thread is launched for agents that
+// share a voxel.  The arithmetic is secrete_element's, per substrate, in the same order.
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+__device__ __forceinline__ float fused_term(float D, float rn, float rd, float rf)
+{
+	return __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(__fsub_rn(1.f, rd), D), rn), rd), rf);
+}
+
+__device__ __forceinline__ float agent_term(float D, float num, float den, float fac)
+{
+	return __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(-den, D), num), __fadd_rn(1.f, den)), fac);
+}
+
+__global__ void __launch_bounds__(256) secrete_sorted4_kernel(int S, float* __restrict__ dens,
+															  const int* __restrict__ counts,
+															  const int* __restrict__ seg_start,
+															  const unsigned int* __restrict__ keys,
+															  const float* __restrict__ snum, const float* __restrict__ sden,
+															  const float* __restrict__ sfac,
+															  const float* __restrict__ red_num,
+															  const float* __restrict__ red_den,
+															  const float* __restrict__ red_fac,
+															  float* __restrict__ sintern, float voxel_volume)
+{
+	const int S4 = S >> 2;
+	const long long n = (long long)counts[0] * S4;
+	const bool conflict = counts[2] != 0;
+	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+	{
+		const int seg = (int)(t / S4);
+		const int s0 = (int)(t - (long long)seg * S4) * 4;
+		const int b = seg_start[seg];
+		const size_t dv = (size_t)keys[b] * S + s0;
+		const size_t r = (size_t)seg * S + s0;
+		const float4 D = ld4(dens + dv);
+		const float4 rn = ld4(red_num + r), rd = ld4(red_den + r), rf = ld4(red_fac + r);
+		if (!conflict)
+		{
+			// compute_fused: the voxel holds this one agent
+			float* ip = sintern + (size_t)b * S + s0;
+			float4 I = ld4(ip);
+			I.x = __fsub_rn(I.x, __fmul_rn(voxel_volume, fused_term(D.x, rn.x, rd.x, rf.x)));
+			I.y = __fsub_rn(I.y, __fmul_rn(voxel_volume, fused_term(D.y, rn.y, rd.y, rf.y)));
+			I.z = __fsub_rn(I.z, __fmul_rn(voxel_volume, fused_term(D.z, rn.z, rd.z, rf.z)));
+			I.w = __fsub_rn(I.w, __fmul_rn(voxel_volume, fused_term(D.w, rn.w, rd.w, rf.w)));
+			st4(ip, I);
+		}
+		else
+		{
+			// compute_internalized for every agent of the voxel, with its own intermediates
+			const int e = seg_start[seg + 1];
+			for (int p = b; p < e; p++)
+			{
+				const size_t k = (size_t)p * S + s0;
+				const float4 nu = ld4(snum + k), de = ld4(sden + k), fa = ld4(sfac + k);
+				float4 I = ld4(sintern + k);
+				I.x = __fsub_rn(I.x, __fmul_rn(voxel_volume, agent_term(D.x, nu.x, de.x, fa.x)));
+				I.y = __fsub_rn(I.y, __fmul_rn(voxel_volume, agent_term(D.y, nu.y, de.y, fa.y)));
+				I.z = __fsub_rn(I.z, __fmul_rn(voxel_volume, agent_term(D.z, nu.z, de.z, fa.z)));
+				I.w = __fsub_rn(I.w, __fmul_rn(voxel_volume, agent_term(D.w, nu.w, de.w, fa.w)));
+				st4(sintern + k, I);
+			}
+		}
+		st4(dens + dv, make_float4(__fadd_rn(__fdiv_rn(__fadd_rn(D.x, rn.x), rd.x), rf.x),
+								   __fadd_rn(__fdiv_rn(__fadd_rn(D.y, rn.y), rd.y), rf.y),
+								   __fadd_rn(__fdiv_rn(__fadd_rn(D.z, rn.z), rd.z), rf.z),
+								   __fadd_rn(__fdiv_rn(__fadd_rn(D.w, rn.w), rd.w), rf.w)));
+	}
+}
+
 // The same release with the internalized amounts in sorted order: agent `index` is at row rank[index].
 __global__ void release_sorted_kernel(int index, int S, int dims, const float* __restrict__ pos, int3 bmin, int3 vox,
 									  int3 grid, float* __restrict__ dens, float* __restrict__ sintern,
@@ -578,6 +653,17 @@ int launch_secretion(bfvm_solver* s, bool recompute)
 	}
 	const long long AS = (long long)a.count * s->S;
 	const float vv = (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]);
+	if (a.sorted && s->S % 4 == 0)
+	{
+		// up to the threads of every segment (at most one per agent), resident at once
+		const long long threads = AS / 4;
+		const unsigned grid = (unsigned)std::max<long long>(
+			1, std::min<long long>((threads + 255) / 256, (long long)sm_count_impl(s->device) * 8));
+		secrete_sorted4_kernel<<<grid, 256, 0, s->stream>>>(s->S, s->dens, a.seg_count_dev, a.seg_start, a.keys,
+															 a.snum, a.sden, a.sfac, a.red_num, a.red_den, a.red_fac,
+															 a.sintern, vv);
+		return check_launch(s, "secrete_sorted4_kernel");
+	}
 	if (a.sorted)
 	{
 		secrete_sorted_kernel<<<(unsigned)((AS + 255) / 256), 256, 0, s->stream>>>(
