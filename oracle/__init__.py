@@ -52,6 +52,8 @@ def _load():
             "get_densities": (None, [vp, tp]),
             "get_gradients": (None, [vp, tp]),
             "set_agents": (None, [vp, ctypes.c_int, tp, tp, tp, tp, tp, tp, tp, tp]),
+            "add_agents": (None, [vp, ctypes.c_int, tp, tp, tp, tp, tp, tp, tp, tp]),
+            "remove_agent": (None, [vp, ctypes.c_int]),
             "get_internalized": (None, [vp, tp]),
             "diffusion": (None, [vp]),
             "dirichlet": (None, [vp]),
@@ -174,6 +176,22 @@ class Oracle:
         self._keep = arrs
         self.agents_count = n
         self._fn("set_agents")(self._h, n, *[_ptr(a, self._ct) for a in arrs])
+
+    def add_agents(self, count, secretion_rates=None, saturation_densities=None, uptake_rates=None,
+                   net_export_rates=None, internalized=None, fraction_released=None, volumes=None, positions=None):
+        """agent_data::add `count` times (src/agent_data.cpp:10-25), the new rows set to these values;
+        an array left None stays 0."""
+        count = int(count)
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=self.dtype).reshape(-1) for a in
+                (secretion_rates, saturation_densities, uptake_rates, net_export_rates, internalized,
+                 fraction_released, volumes, positions)]
+        self._fn("add_agents")(self._h, count, *[None if a is None else _ptr(a, self._ct) for a in arrs])
+        self.agents_count += count
+
+    def remove_agent(self, index):
+        """agent_data::remove (src/agent_data.cpp:27-53): the last agent moves into the freed slot."""
+        self._fn("remove_agent")(self._h, int(index))
+        self.agents_count -= 1
 
     def internalized(self):
         out = np.empty(self.agents_count * self.S, dtype=self.dtype)

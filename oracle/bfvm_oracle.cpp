@@ -650,6 +650,52 @@ void set_agents(oracle_state<real_t>& m, int count, const real_t* sec, const rea
 	m.positions.assign(pos, pos + (std::size_t)count * m.dims);
 }
 
+// agent_data::add (src/agent_data.cpp:10-25) `count` times: every per-agent array grows by one row,
+// value-initialised (0), and the caller's values then fill the new rows (the reference sets them
+// through the agent afterwards); a null array leaves its rows at 0.
+template <typename real_t>
+void add_agents(oracle_state<real_t>& m, int count, const real_t* sec, const real_t* sat, const real_t* upt,
+				const real_t* nex, const real_t* intern, const real_t* frac, const real_t* vol, const real_t* pos)
+{
+	const std::size_t S = (std::size_t)m.S, D = (std::size_t)m.dims, old = (std::size_t)m.A;
+	auto grow = [&](std::vector<real_t>& v, std::size_t row, const real_t* src) {
+		v.resize((old + count) * row, 0);
+		if (src)
+			std::copy(src, src + (std::size_t)count * row, v.begin() + old * row);
+	};
+	grow(m.secretion, S, sec);
+	grow(m.saturation, S, sat);
+	grow(m.uptake, S, upt);
+	grow(m.net_export, S, nex);
+	grow(m.intern, S, intern);
+	grow(m.frac_released, S, frac);
+	grow(m.volumes, 1, vol);
+	grow(m.positions, D, pos);
+	m.A += count;
+}
+
+// agent_data::remove (src/agent_data.cpp:27-53): the last agent's rows move into the freed slot.
+template <typename real_t>
+void remove_agent(oracle_state<real_t>& m, int index)
+{
+	m.A--;
+	auto shrink = [&](std::vector<real_t>& v, std::size_t row) {
+		if ((std::size_t)index != (std::size_t)m.A)
+			std::copy(v.begin() + (std::size_t)m.A * row, v.begin() + ((std::size_t)m.A + 1) * row,
+					  v.begin() + (std::size_t)index * row);
+		v.resize((std::size_t)m.A * row);
+	};
+	const std::size_t S = (std::size_t)m.S;
+	shrink(m.secretion, S);
+	shrink(m.saturation, S);
+	shrink(m.uptake, S);
+	shrink(m.net_export, S);
+	shrink(m.intern, S);
+	shrink(m.frac_released, S);
+	shrink(m.volumes, 1);
+	shrink(m.positions, (std::size_t)m.dims);
+}
+
 // Bulk supply and uptake (src/solver/host/bulk_solver.cpp:20-33, solve_single), for every voxel:
 //   D = (D + dt * S * T) / (1 + dt * (U + S))
 // with the rates the reference's three callbacks return for the voxel, given here as tables:
@@ -763,6 +809,16 @@ void run_steps(oracle_state<real_t>& m, int steps, int first_step)
 												  const T* pos)                                                        \
 	{                                                                                                                  \
 		set_agents(*static_cast<oracle_state<T>*>(h), count, sec, sat, upt, nex, intern, frac, vol, pos);              \
+	}                                                                                                                  \
+	extern "C" void oracle_##SUFFIX##_add_agents(void* h, int count, const T* sec, const T* sat, const T* upt,         \
+												  const T* nex, const T* intern, const T* frac, const T* vol,          \
+												  const T* pos)                                                        \
+	{                                                                                                                  \
+		add_agents(*static_cast<oracle_state<T>*>(h), count, sec, sat, upt, nex, intern, frac, vol, pos);              \
+	}                                                                                                                  \
+	extern "C" void oracle_##SUFFIX##_remove_agent(void* h, int index)                                                 \
+	{                                                                                                                  \
+		remove_agent(*static_cast<oracle_state<T>*>(h), index);                                                        \
 	}                                                                                                                  \
 	extern "C" void oracle_##SUFFIX##_get_internalized(void* h, T* dst)                                               \
 	{                                                                                                                  \

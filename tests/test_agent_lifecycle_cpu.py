@@ -84,3 +84,26 @@ def test_any_removal_sequence_matches_sequential_removal():
         _check(*case)
 
     check()
+
+
+def test_oracle_add_and_remove_follow_agent_data():
+    """The oracle's agent_data::add/remove (src/agent_data.cpp:10-53): new rows appended with the given
+    values (0 where none is given), and a removal moves the then-last agent into the freed slot."""
+    import oracle
+    from scenarios import make_oracle, synthetic
+
+    oracle.build()
+    w = synthetic(12, 2, 30, seed=5, clustered=True, sigma=40.0)
+    o = make_oracle(w, np.float32)
+    intern = np.asarray(w.agents.internalized, np.float32).reshape(30, 2).copy()
+    new_int = np.arange(8, dtype=np.float32).reshape(4, 2) + 1
+    o.add_agents(4, internalized=new_int, volumes=np.full(4, 1000.0), positions=np.full((4, 3), 10.0))
+    rows = np.concatenate([intern, new_int])
+    np.testing.assert_array_equal(o.internalized().reshape(-1, 2), rows)
+    ids = list(range(34))
+    for i in (3, 33 - 1, 0):
+        o.remove_agent(i)
+        ids[i] = ids[-1]
+        ids.pop()
+    np.testing.assert_array_equal(o.internalized().reshape(-1, 2), rows[ids])
+    o.close()

@@ -181,3 +181,37 @@ def test_store_with_same_count_keeps_binning_and_takes_new_amounts():
     np.testing.assert_array_equal(s.load_internalized(), fresh.load_internalized())
     s.close()
     fresh.close()
+
+
+@pytest.mark.gpu
+def test_population_that_gains_and_loses_agents_against_the_oracle():
+    """A stepped population that gains and loses agents, on the GPU (bfvm_add_agents,
+    bfvm_remove_agents) and in the FP32 oracle (agent_data::add/remove restated,
+    src/agent_data.cpp:10-53), between recompute steps.  Lines of one register block keep the GPU
+    bit-identical to the oracle."""
+    from scenarios import make_oracle
+
+    w = synthetic(32, 3, 1500, seed=41, clustered=True, sigma=60.0, interior_fraction=0.02)
+    g = make_solver(w)
+    o = make_oracle(w, np.float32)
+    rng = np.random.default_rng(42)
+    first = 0
+    for change in range(3):
+        g.run_steps(10, first)
+        o.run_steps(10, first)
+        first += 10
+        new = _new_rows(rng, 200 + 50 * change, w.S, 32 * 20)
+        args = [new[k] for k in KEYS]
+        g.add_agents(len(new["vol"]), *args)
+        o.add_agents(len(new["vol"]), *args)
+        idx = _removals(rng, g.agents_count, 150)
+        g.remove_agents(idx)
+        for i in idx:
+            o.remove_agent(i)
+    g.run_steps(10, first)
+    o.run_steps(10, first)
+    np.testing.assert_array_equal(g.load_densities(), o.densities())
+    np.testing.assert_array_equal(g.load_gradients(), o.gradients())
+    np.testing.assert_array_equal(g.load_internalized(), o.internalized())
+    g.close()
+    o.close()
