@@ -988,6 +988,8 @@ int bfvm_run_steps(bfvm_solver* s, int32_t steps, int32_t first_step)
 	int oc;
 	if (s->ag.count > 0 && (oc = ensure_copy_stream(s)))
 		return oc;
+	if (s->grad_fused && (oc = grad_fuse_buffers(s)))
+		return oc;
 	for (int i = 0; i < steps; i++)
 	{
 		const int rc = ((first_step + i) % 10 == 0) ? 1 : 0;

@@ -246,6 +246,7 @@ int launch_sweep(bfvm_solver* s, int axis, bool final_dirichlet);
 // the LOD step, overwrites fused into the staged sweeps; with `gradient`, the z sweep also
 // computes the gradient where it can, and *gradient_done tells whether it did
 int launch_diffusion(bfvm_solver* s, bool gradient = false, bool* gradient_done = nullptr);
+int grad_fuse_buffers(bfvm_solver* s); // buffers of the gradient inside the z sweep (outside a capture)
 // the staged sweep of one axis alone, with launch shape `tune` (groups 0: built-in choice);
 // `handled` is false when the staged path does not take the shape
 int launch_staged_sweep(bfvm_solver* s, int axis, const sweep_tuning& tune, bool& handled);

@@ -284,6 +284,30 @@ int launch_sweep(bfvm_solver* st, int axis, bool final_dirichlet)
 	return rc;
 }
 
+// The tile flags and deferred-tile list of the gradient inside the z sweep, allocated outside any
+// stream capture (bfvm_run_steps calls this before it captures a step); inside a capture nothing
+// is allocated.
+int grad_fuse_buffers(bfvm_solver* st)
+{
+	if (st->dims != 3)
+		return BFVM_OK;
+	const long long items = ((long long)st->grid[1] * st->grid[0] * st->S + 31) / 32; // z tiles
+	if (st->grad_tiles >= items)
+		return BFVM_OK;
+	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+	BFVM_CUDA(cudaStreamIsCapturing(st->stream, &cs));
+	if (cs != cudaStreamCaptureStatusNone)
+		return BFVM_OK;
+	device_free(st->grad_tile_done);
+	device_free(st->grad_deferred);
+	st->grad_tiles = 0;
+	int rc;
+	if ((rc = device_alloc(&st->grad_tile_done, (size_t)items)) || (rc = device_alloc(&st->grad_deferred, (size_t)items + 1)))
+		return rc;
+	st->grad_tiles = items;
+	return BFVM_OK;
+}
+
 // The whole LOD step (src/solver/host/diffusion_solver.cpp:512-544): overwrite, then per axis the
 // sweep and the overwrite after it.  A staged sweep writes that overwrite itself, tile by tile
 // right after storing the tile, from the list grouped by its tiles; other sweeps are followed by
@@ -304,21 +328,14 @@ int launch_diffusion(bfvm_solver* st, bool gradient, bool* gradient_done)
 		// the overwrite written by the sweep itself
 		const bool overwrite_after = st->dir_qcount + st->dir_count > 0;
 		grad_fuse gf;
-		const bool fuse_grad = gradient && axis == 2 && st->grad_fused && st->batch_refs == 0 && st->slab_count == 1
+		bool fuse_grad = gradient && axis == 2 && st->grad_fused && st->batch_refs == 0 && st->slab_count == 1
 							   && st->plan[2].vP > 1 && (!overwrite_after || a.dir.items > 0);
+		if (fuse_grad && (rc = grad_fuse_buffers(st)))
+			return rc;
+		if (fuse_grad && st->grad_tiles < ((long long)st->grid[1] * st->grid[0] * st->S + 31) / 32)
+			fuse_grad = false; // inside a capture before the buffers exist: the gradient kernel follows
 		if (fuse_grad)
 		{
-			const long long items = ((long long)st->grid[1] * st->grid[0] * st->S + 31) / 32; // z tiles
-			if (st->grad_tiles < items)
-			{
-				device_free(st->grad_tile_done);
-				device_free(st->grad_deferred);
-				st->grad_tiles = 0;
-				if ((rc = device_alloc(&st->grad_tile_done, (size_t)items))
-					|| (rc = device_alloc(&st->grad_deferred, (size_t)items + 1)))
-					return rc;
-				st->grad_tiles = items;
-			}
 			gf.g = st->grad;
 			gf.tile_done = st->grad_tile_done;
 			gf.deferred = st->grad_deferred;

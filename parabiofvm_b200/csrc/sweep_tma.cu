@@ -257,9 +257,13 @@ __device__ __forceinline__ void publish_tile(const grad_fuse& f, long long t)
 
 // The gradient of z tile g: columns 32g .. 32g + 31 of the y*x*s plane over every plane, the same
 // arithmetic as gradient.cu (bit for bit).  Thread (lane, j) of a group of P warps marches column
-// 32g + lane over planes [j c, (j + 1) c), c = ceil(Z / P), keeping u(z-1), u(z), u(z+1) in
-// registers; x and y neighbours are read through L2 (coherent loads: other CTAs wrote them in this
-// kernel), the three components are stored streaming.
+// 32g + lane over planes [j c, (j + 1) c), c = ceil(Z / P), GZU planes at a time with every load
+// of those planes issued before their arithmetic, keeping u(z-1), u(z) in registers.  The field is
+// read with ordinary loads after the neighbour tiles were acquired: a 128-byte line of a plane
+// belongs to one tile, and no line is read before its tile is published, so L1 can only hold final
+// values.  The three components are stored streaming.
+static constexpr int GZU = 4;
+
 __device__ __forceinline__ void gradient_tile(const grad_fuse& f, const float* u, long long g, int lane, int j, int P)
 {
 	const long long plane = (long long)f.Y * f.X * f.S;
@@ -278,27 +282,51 @@ __device__ __forceinline__ void gradient_tile(const grad_fuse& f, const float* u
 	const float fx = (x == 0 || x == f.X - 1) ? f.bx : f.cx;
 	const int yo_hi = y == f.Y - 1 ? 0 : XS, yo_lo = y == 0 ? 0 : XS;
 	const float fy = (y == 0 || y == f.Y - 1) ? f.by : f.cy;
+	const bool hasx = f.X > 1, hasy = f.Y > 1;
 	const float* p = u + (long long)z0 * plane + q;
 	float* gp = f.g + (long long)z0 * plane + q;
-	float prev = z0 > 0 ? __ldcg(p - plane) : 0.f;
-	float cur = __ldcg(p);
-	for (int z = z0; z < z1; z++, p += plane, gp += plane)
+	float prev = z0 > 0 ? p[-plane] : 0.f;
+	float cur = *p;
+	for (int z = z0; z < z1; z += GZU)
 	{
-		const float next = z + 1 < f.Z ? __ldcg(p + plane) : cur;
-		const float gx = f.X == 1 ? 0.f : __fmul_rn(__fsub_rn(__ldcg(p + xo_hi), __ldcg(p - xo_lo)), fx);
-		const float gy = f.Y == 1 ? 0.f : __fmul_rn(__fsub_rn(__ldcg(p + yo_hi), __ldcg(p - yo_lo)), fy);
-		float gz;
-		if (z == 0)
-			gz = __fmul_rn(__fsub_rn(next, cur), f.bz);
-		else if (z == f.Z - 1)
-			gz = __fmul_rn(__fsub_rn(cur, prev), f.bz);
-		else
-			gz = __fmul_rn(__fsub_rn(next, prev), f.cz);
-		__stcs(gp, gx);
-		__stcs(gp + f.total, gy);
-		__stcs(gp + 2 * f.total, gz);
-		prev = cur;
-		cur = next;
+		float nx[GZU], xa[GZU], xb[GZU], ya[GZU], yb[GZU];
+#pragma unroll
+		for (int k = 0; k < GZU; k++)
+		{
+			const int zz = z + k;
+			const float* pk = p + (long long)k * plane;
+			const bool in = zz < z1;
+			nx[k] = (in && zz + 1 < f.Z) ? pk[plane] : 0.f;
+			xa[k] = (in && hasx) ? pk[xo_hi] : 0.f;
+			xb[k] = (in && hasx) ? pk[-xo_lo] : 0.f;
+			ya[k] = (in && hasy) ? pk[yo_hi] : 0.f;
+			yb[k] = (in && hasy) ? pk[-yo_lo] : 0.f;
+		}
+#pragma unroll
+		for (int k = 0; k < GZU; k++)
+		{
+			const int zz = z + k;
+			if (zz >= z1)
+				break;
+			const float next = zz + 1 < f.Z ? nx[k] : cur;
+			const float gx = hasx ? __fmul_rn(__fsub_rn(xa[k], xb[k]), fx) : 0.f;
+			const float gy = hasy ? __fmul_rn(__fsub_rn(ya[k], yb[k]), fy) : 0.f;
+			float gz;
+			if (zz == 0)
+				gz = __fmul_rn(__fsub_rn(next, cur), f.bz);
+			else if (zz == f.Z - 1)
+				gz = __fmul_rn(__fsub_rn(cur, prev), f.bz);
+			else
+				gz = __fmul_rn(__fsub_rn(next, prev), f.cz);
+			float* o = gp + (long long)k * plane;
+			__stcs(o, gx);
+			__stcs(o + f.total, gy);
+			__stcs(o + 2 * f.total, gz);
+			prev = cur;
+			cur = next;
+		}
+		p += (long long)GZU * plane;
+		gp += (long long)GZU * plane;
 	}
 }
 
