@@ -330,6 +330,86 @@ __device__ __forceinline__ void gradient_tile(const grad_fuse& f, const float* u
 	}
 }
 
+// The same gradient four substrates at a time (S % 4 == 0), with 16-byte accesses: thread (lane, j)
+// owns columns 32g + 4 (lane % 8) .. + 3, and the four lanes that share them (lane / 8) split warp
+// j's planes between them.  Four times the bytes in flight per load of the scalar form.
+static constexpr int GZU4 = 1;
+
+__device__ __forceinline__ float4 grad4(float4 a, float4 b, float f)
+{
+	return make_float4(__fmul_rn(__fsub_rn(a.x, b.x), f), __fmul_rn(__fsub_rn(a.y, b.y), f),
+					   __fmul_rn(__fsub_rn(a.z, b.z), f), __fmul_rn(__fsub_rn(a.w, b.w), f));
+}
+
+__device__ __forceinline__ void gradient_tile4(const grad_fuse& f, const float* u, long long g, int lane, int j, int P)
+{
+	const long long plane = (long long)f.Y * f.X * f.S;
+	const long long q = g * 32 + 4 * (lane & 7);
+	if (q >= plane)
+		return;
+	const int XS = f.X * f.S;
+	const int y = (int)(q / XS);
+	const int x = (int)(q - (long long)y * XS) / f.S;
+	const int chunk = (f.Z + P - 1) / P;
+	const int sub = (chunk + 3) / 4;
+	const int zj = j * chunk, zj1 = min(f.Z, zj + chunk);
+	const int z0 = zj + (lane >> 3) * sub;
+	const int z1 = min(zj1, z0 + sub);
+	if (z0 >= z1)
+		return;
+	const int xo_hi = x == f.X - 1 ? 0 : f.S, xo_lo = x == 0 ? 0 : f.S;
+	const float fx = (x == 0 || x == f.X - 1) ? f.bx : f.cx;
+	const int yo_hi = y == f.Y - 1 ? 0 : XS, yo_lo = y == 0 ? 0 : XS;
+	const float fy = (y == 0 || y == f.Y - 1) ? f.by : f.cy;
+	const bool hasx = f.X > 1, hasy = f.Y > 1;
+	const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+	const float* p = u + (long long)z0 * plane + q;
+	float* gp = f.g + (long long)z0 * plane + q;
+	float4 prev = z0 > 0 ? *reinterpret_cast<const float4*>(p - plane) : zero;
+	float4 cur = *reinterpret_cast<const float4*>(p);
+	for (int z = z0; z < z1; z += GZU4)
+	{
+		float4 nx[GZU4], xa[GZU4], xb[GZU4], ya[GZU4], yb[GZU4];
+#pragma unroll
+		for (int k = 0; k < GZU4; k++)
+		{
+			const int zz = z + k;
+			const float* pk = p + (long long)k * plane;
+			const bool in = zz < z1;
+			nx[k] = (in && zz + 1 < f.Z) ? *reinterpret_cast<const float4*>(pk + plane) : zero;
+			xa[k] = (in && hasx) ? *reinterpret_cast<const float4*>(pk + xo_hi) : zero;
+			xb[k] = (in && hasx) ? *reinterpret_cast<const float4*>(pk - xo_lo) : zero;
+			ya[k] = (in && hasy) ? *reinterpret_cast<const float4*>(pk + yo_hi) : zero;
+			yb[k] = (in && hasy) ? *reinterpret_cast<const float4*>(pk - yo_lo) : zero;
+		}
+#pragma unroll
+		for (int k = 0; k < GZU4; k++)
+		{
+			const int zz = z + k;
+			if (zz >= z1)
+				break;
+			const float4 next = zz + 1 < f.Z ? nx[k] : cur;
+			const float4 gx = hasx ? grad4(xa[k], xb[k], fx) : zero;
+			const float4 gy = hasy ? grad4(ya[k], yb[k], fy) : zero;
+			float4 gz;
+			if (zz == 0)
+				gz = grad4(next, cur, f.bz);
+			else if (zz == f.Z - 1)
+				gz = grad4(cur, prev, f.bz);
+			else
+				gz = grad4(next, prev, f.cz);
+			float* o = gp + (long long)k * plane;
+			__stcs(reinterpret_cast<float4*>(o), gx);
+			__stcs(reinterpret_cast<float4*>(o + f.total), gy);
+			__stcs(reinterpret_cast<float4*>(o + 2 * f.total), gz);
+			prev = cur;
+			cur = next;
+		}
+		p += (long long)GZU4 * plane;
+		gp += (long long)GZU4 * plane;
+	}
+}
+
 // Whether the tiles holding the x and y neighbours of tile g (and g itself) are published: the
 // group's threads each watch some of them, for at most spin_limit cycles.
 __device__ __forceinline__ bool neighbours_ready(const grad_fuse& f, long long g, int gtid, int gthr, int bar_id)
@@ -368,18 +448,24 @@ __device__ __forceinline__ bool neighbours_ready(const grad_fuse& f, long long g
 }
 
 // The gradient of tile g by a group: now if its neighbours are published, else left to
-// grad_deferred_kernel.
+// grad_deferred_kernel.  VEC: the four-substrate form (S % 4 == 0).
+template <bool VEC>
 __device__ __forceinline__ void gradient_work(const grad_fuse& f, const float* u, long long g, int lane, int j, int P,
 											  int bar_id)
 {
 	const int gtid = lane + 32 * j, gthr = 32 * P;
-	if (neighbours_ready(f, g, gtid, gthr, bar_id))
-		gradient_tile(f, u, g, lane, j, P);
-	else if (gtid == 0)
+	if (!neighbours_ready(f, g, gtid, gthr, bar_id))
 	{
-		const int k = atomicAdd(f.deferred, 1);
-		f.deferred[1 + k] = (int)g;
+		if (gtid == 0)
+		{
+			const int k = atomicAdd(f.deferred, 1);
+			f.deferred[1 + k] = (int)g;
+		}
 	}
+	else if (VEC)
+		gradient_tile4(f, u, g, lane, j, P);
+	else
+		gradient_tile(f, u, g, lane, j, P);
 }
 
 // The tiles whose gradient the sweep left behind, after the sweep: CTAs of (32, P) threads.
@@ -387,14 +473,20 @@ __global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constan
 {
 	const int n = *(volatile int*)f.deferred;
 	for (int k = blockIdx.x; k < n; k += gridDim.x)
-		gradient_tile(f, u, f.deferred[1 + k], threadIdx.x, threadIdx.y, blockDim.y);
+	{
+		if (f.S % 4 == 0)
+			gradient_tile4(f, u, f.deferred[1 + k], threadIdx.x, threadIdx.y, blockDim.y);
+		else
+			gradient_tile(f, u, f.deferred[1 + k], threadIdx.x, threadIdx.y, blockDim.y);
+	}
 }
 
 // SLAB (y/z tiles only): 0 a plain sweep; 1 the solve pass of a z-slab, which enters every line
 // with the carries C (left) and X (right) of slab_carry: it always runs the carry folds, from C and
 // X instead of zero, with the tables of precompute_padded_range.
-// GRAD (z sweep, P > 1): the gradient of the step inside the sweep (grad_fuse).
-template <bool ROWS, bool NOALLOC, int SLAB, bool GRAD>
+// GRAD (z sweep, P > 1): the gradient of the step inside the sweep (grad_fuse); 1 the scalar form,
+// 4 the four-substrate form (S % 4 == 0).
+template <bool ROWS, bool NOALLOC, int SLAB, int GRAD>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt, const __grid_constant__ grad_fuse gf)
@@ -640,7 +732,7 @@ __global__ void __launch_bounds__(640, 1)
 			}
 		}
 		if (GRAD && w >= gf.lag)
-			gradient_work(gf, a.data, w - gf.lag, lane, j, P, bar_id);
+			gradient_work<GRAD == 4>(gf, a.data, w - gf.lag, lane, j, P, bar_id);
 #pragma unroll
 		for (int k = 0; k < 4; k++)
 			dir_prev[k] = dir_cur[k];
@@ -662,7 +754,7 @@ __global__ void __launch_bounds__(640, 1)
 		// the gradients still owed: tiles w - lag of this group's stride past the last tile
 		for (; w - gf.lag < tt.items; w += wstride)
 			if (w >= gf.lag)
-				gradient_work(gf, a.data, w - gf.lag, lane, j, P, bar_id);
+				gradient_work<GRAD == 4>(gf, a.data, w - gf.lag, lane, j, P, bar_id);
 	}
 	if (failed && leader)
 	{
@@ -701,7 +793,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 
 static constexpr int TMA_MAX_P = 16;
 
-template <bool ROWS, bool NOALLOC, int SLAB = 0, bool GRAD = false>
+template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem, const grad_fuse* gfp = nullptr)
 {
@@ -870,7 +962,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	if (gf && a.vP > 1)
 	{
 		tt.evict_first = st->grad_evict_first ? 1 : 0;
-		return launch_tma_variant<false, false, 0, true>(st, a, map, tt, smem, gf);
+		if (S % 4 == 0)
+			return launch_tma_variant<false, false, 0, 4>(st, a, map, tt, smem, gf);
+		return launch_tma_variant<false, false, 0, 1>(st, a, map, tt, smem, gf);
 	}
 	handled = !gf; // a gradient was asked for and this shape cannot compute it: the caller sweeps
 	if (!handled)
