@@ -684,25 +684,26 @@ def measure_surrogate(train_steps=10, warmup=3, fallback_macro_steps=100, fresh_
     # the trained network rolled out alone for 8 macro-steps from a field and agents of its training
     # distribution (uniform agents), against plain stepping: its relative L2 error after each
     rollout = []
-    with torch.cuda.stream(net.stream):
-        g_field, g_src, g_sink = [torch.empty((1, VS), device="cuda") for _ in range(3)]
-    su.random_field(env.grid, env.S, np.random.default_rng(19), g_field[0], net.stream)
     ua = su.random_agents(env, np.random.default_rng(17), 55_000)
+    dev_ua = {k: torch.from_numpy(np.ascontiguousarray(v, np.float32)).cuda() for k, v in ua.items()}
+    torch.cuda.synchronize()
     s = env.solver()
     s.set_stream(net.stream.cuda_stream)
     s.store_agents(ua["sec"], ua["sat"], ua["upt"], ua["nex"], np.zeros_like(ua["sec"]), None, ua["vol"], ua["pos"])
-    dev_ua = {k: torch.from_numpy(np.ascontiguousarray(v, np.float32)).cuda() for k, v in ua.items()}
-    su.agent_rates((0, 0, 0), (env.dx,) * 3, env.grid, env.time_step, dev_ua, g_src[0], g_sink[0], net.stream)
-    s.store_densities_device(g_field[0])
-    sur_field = g_field[0].clone()
-    plain_now = torch.empty_like(sur_field)
-    for m in range(8):
-        run_net.infer(sur_field, g_src[0], g_sink[0], out1)
-        sur_field.copy_(out1)
-        s.run_steps(16, 16 * m)
-        s.load_densities_device(plain_now)
-        s.synchronize()
-        rollout.append(su.rel_l2(sur_field, plain_now))
+    with torch.cuda.stream(net.stream):  # every step below in order on the network's stream
+        g_field, g_src, g_sink = [torch.empty((1, VS), device="cuda") for _ in range(3)]
+        su.random_field(env.grid, env.S, np.random.default_rng(19), g_field[0], net.stream)
+        su.agent_rates((0, 0, 0), (env.dx,) * 3, env.grid, env.time_step, dev_ua, g_src[0], g_sink[0], net.stream)
+        s.store_densities_device(g_field[0])
+        sur_field = g_field[0].clone()
+        plain_now = torch.empty_like(sur_field)
+        for m in range(8):
+            run_net.infer(sur_field, g_src[0], g_sink[0], out1)
+            sur_field.copy_(out1)
+            s.run_steps(16, 16 * m)
+            s.load_densities_device(plain_now)
+            rollout.append(su.rel_l2(sur_field, plain_now))
+    s.synchronize()
     s.close()
 
     # the controller over 1,600 steps, from a field of the training distribution
@@ -1013,14 +1014,15 @@ def run_ours(args):
     names = ["sweep_x", "sweep_y", "sweep_z"]
     for axis in range(w.dims):
         kernels[names[axis]] = {"ms": timed(lambda: s.sweep(axis)), "bytes": 8 * VS}
-    # the three sweeps with the gradient inside the z sweep (bfvm_diffusion_gradient_solve): the
-    # z sweep with its gradient is that time less the x and y sweeps
+    # the three sweeps with the gradient inside the z sweep (option fused_gradient): the z sweep
+    # with its gradient is that time less the x and y sweeps
     if w.dims == 3:
+        s.set_option("fused_gradient", 1)
         ms_dg = timed(s.diffusion_gradient)
-        kernels["diffusion_gradient"] = {"ms": ms_dg, "bytes": (24 + 12) * VS}
-        kernels["sweep_z_gradient"] = {"ms": ms_dg - kernels["sweep_x"]["ms"] - kernels["sweep_y"]["ms"],
-                                       "bytes": (8 + 12) * VS,
-                                       "how": "diffusion_gradient less the x and y sweeps"}
+        s.set_option("fused_gradient", 0)
+        kernels["sweep_z_with_gradient_inside"] = {
+            "ms": ms_dg - kernels["sweep_x"]["ms"] - kernels["sweep_y"]["ms"], "bytes": (8 + 12) * VS,
+            "how": "bfvm_diffusion_gradient_solve with the option fused_gradient, less the x and y sweeps"}
     for (dim, is_max), (vals, conds) in w.boundary.items():
         s.set_boundary_dirichlet(dim, is_max, vals, conds)
     if w.interior_voxels is not None:
@@ -1032,15 +1034,16 @@ def run_ours(args):
     kernels["secretion"] = {"ms": timed(lambda: s.secretion(False)),
                             "bytes": A * w.S * (12 + 8 + (20 if w.compute_internalized else 0))}
     kernels["secretion_rebin"] = {"ms": timed(lambda: s.secretion(True)), "bytes": None}
-    # a whole non-recompute step (graph replay) with the gradient inside the z sweep (the default)
-    # and with the gradient kernel after the sweep and the Dirichlet overwrites as scatters
-    kernels["step_fused"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
-    s.set_option("fused_gradient", 0)
-    kernels["step_gradient_kernel"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
-    s.set_option("fused_dirichlet", 0)
-    kernels["step_unfused"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
+    # a whole non-recompute step (graph replay) as configured by default (the Dirichlet scatters and
+    # the gradient kernel), then with the Dirichlet overwrites written by the sweeps, then with the
+    # gradient inside the z sweep as well
+    kernels["step"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
     s.set_option("fused_dirichlet", 1)
+    kernels["step_fused_dirichlet"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
     s.set_option("fused_gradient", 1)
+    kernels["step_fused_dirichlet_gradient"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
+    s.set_option("fused_dirichlet", 0)
+    s.set_option("fused_gradient", 0)
     s.synchronize()
     peak, peak_kind = measured_peak()
     for k in kernels.values():
@@ -1049,20 +1052,13 @@ def run_ours(args):
     sweep_ms = sum(k["ms"] for k in sweeps) / len(sweeps)
     kernels["sweep_mean"] = {"ms": sweep_ms, "bytes": 8 * VS, "gbs": 8 * VS / (sweep_ms / 1e3) / 1e9}
     traffic_rec = committed_traffic().get(args.workload, {})
-    if "sweep_z_gradient" in kernels:
-        # the dominant kernel: the z sweep with the gradient inside it (the largest share of the
-        # step): 4 B read + 4 B written by the sweep and 12 B of gradient written per voxel*substrate
-        kz = kernels["sweep_z_gradient"]
-        roofline = {"bound": "hbm", "kernel": "sweep_tma_kernel z with the gradient inside (sweep_z_gradient)",
-                    "achieved": kz["bytes"] / (kz["ms"] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                    "traffic": traffic_rec.get("sweep_z_gradient"), "peak_source": f"{peak_kind} hbm_gbs (copy)",
-                    "algorithmic_bytes_per_launch": kz["bytes"], "ms_per_launch": kz["ms"],
-                    "ms_how": kz["how"]}
-    else:
-        roofline = {"bound": "hbm", "kernel": "sweep (mean of the launches)",
-                    "achieved": 8 * VS / (sweep_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                    "traffic": traffic_rec.get("sweep"), "peak_source": f"{peak_kind} hbm_gbs (copy)",
-                    "algorithmic_bytes_per_launch": 8 * VS, "ms_per_launch": sweep_ms}
+    # the dominant kernel: the sweep kernel (three launches per step, the largest share of the
+    # step's launch list); its achieved bandwidth is the per-launch algorithmic bytes over the mean
+    # launch time
+    roofline = {"bound": "hbm", "kernel": "sweep_tma_kernel (mean of the x, y, z launches)",
+                "achieved": 8 * VS / (sweep_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "traffic": traffic_rec.get("sweep"), "peak_source": f"{peak_kind} hbm_gbs (copy)",
+                "algorithmic_bytes_per_launch": 8 * VS, "ms_per_launch": sweep_ms}
     roofline["frac"] = roofline["achieved"] / peak
     step_bytes = algorithmic_step_bytes(w)
     step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9

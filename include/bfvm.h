@@ -139,9 +139,9 @@ int bfvm_dirichlet_solve(bfvm_solver* s);
 int bfvm_gradient_solve(bfvm_solver* s);
 /* bfvm_diffusion_solve followed by bfvm_gradient_solve (diffusion_solver::solve then
  * gradient_solver::solve, as src/main.cpp:76-90 calls them), with the gradient computed inside the
- * z sweep where the staged sweep takes the mesh: each tile's gradient is computed from the planes
- * the sweep just wrote, while they are still in L2, instead of re-reading the field from memory.
- * The results are the same bits as the two calls. */
+ * z sweep when the option "fused_gradient" is set and the staged sweep takes the mesh: each tile's
+ * gradient is computed from the planes the sweep just wrote, while they are still in L2.  The
+ * results are the same bits as the two calls. */
 int bfvm_diffusion_gradient_solve(bfvm_solver* s);
 /* Secretion and uptake (cell_solver::simulate_secretion_and_uptake); recompute != 0 rebuilds the
  * per-voxel reductions from the current agent data and positions. */
@@ -195,12 +195,12 @@ int bfvm_synchronize(bfvm_solver* s);
  * - "tma_sweeps" 0/1 stages sweep tiles through shared memory with the TMA (default 1; 0 selects
  *   the kernels that read the field directly).  Results agree to rounding either way.
  * - "fused_dirichlet" 0/1: in the LOD step (bfvm_diffusion_solve, bfvm_run_steps) a staged sweep
- *   writes the Dirichlet overwrite that follows it, tile by tile (default 1; 0 runs it as a
- *   separate scatter).  Results are identical either way.
+ *   writes the Dirichlet overwrite that follows it, tile by tile (default 0: the scatter kernel
+ *   after the sweep, measured faster).  Results are identical either way.
  * - "fused_gradient" 0/1: in bfvm_run_steps and bfvm_diffusion_gradient_solve the z sweep computes
- *   the gradient from the planes it has just written (default 1; 0 runs the gradient kernel after
- *   the sweep).  Results are identical either way.  "fused_gradient_evict_first" 0/1 (default 1):
- *   that sweep reads its tiles with an L2 evict-first policy, keeping the written planes in L2.
+ *   the gradient from the planes it has just written (default 0: the gradient kernel after the
+ *   sweep, measured faster).  Results are identical either way.  "fused_gradient_evict_first" 0/1
+ *   (default 1): that sweep reads its tiles with an L2 evict-first policy.
  * - "wait_limit_cycles" bounds every wait of the staged sweeps on a tile copy, in GPU clock cycles
  *   (default 4e9, about two seconds; accepted range [1e4, 4e10]).  A wait that runs out makes the
  *   kernel give up its tile, let its copies in flight land and return; the next synchronising call

@@ -170,8 +170,11 @@ struct bfvm_solver
 
 	long long launches = 0;
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
-	bool dir_fused = true;		 // staged sweeps of the LOD step write the overwrite that follows them
-	bool grad_fused = true;		 // the z sweep of a step computes the gradient (sweep_tma.cu)
+	// measured slower than the scatter kernel and the gradient kernel at 320^3 x 16 (the extra work
+	// in every tile of a latency-bound sweep costs more than the launches it saves), so off unless
+	// asked for with bfvm_set_option
+	bool dir_fused = false;		 // staged sweeps of the LOD step write the overwrite that follows them
+	bool grad_fused = false;	 // the z sweep of a step computes the gradient (sweep_tma.cu)
 	bool grad_evict_first = true; // ... reading its tiles with an L2 evict-first policy
 	int* grad_tile_done = nullptr; // [z tiles] and [1 + z tiles] of the gradient inside the z sweep
 	int* grad_deferred = nullptr;

@@ -159,13 +159,14 @@ def test_dirichlet_interior_duplicates_last_wins():
 
 @pytest.mark.parametrize("edge,S,dims", [(48, 4, 3), (40, 16, 3), (70, 5, 3), (100, 4, 2), (300, 8, 1)])
 def test_fused_dirichlet_identical_to_scatter(edge, S, dims):
-    """The staged sweeps write the overwrite that follows them tile by tile; the result must be the
-    same bits as the separate scatter kernel (option fused_dirichlet 0), faces and interior voxels
-    with duplicates alike."""
+    """With the option fused_dirichlet the staged sweeps write the overwrite that follows them tile
+    by tile; the result must be the same bits as the scatter kernel (the default), for faces and
+    interior voxels alike."""
     scn = synthetic(edge, S, 1500 if dims == 3 else 0, seed=edge + S, clustered=True, sigma=60.0,
                     interior_fraction=0.03, dims=dims)
     fused = gpu_runner(scn)
     plain = gpu_runner(scn)
+    fused.s.set_option("fused_dirichlet", 1)
     plain.s.set_option("fused_dirichlet", 0)
     fused.run_steps(4)
     plain.run_steps(4)
@@ -179,15 +180,17 @@ def test_fused_dirichlet_identical_to_scatter(edge, S, dims):
 @pytest.mark.parametrize("edge,S,dirichlet", [(96, 16, True), (70, 4, True), (54, 2, False), (40, 8, True),
                                               (100, 5, False)])
 def test_gradient_inside_z_sweep_identical(edge, S, dirichlet):
-    """Within a step the z sweep computes the gradient itself, tile by tile once the neighbouring
-    tiles hold their final values (option fused_gradient; 0 runs the gradient kernel after the
-    sweep).  The gradients and fields must be the same bits.  The cases cover tiles that straddle
+    """With the option fused_gradient the z sweep of a step computes the gradient itself, tile by
+    tile once the neighbouring tiles hold their final values (the default runs the gradient kernel
+    after the sweep).  The gradients and fields must be the same bits.  The cases cover tiles that straddle
     rows of the y*x*s plane (54 x 2), meshes smaller than the lag (every gradient after the sweep
     loop), and steps with and without the Dirichlet overwrite written by the sweep."""
     scn = synthetic(edge, S, 1200, seed=3 * edge + S, clustered=True, sigma=60.0,
                     interior_fraction=0.02 if dirichlet else 0.0, boundary_substrate0=dirichlet)
     fused = gpu_runner(scn)
     plain = gpu_runner(scn)
+    fused.s.set_option("fused_dirichlet", 1)
+    fused.s.set_option("fused_gradient", 1)
     plain.s.set_option("fused_gradient", 0)
     for first, n in ((0, 3), (3, 9)):
         fused.run_steps(n, first)
