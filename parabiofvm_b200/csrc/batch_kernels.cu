@@ -321,8 +321,10 @@ __device__ __forceinline__ void x_tile_rows(const ens_inst& m, long long local, 
 // double-buffered, measured 8% slower over a 256-mesh ensemble.)
 // Two CTAs of 512 threads per SM (64 registers): at 114 registers a mesh of 3 blocks per line ran 5
 // CTAs of 3 warps per SM, too few warps to hide the loads and barriers.
+// MINB 0: lines of 17 to 32 blocks (one mesh alone), CTAs of up to 1024 threads, one per SM; the
+// register cap (64) is that of MINB 2.
 template <int AXIS, int MINB>
-__global__ void __launch_bounds__(512, MINB) ens_sweep_kernel(const ens_inst* __restrict__ inst,
+__global__ void __launch_bounds__(MINB == 0 ? 1024 : 512, MINB == 0 ? 1 : MINB) ens_sweep_kernel(const ens_inst* __restrict__ inst,
 														 const long long* __restrict__ first, int count,
 														 long long units, long long chunk, int maxP)
 {
@@ -640,12 +642,17 @@ int ensemble_secretion(const ensemble_plan& plan, cudaStream_t stream)
 	return launched("ens_secretion_kernel");
 }
 
+static size_t ens_sweep_smem(const ensemble_plan& plan, int axis)
+{
+	return (2 * (size_t)plan.maxP[axis] * 32 + plan.table_floats[axis]) * sizeof(float);
+}
+
 template <int AXIS, int MINB>
 static int launch_ens_sweep(const ensemble_plan& plan, long long units, cudaStream_t stream)
 {
 	auto kernel = ens_sweep_kernel<AXIS, MINB>;
 	const int P = plan.maxP[AXIS];
-	const size_t smem = (2 * (size_t)P * 32 + plan.table_floats[AXIS]) * sizeof(float);
+	const size_t smem = ens_sweep_smem(plan, AXIS);
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
@@ -658,11 +665,27 @@ static int launch_ens_sweep(const ensemble_plan& plan, long long units, cudaStre
 	return launched("ens_sweep_kernel");
 }
 
+bool ensemble_sweep_fits(const ensemble_plan& plan, int axis)
+{
+	int dev = 0, optin = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+	return plan.maxP[axis] <= ENS_MAX_P_ONE && ens_sweep_smem(plan, axis) <= (size_t)optin;
+}
+
 int ensemble_sweep(const ensemble_plan& plan, int axis, cudaStream_t stream)
 {
 	const long long units = plan.count ? plan.first_h[ENS_SWEEP_X + axis][plan.count] : 0;
 	if (units == 0)
 		return BFVM_OK;
+	if (plan.maxP[axis] > ENS_MAX_P)
+	{
+		if (axis == 0)
+			return launch_ens_sweep<0, 0>(plan, units, stream);
+		if (axis == 1)
+			return launch_ens_sweep<1, 0>(plan, units, stream);
+		return launch_ens_sweep<2, 0>(plan, units, stream);
+	}
 	const bool one = plan.tune.sweep_minb[axis] == 1;
 	if (axis == 0)
 		return one ? launch_ens_sweep<0, 1>(plan, units, stream) : launch_ens_sweep<0, 2>(plan, units, stream);

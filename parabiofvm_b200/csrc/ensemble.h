@@ -8,7 +8,8 @@
 
 namespace bfvm {
 
-static constexpr int ENS_MAX_P = 16; // blocks of 32 per line the ensemble sweep handles
+static constexpr int ENS_MAX_P = 16;	 // blocks of 32 per line the ensemble sweep handles in a batch
+static constexpr int ENS_MAX_P_ONE = 32; // ... for one mesh alone (CTAs of up to 1024 threads)
 
 // Everything a kernel needs of one mesh (device copy in ensemble_plan::inst).
 struct ens_inst
@@ -90,6 +91,8 @@ void ensemble_free(ensemble_plan& plan);
 // meshes with k <= dims (before sweep k, or after the last sweep).
 int ensemble_dirichlet(const ensemble_plan& plan, int dirichlet_phase, cudaStream_t stream);
 int ensemble_sweep(const ensemble_plan& plan, int axis, cudaStream_t stream);
+// whether the ensemble sweep of `axis` fits the shared memory of a CTA on this device
+bool ensemble_sweep_fits(const ensemble_plan& plan, int axis);
 int ensemble_gradient(const ensemble_plan& plan, cudaStream_t stream);
 int ensemble_secretion(const ensemble_plan& plan, cudaStream_t stream);
 

@@ -258,7 +258,8 @@ static int sweep_axis(bfvm_solver* st, int axis, const sweep_args& a, bool& stag
 		return sweep_axis(st, axis, a, staged); // the shape cannot take the gradient: sweep alone
 	staged = handled;
 	// the same front-padded block algebra without TMA staging, where the lines fit 16 blocks
-	if (!rc && !handled && st->self_plan && pl.vtab && pl.vP <= ENS_MAX_P && (axis > 0 || st->S <= 32))
+	if (!rc && !handled && st->self_plan && pl.vtab && pl.vP <= ENS_MAX_P_ONE && (axis > 0 || st->S <= 32)
+		&& ensemble_sweep_fits(*st->self_plan, axis))
 	{
 		rc = ensemble_sweep(*st->self_plan, axis, st->stream);
 		if (!rc)

@@ -197,3 +197,46 @@ def test_gradient_inside_z_sweep_identical(edge, S, dirichlet):
         plain.run_steps(n, first)
         np.testing.assert_array_equal(fused.gradients(), plain.gradients())
         np.testing.assert_array_equal(fused.densities(), plain.densities())
+
+
+def _box(grid, S, seed, interior_fraction=0.01):
+    """A seeded mesh of grid = (X, Y, Z) voxels of 20 um, the synthetic distributions of
+    workloads.synthetic, Dirichlet 1.0 on substrate 0 at every face and some interior voxels."""
+    from parabiofvm_b200.workloads import Workload
+
+    rng = np.random.default_rng(seed)
+    w = Workload(dims=3, bbox_min=(0, 0, 0), bbox_max=tuple(20 * g for g in grid), voxel_shape=(20, 20, 20),
+                 diffusion_coefficients=list(np.exp(rng.uniform(np.log(1e3), np.log(1e5), S))),
+                 decay_rates=list(rng.uniform(0.01, 1.0, S)), time_step=0.01, initial_conditions=[0.0] * S)
+    w.densities = rng.uniform(0, 1, grid[0] * grid[1] * grid[2] * S).astype(np.float32)
+    for d in range(3):
+        for is_max in (False, True):
+            vals = np.zeros(S)
+            conds = np.zeros(S, dtype=bool)
+            vals[0], conds[0] = 1.0, True
+            w.boundary[(d, is_max)] = (vals, conds)
+    inner = [g - 2 for g in grid]
+    n = int(interior_fraction * inner[0] * inner[1] * inner[2])
+    pick = rng.choice(inner[0] * inner[1] * inner[2], size=n, replace=False)
+    w.interior_voxels = np.stack([pick % inner[0] + 1, (pick // inner[0]) % inner[1] + 1,
+                                  pick // (inner[0] * inner[1]) + 1], axis=1).astype(np.int32)
+    w.interior_values = rng.uniform(0, 1, (n, S))
+    w.interior_conditions = np.ones((n, S), dtype=bool)
+    return w
+
+
+@pytest.mark.parametrize("grid,S", [((1000, 12, 12), 4), ((12, 700, 12), 4), ((12, 12, 1000), 3), ((640, 20, 8), 8)])
+def test_lines_longer_than_512_voxels(grid, S):
+    """Lines of 17 to 32 blocks of 32 (513 to 1024 voxels), beyond the staged sweep's 16 blocks, run
+    the same front-padded block algebra in the ensemble sweep on one mesh, CTAs of up to 1024
+    threads; one step and three full steps against the FP32 oracle at the multi-block bar."""
+    w = _box(grid, S, seed=sum(grid) + S)
+    o = make_oracle(w, np.float32)
+    g = gpu_runner(w)
+    o.diffusion()
+    g.diffusion()
+    assert rel_err(g.densities(), o.densities()) < 1e-5
+    o.run_steps(3, 1)
+    g.run_steps(3, 1)
+    assert rel_err(g.densities(), o.densities()) < 1e-5
+    g.close()
