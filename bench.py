@@ -988,78 +988,82 @@ def run_ours(args):
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = whole_job_rate(world, VS, args.steps, ms)
 
-    # ---- per-kernel timing on the same stream (the roofline numerator)
-    kernels = {}
-    reps = args.kernel_reps
-
-    def timed(fn):
-        fn()
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(reps):
-            fn()
-        b.record(stream)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / reps
-
-    # the sweeps alone: the Dirichlet conditions are lifted while they are timed, then put back
-    # and their overwrite is timed on its own
-    for dim in range(w.dims):
-        for is_max in (0, 1):
-            s.set_boundary_dirichlet(dim, is_max, None, None)
-    s.set_interior_dirichlet(np.zeros((0, w.dims), np.int32), np.zeros((0, w.S), np.float32),
-                             np.zeros((0, w.S), bool))
-    names = ["sweep_x", "sweep_y", "sweep_z"]
-    for axis in range(w.dims):
-        kernels[names[axis]] = {"ms": timed(lambda: s.sweep(axis)), "bytes": 8 * VS}
-    # the three sweeps with the gradient inside the z sweep (option fused_gradient): the z sweep
-    # with its gradient is that time less the x and y sweeps
-    if w.dims == 3:
-        s.set_option("fused_gradient", 1)
-        ms_dg = timed(s.diffusion_gradient)
-        s.set_option("fused_gradient", 0)
-        kernels["sweep_z_with_gradient_inside"] = {
-            "ms": ms_dg - kernels["sweep_x"]["ms"] - kernels["sweep_y"]["ms"], "bytes": (8 + 12) * VS,
-            "how": "bfvm_diffusion_gradient_solve with the option fused_gradient, less the x and y sweeps"}
-    for (dim, is_max), (vals, conds) in w.boundary.items():
-        s.set_boundary_dirichlet(dim, is_max, vals, conds)
-    if w.interior_voxels is not None:
-        s.set_interior_dirichlet(w.interior_voxels, w.interior_values, w.interior_conditions)
-    n_dir = dirichlet_elements(w)
-    kernels["dirichlet"] = {"ms": timed(s.dirichlet), "bytes": 16 * n_dir}
-    kernels["gradient"] = {"ms": timed(s.gradient), "bytes": (4 + 4 * w.dims) * VS}
-    A = w.agents.count
-    kernels["secretion"] = {"ms": timed(lambda: s.secretion(False)),
-                            "bytes": A * w.S * (12 + 8 + (20 if w.compute_internalized else 0))}
-    kernels["secretion_rebin"] = {"ms": timed(lambda: s.secretion(True)), "bytes": None}
-    # a whole non-recompute step (graph replay) as configured by default (the Dirichlet scatters and
-    # the gradient kernel), then with the Dirichlet overwrites written by the sweeps, then with the
-    # gradient inside the z sweep as well
-    kernels["step"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
-    s.set_option("fused_dirichlet", 1)
-    kernels["step_fused_dirichlet"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
-    s.set_option("fused_gradient", 1)
-    kernels["step_fused_dirichlet_gradient"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
-    s.set_option("fused_dirichlet", 0)
-    s.set_option("fused_gradient", 0)
-    s.synchronize()
+    # ---- per-kernel timing on the same stream (the roofline numerator); --kernel-reps 0 leaves
+    # it out (launch lists of the steps alone)
+    kernels, roofline = {}, None
     peak, peak_kind = measured_peak()
-    for k in kernels.values():
-        k["gbs"] = (k["bytes"] / (k["ms"] / 1e3) / 1e9) if k["bytes"] else None
-    sweeps = [kernels[n] for n in names[:w.dims]]
-    sweep_ms = sum(k["ms"] for k in sweeps) / len(sweeps)
-    kernels["sweep_mean"] = {"ms": sweep_ms, "bytes": 8 * VS, "gbs": 8 * VS / (sweep_ms / 1e3) / 1e9}
-    traffic_rec = committed_traffic().get(args.workload, {})
-    # the dominant kernel: the sweep kernel (three launches per step, the largest share of the
-    # step's launch list); its achieved bandwidth is the per-launch algorithmic bytes over the mean
-    # launch time
-    roofline = {"bound": "hbm", "kernel": "sweep_tma_kernel (mean of the x, y, z launches)",
-                "achieved": 8 * VS / (sweep_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                "traffic": traffic_rec.get("sweep"), "peak_source": f"{peak_kind} hbm_gbs (copy)",
-                "algorithmic_bytes_per_launch": 8 * VS, "ms_per_launch": sweep_ms}
-    roofline["frac"] = roofline["achieved"] / peak
+    if args.kernel_reps > 0:
+        kernels = {}
+        reps = args.kernel_reps
+
+        def timed(fn):
+            fn()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(reps):
+                fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) / reps
+
+        # the sweeps alone: the Dirichlet conditions are lifted while they are timed, then put back
+        # and their overwrite is timed on its own
+        for dim in range(w.dims):
+            for is_max in (0, 1):
+                s.set_boundary_dirichlet(dim, is_max, None, None)
+        s.set_interior_dirichlet(np.zeros((0, w.dims), np.int32), np.zeros((0, w.S), np.float32),
+                                 np.zeros((0, w.S), bool))
+        names = ["sweep_x", "sweep_y", "sweep_z"]
+        for axis in range(w.dims):
+            kernels[names[axis]] = {"ms": timed(lambda: s.sweep(axis)), "bytes": 8 * VS}
+        # the three sweeps with the gradient inside the z sweep (option fused_gradient): the z sweep
+        # with its gradient is that time less the x and y sweeps
+        if w.dims == 3:
+            s.set_option("fused_gradient", 1)
+            ms_dg = timed(s.diffusion_gradient)
+            s.set_option("fused_gradient", 0)
+            kernels["sweep_z_with_gradient_inside"] = {
+                "ms": ms_dg - kernels["sweep_x"]["ms"] - kernels["sweep_y"]["ms"], "bytes": (8 + 12) * VS,
+                "how": "bfvm_diffusion_gradient_solve with the option fused_gradient, less the x and y sweeps"}
+        for (dim, is_max), (vals, conds) in w.boundary.items():
+            s.set_boundary_dirichlet(dim, is_max, vals, conds)
+        if w.interior_voxels is not None:
+            s.set_interior_dirichlet(w.interior_voxels, w.interior_values, w.interior_conditions)
+        n_dir = dirichlet_elements(w)
+        kernels["dirichlet"] = {"ms": timed(s.dirichlet), "bytes": 16 * n_dir}
+        kernels["gradient"] = {"ms": timed(s.gradient), "bytes": (4 + 4 * w.dims) * VS}
+        A = w.agents.count
+        kernels["secretion"] = {"ms": timed(lambda: s.secretion(False)),
+                                "bytes": A * w.S * (12 + 8 + (20 if w.compute_internalized else 0))}
+        kernels["secretion_rebin"] = {"ms": timed(lambda: s.secretion(True)), "bytes": None}
+        # a whole non-recompute step (graph replay) as configured by default (the Dirichlet scatters and
+        # the gradient kernel), then with the Dirichlet overwrites written by the sweeps, then with the
+        # gradient inside the z sweep as well
+        kernels["step"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
+        s.set_option("fused_dirichlet", 1)
+        kernels["step_fused_dirichlet"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
+        s.set_option("fused_gradient", 1)
+        kernels["step_fused_dirichlet_gradient"] = {"ms": timed(lambda: s.run_steps(1, 11)), "bytes": None}
+        s.set_option("fused_dirichlet", 0)
+        s.set_option("fused_gradient", 0)
+        s.synchronize()
+        peak, peak_kind = measured_peak()
+        for k in kernels.values():
+            k["gbs"] = (k["bytes"] / (k["ms"] / 1e3) / 1e9) if k["bytes"] else None
+        sweeps = [kernels[n] for n in names[:w.dims]]
+        sweep_ms = sum(k["ms"] for k in sweeps) / len(sweeps)
+        kernels["sweep_mean"] = {"ms": sweep_ms, "bytes": 8 * VS, "gbs": 8 * VS / (sweep_ms / 1e3) / 1e9}
+        traffic_rec = committed_traffic().get(args.workload, {})
+        # the dominant kernel: the sweep kernel (three launches per step, the largest share of the
+        # step's launch list); its achieved bandwidth is the per-launch algorithmic bytes over the mean
+        # launch time
+        roofline = {"bound": "hbm", "kernel": "sweep_tma_kernel (mean of the x, y, z launches)",
+                    "achieved": 8 * VS / (sweep_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                    "traffic": traffic_rec.get("sweep"), "peak_source": f"{peak_kind} hbm_gbs (copy)",
+                    "algorithmic_bytes_per_launch": 8 * VS, "ms_per_launch": sweep_ms}
+        roofline["frac"] = roofline["achieved"] / peak
     step_bytes = algorithmic_step_bytes(w)
     step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
     step_hbm = {"algorithmic_bytes": step_bytes, "achieved_gbs": step_gbs, "frac_of_measured": step_gbs / peak,
