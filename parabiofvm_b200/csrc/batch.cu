@@ -425,22 +425,21 @@ int bfvm_batch_autotune(bfvm_batch* b, int32_t* choices)
 			float best_ms = 0.f;
 			ens_tuning keep = best;
 			bool first = true;
-			for (int minb : { 2, 1 })
-				for (int split : { 1, 2, 4 })
+			static constexpr int sweep_choices[6][2] = { { 2, 1 }, { 2, 2 }, { 2, 4 }, { 1, 1 }, { 1, 2 }, { 1, 4 } };
+			for (int c = 0; c < 6 && !st; c++)
+			{
+				ens_tuning t = best;
+				t.sweep_minb[axis] = sweep_choices[c][0];
+				t.sweep_split[axis] = sweep_choices[c][1];
+				float ms = 0.f;
+				st = time_phase(t, [&](const ensemble_plan& p) { return ensemble_sweep(p, axis, b->stream); }, ms);
+				if (!st && (first || ms < best_ms))
 				{
-					ens_tuning t = best;
-					t.sweep_minb[axis] = minb;
-					t.sweep_split[axis] = split;
-					float ms = 0.f;
-					if ((st = time_phase(t, [&](const ensemble_plan& p) { return ensemble_sweep(p, axis, b->stream); }, ms)))
-						break;
-					if (first || ms < best_ms)
-					{
-						best_ms = ms;
-						keep = t;
-						first = false;
-					}
+					best_ms = ms;
+					keep = t;
+					first = false;
 				}
+			}
 			best = keep;
 		}
 		if (!st)
@@ -448,22 +447,21 @@ int bfvm_batch_autotune(bfvm_batch* b, int32_t* choices)
 			float best_ms = 0.f;
 			ens_tuning keep = best;
 			bool first = true;
-			for (int zc : { 64, 32, 128 })
-				for (int zu : { 8, 4 })
+			static constexpr int grad_choices[6][2] = { { 64, 8 }, { 64, 4 }, { 32, 8 }, { 32, 4 }, { 128, 8 }, { 128, 4 } };
+			for (int c = 0; c < 6 && !st; c++)
+			{
+				ens_tuning t = best;
+				t.grad_zc = grad_choices[c][0];
+				t.grad_zu = grad_choices[c][1];
+				float ms = 0.f;
+				st = time_phase(t, [&](const ensemble_plan& p) { return ensemble_gradient(p, b->stream); }, ms);
+				if (!st && (first || ms < best_ms))
 				{
-					ens_tuning t = best;
-					t.grad_zc = zc;
-					t.grad_zu = zu;
-					float ms = 0.f;
-					if ((st = time_phase(t, [&](const ensemble_plan& p) { return ensemble_gradient(p, b->stream); }, ms)))
-						break;
-					if (first || ms < best_ms)
-					{
-						best_ms = ms;
-						keep = t;
-						first = false;
-					}
+					best_ms = ms;
+					keep = t;
+					first = false;
 				}
+			}
 			best = keep;
 		}
 		cudaStreamSynchronize(b->stream);
