@@ -194,6 +194,8 @@ int bfvm_synchronize(bfvm_solver* s);
  * device error, src/solver/device/CUDA/device_context.h:12-21, with a bounded wait and a status):
  * - "tma_sweeps" 0/1 stages sweep tiles through shared memory with the TMA (default 1; 0 selects
  *   the kernels that read the field directly).  Results agree to rounding either way.
+ * - "tma_prefetch" 0/1: each staged-sweep refill also prefetches into L2 the tile after the one it
+ *   copies (default 0).  Results are identical either way.
  * - "fused_dirichlet" 0/1: in the LOD step (bfvm_diffusion_solve, bfvm_run_steps) a staged sweep
  *   writes the Dirichlet overwrite that follows it, tile by tile (default 0: the scatter kernel
  *   after the sweep, measured faster).  Results are identical either way.

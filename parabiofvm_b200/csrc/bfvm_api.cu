@@ -1063,6 +1063,8 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 	const std::string n(name);
 	if (n == "tma_sweeps")
 		s->use_tma = value != 0;
+	else if (n == "tma_prefetch")
+		s->tma_prefetch = value != 0;
 	else if (n == "fused_dirichlet")
 		s->dir_fused = value != 0;
 	else if (n == "fused_gradient")

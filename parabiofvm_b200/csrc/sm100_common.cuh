@@ -72,6 +72,27 @@ __device__ __forceinline__ void tma_load_2d_hint(float* dst, const CUtensorMap* 
 				 : "memory");
 }
 
+// Prefetches into L2 of a tensor-map box, or of a contiguous range (no shared memory, no barrier).
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int c0, int c1)
+{
+	asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+				 "r"(c0), "r"(c1)
+				 : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int c0, int c1, int c2)
+{
+	asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+					 reinterpret_cast<uint64_t>(map)),
+				 "r"(c0), "r"(c1), "r"(c2)
+				 : "memory");
+}
+
+__device__ __forceinline__ void bulk_prefetch(const void* src, uint32_t bytes)
+{
+	asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar)
 {
 	asm volatile(

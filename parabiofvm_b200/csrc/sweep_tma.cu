@@ -55,6 +55,8 @@ struct tma_tile
 	// z tiles read with an L2 evict-first policy, so that the planes the sweep writes (which the
 	// gradient inside it reads back) are the lines L2 keeps
 	int evict_first;
+	// with each refill, an L2 prefetch of the tile after it (option tma_prefetch)
+	int prefetch;
 };
 
 // Issue the copies of tile w into `dst`, completing on `bar` (one thread).  The line elements land
@@ -143,13 +145,38 @@ __host__ __device__ __forceinline__ int staged_table_floats(int P, int S)
 }
 
 // Copy tile wn (if it exists) into a stage whose previous contents every thread has read.
+// An L2 prefetch of tile w (no stage, no barrier): its reads start a tile earlier than its copy.
+__device__ __forceinline__ void prefetch_tile(const sweep_args& a, const CUtensorMap* map, const tma_tile& tt, long long w)
+{
+	if (w >= tt.items)
+		return;
+	if (tt.axis == 0)
+	{
+		const long long row0 = w * tt.R;
+		const int rows = (int)min((long long)tt.R, tt.nrows - row0);
+		bulk_prefetch(a.data + row0 * tt.XS, (uint32_t)(rows * tt.XS * sizeof(float)));
+		return;
+	}
+	const long long outer = w / tt.col_tiles;
+	const int c0 = (int)((w % tt.col_tiles) * 32);
+	for (int b = 0; b < tt.nbox; b++)
+	{
+		if (tt.axis == 1)
+			tma_prefetch_3d(map, c0, b * tt.box_h, (int)outer);
+		else
+			tma_prefetch_2d(map, c0, b * tt.box_h);
+	}
+}
+
 __device__ __forceinline__ void refill(const sweep_args& a, const CUtensorMap& map, const tma_tile& tt, long long wn,
-									   float* stage, uint64_t* bar)
+									   float* stage, uint64_t* bar, long long wstride)
 {
 	if (wn >= tt.items)
 		return;
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 	issue_tile(a, &map, tt, wn, stage, bar);
+	if (tt.prefetch)
+		prefetch_tile(a, &map, tt, wn + wstride);
 }
 
 // Barriers of one warp group (ids 1 + group; id 0 is the CTA-wide __syncthreads).
@@ -632,7 +659,7 @@ __global__ void __launch_bounds__(640, 1)
 		// consumed by the recurrences before the barrier): refill the stage with the tile NST
 		// ahead, so NST tiles stay in flight through the rest of this tile's solve
 		if (leader)
-			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st]);
+			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st], wstride);
 		// the barrier also ordered the previous tile's stores: its Dirichlet entries go on top
 		if (a.dir.items > 0 && it > 0)
 			dir_hold.store(a.dir, dir_prev, a.data, lane + 32 * j, gthr);
@@ -950,6 +977,7 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	}
 	tt.groups = G;
 	tt.stages = NST;
+	tt.prefetch = st->tma_prefetch ? 1 : 0;
 	const size_t smem = fixed_bytes(G) + (size_t)G * tt.stages * stage_bytes;
 
 	handled = true;
