@@ -203,6 +203,14 @@ int bfvm_synchronize(bfvm_solver* s);
  *   the gradient from the planes it has just written (default 0: the gradient kernel after the
  *   sweep, measured faster).  Results are identical either way.  "fused_gradient_evict_first" 0/1
  *   (default 1): that sweep reads its tiles with an L2 evict-first policy.
+ * - "face_dirichlet" 0/1: in the LOD step the staged sweeps write the Dirichlet face conditions by
+ *   position into the values they store (the reference's face order decides where faces meet), and
+ *   the scatter after each sweep keeps the interior elements alone (default 0: the scatter of every
+ *   conditioned element).  Taken only when no interior Dirichlet voxel lies on a conditioned face.
+ *   Results are identical either way.
+ * - "xy_band_planes" N, "zg_band_rows" N (default 0: off): the LOD step in bands that stay in L2
+ *   between two kernels: the x and y sweeps band by band of N z planes, the z sweep and the gradient
+ *   band by band of N y rows.  Results are identical either way; measured slower at 320^3 x 16.
  * - "wait_limit_cycles" bounds every wait of the staged sweeps on a tile copy, in GPU clock cycles
  *   (default 4e9, about two seconds; accepted range [1e4, 4e10]).  A wait that runs out makes the
  *   kernel give up its tile, let its copies in flight land and return; the next synchronising call

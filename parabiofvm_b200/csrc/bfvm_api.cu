@@ -1069,8 +1069,16 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 		s->dir_fused = value != 0;
 	else if (n == "fused_gradient")
 		s->grad_fused = value != 0;
+	else if (n == "face_dirichlet")
+		s->face_dirichlet = value != 0;
 	else if (n == "fused_gradient_evict_first")
 		s->grad_evict_first = value != 0;
+	else if (n == "xy_band_planes" || n == "zg_band_rows")
+	{
+		if (value < 0 || value > (1 << 20))
+			return fail(BFVM_ERR_INVALID_ARGUMENT, n + " must lie in [0, 2^20]");
+		(n == "xy_band_planes" ? s->xy_band_planes : s->zg_band_rows) = (int)value;
+	}
 	else if (n == "wait_limit_cycles")
 	{
 		if (value < 10000 || value > 40000000000LL)

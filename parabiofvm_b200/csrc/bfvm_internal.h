@@ -84,6 +84,18 @@ struct dirichlet_tiles
 	float* sval = nullptr;
 };
 
+// A Dirichlet overwrite list (dirichlet.cu): aligned runs of four consecutive elements (one float4
+// store each) and single elements, by element index.
+struct overwrite_list
+{
+	long long* qidx = nullptr;
+	float4* qval = nullptr;
+	long long qcount = 0;
+	long long* idx = nullptr;
+	float* val = nullptr;
+	long long count = 0;
+};
+
 struct agent_state
 {
 	int count = 0;
@@ -157,6 +169,15 @@ struct bfvm_solver
 	// the same list grouped by the tiles of each axis's staged sweep, which applies a tile's entries
 	// right after storing the tile (the overwrite that follows the sweep in the LOD step)
 	bfvm::dirichlet_tiles dir_tiles[3];
+	// The face conditions by position: when no interior Dirichlet voxel lies on a conditioned face,
+	// the staged sweeps of the LOD step write the face conditions themselves (the x sweep also right
+	// after its loads, for the overwrite before it) and the scatter takes the interior elements alone
+	bool face_pos_ok = false;
+	bool face_dirichlet = false;		  // option face_dirichlet (measured no faster than the scatter)
+	int* face_bits = nullptr;			  // [S]: bit f set when face f conditions the substrate
+	float* face_vals_d = nullptr;		  // [6][S]
+	unsigned char* face_tiles[3] = {};	  // per staged tile of each axis: a line lies on a face of another axis
+	bfvm::overwrite_list dir_interior;	  // the interior elements of the list
 
 	bfvm::agent_state ag;
 
@@ -177,6 +198,11 @@ struct bfvm_solver
 	bool dir_fused = false;		 // staged sweeps of the LOD step write the overwrite that follows them
 	bool grad_fused = false;	 // the z sweep of a step computes the gradient (sweep_tma.cu)
 	bool grad_evict_first = true; // ... reading its tiles with an L2 evict-first policy
+	// the LOD step in bands that stay in L2 between two kernels (0: whole-field launches): the x and
+	// y sweeps band by band of `xy_band_planes` z planes, the z sweep and the gradient band by band
+	// of `zg_band_rows` y rows (sweep.cu)
+	int xy_band_planes = 0;
+	int zg_band_rows = 0;
 	int* grad_tile_done = nullptr; // [z tiles] and [1 + z tiles] of the gradient inside the z sweep
 	int* grad_deferred = nullptr;
 	long long grad_tiles = 0;
@@ -261,12 +287,17 @@ bool cached_tuning(const bfvm_solver* s, int axis, sweep_tuning& out);
 // the solve pass of a slab solver's z sweep, with the carries in s->slab_carry
 int launch_slab_z(bfvm_solver* s);
 // dirichlet.cu
-int launch_dirichlet(bfvm_solver* s);
+int launch_dirichlet(bfvm_solver* s, bool interior_only = false);
+// the step's staged sweep of `axis` can write the face conditions (face_pos_ok and the option)
+bool faces_by_position(const bfvm_solver* s);
 int rebuild_dirichlet(bfvm_solver* s);
 void free_dirichlet(bfvm_solver* s);
 
 // gradient.cu
 int launch_gradient(bfvm_solver* s);
+// the 3D gradient of rows [y0, y1) of every plane, when substrates % 4 == 0 (false: not this shape)
+bool gradient_rows_possible(const bfvm_solver* s);
+int launch_gradient_rows(bfvm_solver* s, int y0, int y1);
 
 // bulk.cu
 int set_bulk_rates(bfvm_solver* s, int per_voxel, const float* supply, const float* uptake, const float* target);

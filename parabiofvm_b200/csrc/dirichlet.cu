@@ -13,6 +13,7 @@
 #include <cstring>
 
 #include "bfvm_internal.h"
+#include "sweep_common.cuh"
 
 namespace bfvm {
 
@@ -32,16 +33,31 @@ __global__ void __launch_bounds__(256) dirichlet_scatter_kernel(float* __restric
 	}
 }
 
-int launch_dirichlet(bfvm_solver* st)
+// interior_only: the interior elements alone, when the sweeps write the face conditions
+// (faces_by_position); otherwise every conditioned element
+int launch_dirichlet(bfvm_solver* st, bool interior_only)
 {
-	const long long n = st->dir_qcount + st->dir_count;
+	overwrite_list full;
+	full.qidx = st->dir_qidx;
+	full.qval = st->dir_qval;
+	full.qcount = st->dir_qcount;
+	full.idx = st->dir_idx;
+	full.val = st->dir_val;
+	full.count = st->dir_count;
+	const overwrite_list& l = interior_only && st->face_pos_ok ? st->dir_interior : full;
+	const long long n = l.qcount + l.count;
 	if (n == 0)
 		return BFVM_OK;
 	const int threads = 256;
 	const long long blocks = std::min<long long>((n + threads - 1) / threads, 148LL * 16);
-	dirichlet_scatter_kernel<<<(unsigned)blocks, threads, 0, st->stream>>>(
-		st->dens, st->dir_qidx, st->dir_qval, st->dir_qcount, st->dir_idx, st->dir_val, st->dir_count);
+	dirichlet_scatter_kernel<<<(unsigned)blocks, threads, 0, st->stream>>>(st->dens, l.qidx, l.qval, l.qcount, l.idx,
+																		   l.val, l.count);
 	return check_launch(st, "dirichlet_scatter_kernel");
+}
+
+bool faces_by_position(const bfvm_solver* s)
+{
+	return s->face_pos_ok && s->face_dirichlet && !s->dir_fused && s->slab_count == 1;
 }
 
 static void free_tiles(dirichlet_tiles& t)
@@ -65,27 +81,135 @@ void free_dirichlet(bfvm_solver* s)
 	s->dir_count = 0;
 	for (auto& t : s->dir_tiles)
 		free_tiles(t);
+	s->face_pos_ok = false;
+	device_free(s->face_bits);
+	device_free(s->face_vals_d);
+	for (auto& t : s->face_tiles)
+		device_free(t);
+	overwrite_list& l = s->dir_interior;
+	device_free(l.qidx);
+	device_free(l.qval);
+	device_free(l.idx);
+	device_free(l.val);
+	l = overwrite_list();
 }
 
-// The tiles of the staged sweep along `axis` (sweep_tma.cu): x, R = 32 / S whole rows; y, 32
-// columns of the x*s plane of one z plane; z, 32 columns of the y*x*s plane.  Returns the tile
-// count (0 when the staged sweep cannot take the axis) and sets tile(e) for element e.
-struct staged_tiling
+// Elements sorted by index, split into aligned runs of four consecutive elements and the rest.
+struct split_list
 {
-	int axis = 0;
-	long long XS = 0, YXS = 0, R = 1, col_tiles = 0, items = 0;
-
-	long long tile(long long e) const
-	{
-		if (axis == 0)
-			return (e / XS) / R;
-		if (axis == 1)
-			return (e / YXS) * col_tiles + (e % XS) / 32;
-		return (e % YXS) / 32;
-	}
+	std::vector<long long> qidx, sidx;
+	std::vector<float4> qval;
+	std::vector<float> sval;
 };
 
-static staged_tiling staged_tiles(const bfvm_solver* s, int axis)
+static split_list split_runs(const std::vector<long long>& idx, const std::vector<float>& val)
+{
+	std::vector<size_t> order(idx.size());
+	for (size_t k = 0; k < order.size(); k++)
+		order[k] = k;
+	std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return idx[a] < idx[b]; });
+	split_list r;
+	for (size_t k = 0; k < order.size();)
+	{
+		const long long e = idx[order[k]];
+		if (e % 4 == 0 && k + 3 < order.size() && idx[order[k + 3]] == e + 3)
+		{
+			r.qidx.push_back(e);
+			r.qval.push_back(make_float4(val[order[k]], val[order[k + 1]], val[order[k + 2]], val[order[k + 3]]));
+			k += 4;
+		}
+		else
+		{
+			r.sidx.push_back(e);
+			r.sval.push_back(val[order[k]]);
+			k++;
+		}
+	}
+	return r;
+}
+
+template <typename T>
+static int upload(T** dst, const std::vector<T>& v)
+{
+	int st = device_alloc(dst, v.size());
+	if (st || v.empty())
+		return st;
+	BFVM_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+	return BFVM_OK;
+}
+
+// The face conditions by position (face_pos_ok): the per-substrate face bits and values, the
+// interior elements as their own list, and per staged tile of each axis whether a line of the tile
+// lies on a conditioned face of another axis.
+static int build_face_tables(bfvm_solver* s, const std::vector<long long>& iidx, const std::vector<float>& ival)
+{
+	const int S = s->S;
+	const long long X = s->grid[0], Y = s->grid[1], Z = s->grid[2];
+	std::vector<int> bits(S, 0);
+	std::vector<float> vals((size_t)6 * S, 0.f);
+	for (int f = 0; f < 6; f++)
+		for (int k = 0; k < S; k++)
+			if (((s->face_mask >> f) & 1) && s->face_conds_h[(size_t)f * S + k])
+			{
+				bits[k] |= 1 << f;
+				vals[(size_t)f * S + k] = s->face_vals_h[(size_t)f * S + k];
+			}
+	int st;
+	if ((st = upload(&s->face_bits, bits)) || (st = upload(&s->face_vals_d, vals)))
+		return st;
+	const split_list r = split_runs(iidx, ival);
+	overwrite_list& l = s->dir_interior;
+	if ((st = upload(&l.qidx, r.qidx)) || (st = upload(&l.qval, r.qval)) || (st = upload(&l.idx, r.sidx))
+		|| (st = upload(&l.val, r.sval)))
+		return st;
+	l.qcount = (long long)r.qidx.size();
+	l.count = (long long)r.sidx.size();
+	auto on = [&](int f) { return ((s->face_mask >> f) & 1) != 0; };
+	for (int axis = 0; axis < s->dims; axis++)
+	{
+		const staged_tiling tl = staged_tiles(s, axis);
+		if (tl.items == 0)
+			continue;
+		std::vector<unsigned char> t(tl.items, 0);
+		const long long XS = tl.XS;
+		if (axis == 0)
+		{
+			// rows (y, z) on a y or z face
+			for (long long z = 0; z < Z; z++)
+				for (long long y = 0; y < Y; y++)
+					if ((y == 0 && on(2)) || (y == Y - 1 && on(3)) || (z == 0 && on(4)) || (z == Z - 1 && on(5)))
+						t[(z * Y + y) / tl.R] = 1;
+		}
+		else if (axis == 1)
+		{
+			// columns (x, s) of a plane on an x face, and every column of a z-face plane
+			for (long long z = 0; z < Z; z++)
+				for (long long q = 0; q < XS; q++)
+				{
+					const long long x = q / S;
+					if ((x == 0 && on(0)) || (x == X - 1 && on(1)) || (z == 0 && on(4)) || (z == Z - 1 && on(5)))
+						t[z * tl.col_tiles + q / 32] = 1;
+				}
+		}
+		else
+		{
+			// columns (y, x, s) on an x or y face
+			for (long long y = 0; y < Y; y++)
+				for (long long q = 0; q < XS; q++)
+				{
+					const long long x = q / S;
+					if ((x == 0 && on(0)) || (x == X - 1 && on(1)) || (y == 0 && on(2)) || (y == Y - 1 && on(3)))
+						t[(y * XS + q) / 32] = 1;
+				}
+		}
+		if ((st = upload(&s->face_tiles[axis], t)))
+			return st;
+	}
+	s->face_pos_ok = true;
+	return BFVM_OK;
+}
+
+staged_tiling staged_tiles(const bfvm_solver* s, int axis)
 {
 	staged_tiling t;
 	t.axis = axis;
@@ -203,6 +327,9 @@ int rebuild_dirichlet(bfvm_solver* s)
 	idx.reserve(face_vox.size() * S + s->int_vids_h.size() * S);
 	val.reserve(idx.capacity());
 	const auto& iv = s->int_vids_h;
+	// the face conditions can be written by position only if no interior voxel lies on a
+	// conditioned face (then the interior list never meets a face element)
+	bool by_position = s->face_mask != 0;
 	for (long long vid : face_vox)
 	{
 		const long long c[3] = { vid % X, (vid / X) % Y, vid / (X * Y) };
@@ -236,42 +363,31 @@ int rebuild_dirichlet(bfvm_solver* s)
 			}
 		}
 	}
+	std::vector<long long> iidx;
+	std::vector<float> ival;
 	for (size_t r = 0; r < iv.size(); r++)
 	{
 		if (std::binary_search(face_vox.begin(), face_vox.end(), iv[r]))
+		{
+			by_position = false;
 			continue; // resolved with the faces
+		}
 		for (int k = 0; k < S; k++)
 			if (s->int_conds_h[r * S + k])
 			{
 				idx.push_back(iv[r] * S + k);
 				val.push_back(s->int_vals_h[r * S + k]);
+				iidx.push_back(iv[r] * S + k);
+				ival.push_back(s->int_vals_h[r * S + k]);
 			}
 	}
 
 	// aligned runs of four consecutive elements, and the rest one by one
-	std::vector<size_t> order(idx.size());
-	for (size_t k = 0; k < order.size(); k++)
-		order[k] = k;
-	std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return idx[a] < idx[b]; });
-	std::vector<long long> qidx, sidx;
-	std::vector<float4> qval;
-	std::vector<float> sval;
-	for (size_t k = 0; k < order.size();)
-	{
-		const long long e = idx[order[k]];
-		if (e % 4 == 0 && k + 3 < order.size() && idx[order[k + 3]] == e + 3)
-		{
-			qidx.push_back(e);
-			qval.push_back(make_float4(val[order[k]], val[order[k + 1]], val[order[k + 2]], val[order[k + 3]]));
-			k += 4;
-		}
-		else
-		{
-			sidx.push_back(e);
-			sval.push_back(val[order[k]]);
-			k++;
-		}
-	}
+	const split_list runs = split_runs(idx, val);
+	const std::vector<long long>& qidx = runs.qidx;
+	const std::vector<float4>& qval = runs.qval;
+	const std::vector<long long>& sidx = runs.sidx;
+	const std::vector<float>& sval = runs.sval;
 
 	free_dirichlet(s);
 	int st;
@@ -295,7 +411,9 @@ int rebuild_dirichlet(bfvm_solver* s)
 	s->dir_count = (long long)sidx.size();
 	if (s->slab_count > 1 || qidx.size() + sidx.size() == 0)
 		return BFVM_OK; // slabs step axis by axis through the unfused calls
-	const int st2 = build_tile_lists(s, qidx, qval, sidx, sval);
+	int st2 = build_tile_lists(s, qidx, qval, sidx, sval);
+	if (!st2 && by_position)
+		st2 = build_face_tables(s, iidx, ival);
 	if (st2)
 		free_dirichlet(s);
 	return st2;

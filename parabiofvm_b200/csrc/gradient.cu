@@ -67,13 +67,13 @@ __device__ __forceinline__ float4 f4sub_mul(float4 a, float4 b, float f)
 
 __global__ void __launch_bounds__(256) gradient3d_vec4_kernel(const float4* __restrict__ u, float4* __restrict__ g,
 															   long long total4, int S4, int X, int Y, int Z, float bx,
-															   float cx, float by, float cy, float bz, float cz)
+															   float cx, float by, float cy, float bz, float cz, int y0)
 {
 	const int XS4 = X * S4;
 	const int q4 = blockIdx.x * blockDim.x + threadIdx.x;
 	if (q4 >= XS4)
 		return;
-	const int y = blockIdx.y;
+	const int y = y0 + blockIdx.y;
 	const int z0 = blockIdx.z * GRAD_ZC;
 	const int z1 = min(Z, z0 + GRAD_ZC);
 	const int x = q4 / S4;
@@ -117,26 +117,46 @@ __global__ void __launch_bounds__(256) gradient3d_vec4_kernel(const float4* __re
 	}
 }
 
-int launch_gradient(bfvm_solver* st)
+static void gradient_factors(const bfvm_solver* st, float (&f)[6])
 {
-	const long long total = st->V * st->S;
-	float f[6] = { 0, 0, 0, 0, 0, 0 };
+	for (int d = 0; d < 6; d++)
+		f[d] = 0.f;
 	for (int d = 0; d < st->dims; d++)
 	{
 		f[2 * d] = 1.f / st->voxel[d];
 		f[2 * d + 1] = 1.f / (st->voxel[d] * 2);
 	}
+}
+
+bool gradient_rows_possible(const bfvm_solver* st) { return st->dims == 3 && st->S % 4 == 0; }
+
+int launch_gradient_rows(bfvm_solver* st, int y0, int y1)
+{
+	if (!gradient_rows_possible(st) || y0 < 0 || y1 > st->grid[1] || y0 > y1)
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "gradient rows outside the mesh or not a 3D mesh of 4k substrates");
+	if (y0 == y1)
+		return BFVM_OK;
+	float f[6];
+	gradient_factors(st, f);
 	const int threads = 256;
 	const int S = st->S, X = st->grid[0], Y = st->grid[1], Z = st->grid[2];
-	if (st->dims == 3 && S % 4 == 0)
-	{
-		const int XS4 = X * (S / 4);
-		const dim3 blocks((unsigned)((XS4 + threads - 1) / threads), (unsigned)Y, (unsigned)((Z + GRAD_ZC - 1) / GRAD_ZC));
-		gradient3d_vec4_kernel<<<blocks, threads, 0, st->stream>>>(
-			reinterpret_cast<const float4*>(st->dens), reinterpret_cast<float4*>(st->grad), total / 4, S / 4, X, Y, Z, f[0],
-			f[1], f[2], f[3], f[4], f[5]);
-		return check_launch(st, "gradient3d_vec4_kernel");
-	}
+	const int XS4 = X * (S / 4);
+	const dim3 blocks((unsigned)((XS4 + threads - 1) / threads), (unsigned)(y1 - y0), (unsigned)((Z + GRAD_ZC - 1) / GRAD_ZC));
+	gradient3d_vec4_kernel<<<blocks, threads, 0, st->stream>>>(reinterpret_cast<const float4*>(st->dens),
+															   reinterpret_cast<float4*>(st->grad), st->V * S / 4, S / 4,
+															   X, Y, Z, f[0], f[1], f[2], f[3], f[4], f[5], y0);
+	return check_launch(st, "gradient3d_vec4_kernel");
+}
+
+int launch_gradient(bfvm_solver* st)
+{
+	const long long total = st->V * st->S;
+	float f[6];
+	gradient_factors(st, f);
+	const int threads = 256;
+	const int S = st->S, X = st->grid[0], Y = st->grid[1], Z = st->grid[2];
+	if (gradient_rows_possible(st))
+		return launch_gradient_rows(st, 0, Y);
 	const dim3 blocks((unsigned)((X * S + threads - 1) / threads), (unsigned)Y, (unsigned)Z);
 	if (st->dims == 1)
 		gradient_kernel<1><<<blocks, threads, 0, st->stream>>>(st->dens, st->grad, total, S, X, Y, Z, f[0], f[1], f[2],

@@ -209,6 +209,10 @@ static sweep_args make_args(bfvm_solver* st, int axis)
 	a.wait_limit = st->wait_limit_cycles;
 	a.drop_tile_copy = st->drop_tile_copy;
 	a.dir = dirichlet_tiles();
+	a.face_apply = 0;
+	a.face_bits = st->face_bits;
+	a.face_vals = st->face_vals_d;
+	a.face_tiles = st->face_tiles[axis];
 	return a;
 }
 
@@ -309,6 +313,85 @@ int grad_fuse_buffers(bfvm_solver* st)
 	return BFVM_OK;
 }
 
+// The band modes of the step.  A band is a slab of the field small enough to stay in L2 between two
+// kernels: the kernel after the first reads the band back from L2 instead of HBM.  The arithmetic of
+// every element is the same as in whole-field launches (each tile is swept by the same code), so
+// results are identical; only the order of tiles changes.  The Dirichlet overwrites between the
+// sweeps come from the per-tile lists, written by the sweep of each tile, so the band modes need them
+// wherever the mesh has Dirichlet nodes.
+static bool band_overwrites_ready(const bfvm_solver* st, int axis)
+{
+	return st->dir_qcount + st->dir_count == 0 || st->dir_tiles[axis].items > 0;
+}
+
+// x then y sweep per band of `xy_band_planes` z planes: a band's y sweep reads what its x sweep
+// wrote.  Needs whole x tiles per plane (rows % (32 / S) == 0).  *done: the band mode ran.
+static int banded_xy(bfvm_solver* st, bool& done)
+{
+	done = false;
+	const long long c = st->xy_band_planes;
+	if (c <= 0 || st->dims != 3 || !st->use_tma || c >= st->grid[2])
+		return BFVM_OK;
+	const staged_tiling tx = staged_tiles(st, 0), ty = staged_tiles(st, 1);
+	const long long Y = st->grid[1], Z = st->grid[2];
+	if (tx.items == 0 || ty.items == 0 || Y % tx.R != 0 || !band_overwrites_ready(st, 0) || !band_overwrites_ready(st, 1)
+		|| staged_sweep_shapes(st, 0).empty() || staged_sweep_shapes(st, 1).empty())
+		return BFVM_OK;
+	sweep_args ax = make_args(st, 0), ay = make_args(st, 1);
+	ax.dir = st->dir_tiles[0];
+	ay.dir = st->dir_tiles[1];
+	for (long long z0 = 0; z0 < Z; z0 += c)
+	{
+		const long long z1 = std::min(Z, z0 + c);
+		bool hx = false, hy = false;
+		int rc = launch_sweep_tma(st, 0, ax, hx, &st->tune[0], nullptr, false, nullptr, z0 * Y / tx.R, z1 * Y / tx.R);
+		if (!rc)
+			rc = launch_sweep_tma(st, 1, ay, hy, &st->tune[1], nullptr, false, nullptr, z0 * ty.col_tiles,
+								  z1 * ty.col_tiles);
+		if (!rc && !(hx && hy))
+			rc = fail(BFVM_ERR_STATE, "a band of the x and y sweeps was not staged");
+		if (rc)
+			return rc;
+	}
+	done = true;
+	return BFVM_OK;
+}
+
+// z sweep then gradient per band of `zg_band_rows` y rows: after the z sweep of rows [0, y1) the
+// gradient of rows [.., y1 - 1) has every neighbour final (row y reads y - 1 and y + 1).  Needs
+// whole z tiles per row (x * substrates % 32 == 0) and the row-range gradient kernel.
+static int banded_zgrad(bfvm_solver* st, bool& done)
+{
+	done = false;
+	const long long c = st->zg_band_rows;
+	if (c <= 0 || st->dims != 3 || !st->use_tma || c >= st->grid[1] || !gradient_rows_possible(st))
+		return BFVM_OK;
+	const staged_tiling tz = staged_tiles(st, 2);
+	const long long Y = st->grid[1], XS = tz.XS;
+	if (tz.items == 0 || XS % 32 != 0 || !band_overwrites_ready(st, 2) || staged_sweep_shapes(st, 2).empty())
+		return BFVM_OK;
+	sweep_args az = make_args(st, 2);
+	az.dir = st->dir_tiles[2];
+	const long long row_tiles = XS / 32;
+	long long g0 = 0;
+	for (long long y0 = 0; y0 < Y; y0 += c)
+	{
+		const long long y1 = std::min(Y, y0 + c);
+		bool hz = false;
+		int rc = launch_sweep_tma(st, 2, az, hz, &st->tune[2], nullptr, false, nullptr, y0 * row_tiles, y1 * row_tiles);
+		if (!rc && !hz)
+			rc = fail(BFVM_ERR_STATE, "a band of the z sweep was not staged");
+		const long long g1 = y1 == Y ? Y : y1 - 1;
+		if (!rc)
+			rc = launch_gradient_rows(st, (int)g0, (int)g1);
+		if (rc)
+			return rc;
+		g0 = g1;
+	}
+	done = true;
+	return BFVM_OK;
+}
+
 // The whole LOD step (src/solver/host/diffusion_solver.cpp:512-544): overwrite, then per axis the
 // sweep and the overwrite after it.  A staged sweep writes that overwrite itself, tile by tile
 // right after storing the tile, from the list grouped by its tiles; other sweeps are followed by
@@ -317,14 +400,39 @@ int launch_diffusion(bfvm_solver* st, bool gradient, bool* gradient_done)
 {
 	if (gradient_done)
 		*gradient_done = false;
-	// the first overwrite stays a scatter: inside the x sweep it would have to reach the staged
-	// tile before any thread reads it, with the entries' load latency on every tile's path
+	// the face conditions by position: each staged sweep writes them into the values it stores, and
+	// the scatter after it keeps the interior elements alone.  An axis whose sweep is not staged is
+	// followed by the whole list.
+	const bool faces = faces_by_position(st) && st->xy_band_planes == 0 && st->zg_band_rows == 0;
+	// the first overwrite stays a scatter of the whole list: inside the x sweep it would have to
+	// reach the values before the recurrences, where the kernel has no registers to spare
 	int rc = launch_dirichlet(st);
-	for (int axis = 0; axis < st->dims && !rc; axis++)
+	int axis = 0;
+	if (!rc)
 	{
+		bool banded = false;
+		rc = banded_xy(st, banded);
+		if (banded)
+			axis = 2;
+	}
+	for (; axis < st->dims && !rc; axis++)
+	{
+		if (axis == 2 && gradient && gradient_done && !st->grad_fused && st->batch_refs == 0 && st->slab_count == 1)
+		{
+			bool banded = false;
+			if ((rc = banded_zgrad(st, banded)))
+				return rc;
+			if (banded)
+			{
+				*gradient_done = true;
+				break;
+			}
+		}
 		sweep_args a = make_args(st, axis);
 		if (st->dir_fused)
 			a.dir = st->dir_tiles[axis];
+		if (faces)
+			a.face_apply = 1;
 		// the gradient inside the z sweep needs the final field there: no overwrite after it, or
 		// the overwrite written by the sweep itself
 		const bool overwrite_after = st->dir_qcount + st->dir_count > 0;
@@ -360,7 +468,7 @@ int launch_diffusion(bfvm_solver* st, bool gradient, bool* gradient_done)
 		if (!rc && fuse_grad && staged && gradient_done)
 			*gradient_done = true;
 		if (!rc && !(staged && a.dir.items > 0))
-			rc = launch_dirichlet(st);
+			rc = launch_dirichlet(st, staged && faces);
 	}
 	return rc;
 }

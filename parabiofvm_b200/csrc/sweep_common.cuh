@@ -33,6 +33,13 @@ struct sweep_args
 	// staged sweeps of the LOD step: the Dirichlet overwrite that follows this sweep, grouped by its
 	// tiles; each tile's entries are written right after the tile (items 0: no overwrite here)
 	dirichlet_tiles dir;
+	// staged sweeps of the LOD step: nonzero to write the Dirichlet face conditions by position into
+	// the stored values (the faces of the overwrite after this sweep).  face_bits [S], face_vals
+	// [6][S], face_tiles: per tile, whether a line of the tile lies on a face of another axis
+	int face_apply;
+	const int* face_bits;
+	const float* face_vals;
+	const unsigned char* face_tiles;
 };
 
 __device__ __forceinline__ void block_range(int j, int base_len, int extra, int& p, int& L)
@@ -217,8 +224,31 @@ struct grad_fuse
 
 // slab_solve (z axis only): the solve pass of a z-slab's sweep.  gf (z axis only): compute the
 // gradient inside the sweep; `handled` then also means the gradient is (being) computed.
+// [w_begin, w_end): sweep only these tiles (w_end -1: to the last tile; not with gf or slab_solve).
+// The launch shape is the one chosen for the whole field.
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled,
 					 const sweep_tuning* tune = nullptr, std::vector<sweep_tuning>* shapes = nullptr,
-					 bool slab_solve = false, const grad_fuse* gf = nullptr);
+					 bool slab_solve = false, const grad_fuse* gf = nullptr, long long w_begin = 0,
+					 long long w_end = -1);
+
+// The tiles of the staged sweep along `axis` (sweep_tma.cu and the Dirichlet tile lists): x,
+// R = 32 / S whole rows; y, 32 columns of the x*s plane of one z plane; z, 32 columns of the y*x*s
+// plane.  items is 0 when the staged sweep cannot take the axis.
+struct staged_tiling
+{
+	int axis = 0;
+	long long XS = 0, YXS = 0, R = 1, col_tiles = 0, items = 0;
+
+	long long tile(long long e) const
+	{
+		if (axis == 0)
+			return (e / XS) / R;
+		if (axis == 1)
+			return (e / YXS) * col_tiles + (e % XS) / 32;
+		return (e % YXS) / 32;
+	}
+};
+
+staged_tiling staged_tiles(const bfvm_solver* s, int axis);
 
 } // namespace bfvm

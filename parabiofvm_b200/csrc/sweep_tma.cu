@@ -38,7 +38,8 @@ namespace bfvm {
 struct tma_tile
 {
 	int axis;			 // 0 x (rows), 1 y, 2 z
-	long long items;	 // tiles
+	long long items;	 // tiles: this launch sweeps [first, items)
+	long long first;
 	long long ncols;	 // columns of the plane (y, z)
 	long long col_tiles; // 32-column tiles per plane (y, z)
 	long long outer_stride, line_stride;
@@ -263,6 +264,90 @@ struct dir_regs
 			data[__ldg(&d.sidx[e])] = __ldg(&d.sval[e]);
 	}
 };
+
+// The Dirichlet face conditions of one line, by its position (sweep_args::face_apply).  The
+// reference writes the faces in the order x-min, x-max, y-min, y-max, z-min, z-max, a later face
+// winning where faces meet.  A line along axis a meets the faces of a at its two ends (elements 0
+// and n - 1) and lies wholly on a face of another axis or not at all; those faces order before a's
+// faces or after them (which then also win at the ends).  The result is packed into one register,
+// which the sweep holds through the solve: bits 0-1 the line's kind (0 on no conditioned face of
+// another axis, 1 on one ordered before a's, 2 after), bits 2-3 whether a's min and max faces
+// condition the substrate, bits 4-6 the face whose value the line takes.
+template <bool ROWS>
+__device__ __forceinline__ int face_code(const sweep_args& a, const tma_tile& tt, long long w, int lane, int s,
+									 bool face_tile)
+{
+	const int m = __ldg(&a.face_bits[s]);
+	const int ax = ROWS ? 0 : tt.axis;
+	int code = ((m >> (2 * ax)) & 3) << 2;
+	if (m == 0 || !face_tile)
+		return code;
+	long long c[3] = { 0, 0, 0 };
+	if (ROWS)
+	{
+		const long long row = w * tt.R + lane / a.S;
+		c[1] = row % a.Y;
+		c[2] = row / a.Y;
+	}
+	else if (ax == 1)
+	{
+		const long long q = (w % tt.col_tiles) * 32 + lane;
+		c[0] = q / a.S;
+		c[2] = w / tt.col_tiles;
+	}
+	else
+	{
+		const long long q = w * 32 + lane;
+		c[1] = q / tt.XS;
+		c[0] = (q % tt.XS) / a.S;
+	}
+	const long long n[3] = { a.X, a.Y, a.Z };
+	int lb = 0;
+#pragma unroll
+	for (int b = 0; b < 3; b++)
+		if (b != ax)
+			lb |= (c[b] == 0 ? 1 << (2 * b) : 0) | (c[b] == n[b] - 1 ? 2 << (2 * b) : 0);
+	lb &= m;
+	const int after = lb >> (2 * ax + 2), before = lb & ((1 << (2 * ax)) - 1);
+	if (after)
+		code |= 2 | ((31 - __clz(after) + 2 * ax + 2) << 4);
+	else if (before)
+		code |= 1 | ((31 - __clz(before)) << 4);
+	return code;
+}
+
+// Write the face conditions of `code` into block j of the line (virtual elements 32j .. 32j + 31;
+// real element 0 is virtual element pad of block 0, element n - 1 the last of block P - 1).
+template <int M>
+__device__ __forceinline__ void apply_faces(float (&d)[M], int code, const sweep_args& a, int axis, int s, int j,
+											int P)
+{
+	if (code == 0)
+		return;
+	const int line = code & 3;
+	if (line != 0)
+	{
+		const float lv = __ldg(&a.face_vals[(code >> 4) * a.S + s]);
+#pragma unroll
+		for (int k = 0; k < M; k++)
+			d[k] = lv;
+		if (line == 2)
+			return;
+	}
+	if ((code & 4) && j == 0)
+	{
+		// element pad of the block, by a select per element: an indexed store would move the
+		// block out of registers
+		const float v = __ldg(&a.face_vals[(2 * axis) * a.S + s]);
+#pragma unroll
+		for (int k = 0; k < M; k++)
+			asm("{\n\t.reg .pred p;\n\tsetp.eq.s32 p, %1, %2;\n\tselp.f32 %0, %3, %0, p;\n}"
+				: "+f"(d[k])
+				: "r"(k), "r"(a.pad), "f"(v));
+	}
+	if ((code & 8) && j == P - 1)
+		d[M - 1] = __ldg(&a.face_vals[(2 * axis + 1) * a.S + s]);
+}
 
 // ------------------------------------------------------------------------------------------------
 // the gradient inside the z sweep (grad_fuse in sweep_common.cuh)
@@ -513,7 +598,7 @@ __global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constan
 // X instead of zero, with the tables of precompute_padded_range.
 // GRAD (z sweep, P > 1): the gradient of the step inside the sweep (grad_fuse); 1 the scalar form,
 // 4 the four-substrate form (S % 4 == 0).
-template <bool ROWS, bool NOALLOC, int SLAB, int GRAD>
+template <bool ROWS, bool NOALLOC, int SLAB, int GRAD, bool DIR>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt, const __grid_constant__ grad_fuse gf)
@@ -580,7 +665,7 @@ __global__ void __launch_bounds__(640, 1)
 	__syncthreads(); // also publishes the barrier init
 
 	// tiles of this group: w0, w0 + stride, ...
-	const long long w0 = (long long)blockIdx.x * G + g;
+	const long long w0 = tt.first + (long long)blockIdx.x * G + g;
 	const long long wstride = (long long)gridDim.x * G;
 
 	// prologue: the first NST tiles of this group, one per stage
@@ -603,12 +688,13 @@ __global__ void __launch_bounds__(640, 1)
 	// their list offsets, loaded an iteration before the entries, and the entries themselves
 	int dir_prev[4] = { 0, 0, 0, 0 };
 	dir_regs dir_hold;
+	int face_tile_next = (SLAB == 0 && GRAD == 0 && !DIR && a.face_apply && w < tt.items) ? __ldg(&a.face_tiles[w]) : 0;
 	for (; w < tt.items; w += wstride, it++)
 	{
 		const int st = it % NST;
 		const uint32_t parity = (uint32_t)((it / NST) & 1);
 		int dir_cur[4] = { 0, 0, 0, 0 };
-		if (a.dir.items > 0)
+		if (DIR && a.dir.items > 0)
 		{
 			if (it > 0)
 				dir_hold.load(a.dir, dir_prev, lane + 32 * j);
@@ -626,6 +712,17 @@ __global__ void __launch_bounds__(640, 1)
 			s = tl.s;
 			sbase = tl.sbase;
 			sstride = ROWS ? tl.sstride : 32;
+		}
+		// the line's face conditions, looked up while the tile's copy is in flight (the plain
+		// sweeps of the step only)
+		constexpr bool FACES = SLAB == 0 && GRAD == 0 && !DIR;
+		// (face_tiles[w] was loaded a tile ahead, so its latency hides behind the previous tile)
+		int faces = 0;
+		if (FACES && a.face_apply)
+		{
+			const bool ftile = face_tile_next != 0;
+			face_tile_next = w + wstride < tt.items ? __ldg(&a.face_tiles[w + wstride]) : 0;
+			faces = face_code<ROWS>(a, tt, w, lane, s, ftile);
 		}
 		const bool ok = mbar_wait(&bars[st], parity, a.wait_limit);
 
@@ -661,7 +758,7 @@ __global__ void __launch_bounds__(640, 1)
 		if (leader)
 			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st], wstride);
 		// the barrier also ordered the previous tile's stores: its Dirichlet entries go on top
-		if (a.dir.items > 0 && it > 0)
+		if (DIR && a.dir.items > 0 && it > 0)
 			dir_hold.store(a.dir, dir_prev, a.data, lane + 32 * j, gthr);
 
 		if (SLAB != 0)
@@ -725,6 +822,8 @@ __global__ void __launch_bounds__(640, 1)
 			}
 		}
 
+		if (FACES && a.face_apply) // the overwrite after this sweep
+			apply_faces(d, faces, a, ROWS ? 0 : tt.axis, s, j, P);
 		{
 			// recompute the line from an opaque copy of the tile index, so nothing of the load
 			// phase stays live across the solve
@@ -765,7 +864,7 @@ __global__ void __launch_bounds__(640, 1)
 			dir_prev[k] = dir_cur[k];
 	}
 
-	if (!failed && a.dir.items > 0 && it > 0)
+	if (DIR && !failed && a.dir.items > 0 && it > 0)
 	{
 		group_sync(bar_id, gthr); // the last tile's stores, then its entries
 		overwrite_tile(a.dir, a.data, w - wstride, lane + 32 * j, gthr);
@@ -820,16 +919,17 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 
 static constexpr int TMA_MAX_P = 16;
 
-template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0>
+template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0, bool DIR = false>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem, const grad_fuse* gfp = nullptr)
 {
-	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD>;
+	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD, DIR>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
 	const int threads = 32 * a.vP * tt.groups;
-	const int grid = persistent_grid(kernel, threads, smem, (tt.items + tt.groups - 1) / tt.groups, st->device);
+	const int grid =
+		persistent_grid(kernel, threads, smem, (tt.items - tt.first + tt.groups - 1) / tt.groups, st->device);
 	grad_fuse gf;
 	std::memset(&gf, 0, sizeof(gf));
 	if (GRAD)
@@ -855,10 +955,13 @@ static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtens
 // tune: launch shape to use (groups 0: the built-in choice).  shapes: when given, nothing is
 // launched; the launch shapes that fit are listed instead.
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled, const sweep_tuning* tune,
-					 std::vector<sweep_tuning>* shapes, bool slab_solve, const grad_fuse* gf)
+					 std::vector<sweep_tuning>* shapes, bool slab_solve, const grad_fuse* gf, long long w_begin,
+					 long long w_end)
 {
 	if (slab_solve && axis != 2)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab passes exist for the z sweep only");
+	if ((w_begin != 0 || w_end >= 0) && (slab_solve || gf))
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "a range of tiles is swept only by the plain staged sweeps");
 	handled = false;
 	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2], S = st->S;
 	const long long XS = X * S;
@@ -979,25 +1082,43 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	tt.stages = NST;
 	tt.prefetch = st->tma_prefetch ? 1 : 0;
 	const size_t smem = fixed_bytes(G) + (size_t)G * tt.stages * stage_bytes;
+	if (w_end >= 0 || w_begin != 0)
+	{
+		if (w_end < 0)
+			w_end = tt.items;
+		if (w_begin < 0 || w_end > tt.items || w_begin > w_end)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "tile range outside the sweep");
+		handled = true;
+		if (w_begin == w_end)
+			return BFVM_OK;
+		tt.first = w_begin;
+		tt.items = w_end;
+	}
 
 	handled = true;
+	// the kernels that write Dirichlet lists per tile are separate instances, so the default ones
+	// keep those registers for the solve
+	const bool dir = a.dir.items > 0;
 	if (axis == 0)
-		return launch_tma_variant<true, true>(st, a, map, tt, smem);
+		return dir ? launch_tma_variant<true, true, 0, 0, true>(st, a, map, tt, smem)
+				   : launch_tma_variant<true, true>(st, a, map, tt, smem);
 	if (axis == 1)
-		return launch_tma_variant<false, true>(st, a, map, tt, smem);
+		return dir ? launch_tma_variant<false, true, 0, 0, true>(st, a, map, tt, smem)
+				   : launch_tma_variant<false, true>(st, a, map, tt, smem);
 	if (slab_solve)
 		return launch_tma_variant<false, false, 1>(st, a, map, tt, smem);
 	if (gf && a.vP > 1)
 	{
 		tt.evict_first = st->grad_evict_first ? 1 : 0;
 		if (S % 4 == 0)
-			return launch_tma_variant<false, false, 0, 4>(st, a, map, tt, smem, gf);
-		return launch_tma_variant<false, false, 0, 1>(st, a, map, tt, smem, gf);
+			return launch_tma_variant<false, false, 0, 4, true>(st, a, map, tt, smem, gf);
+		return launch_tma_variant<false, false, 0, 1, true>(st, a, map, tt, smem, gf);
 	}
 	handled = !gf; // a gradient was asked for and this shape cannot compute it: the caller sweeps
 	if (!handled)
 		return BFVM_OK;
-	return launch_tma_variant<false, false>(st, a, map, tt, smem);
+	return dir ? launch_tma_variant<false, false, 0, 0, true>(st, a, map, tt, smem)
+			   : launch_tma_variant<false, false>(st, a, map, tt, smem);
 }
 
 } // namespace bfvm
