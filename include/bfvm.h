@@ -196,6 +196,9 @@ int bfvm_synchronize(bfvm_solver* s);
  *   the kernels that read the field directly).  Results agree to rounding either way.
  * - "tma_prefetch" 0/1: each staged-sweep refill also prefetches into L2 the tile after the one it
  *   copies (default 0).  Results are identical either way.
+ * - "tma_pairs" 0/1/2: staged sweeps whose two warp groups share each shared-memory stage, which then
+ *   holds two adjacent tiles copied as one 64-column box: 1 (the default) the z sweep, 2 the y and z
+ *   sweeps, 0 neither.  Results are identical either way.
  * - "fused_dirichlet" 0/1: in the LOD step (bfvm_diffusion_solve, bfvm_run_steps) a staged sweep
  *   writes the Dirichlet overwrite that follows it, tile by tile (default 0: the scatter kernel
  *   after the sweep, measured faster).  Results are identical either way.

@@ -1065,6 +1065,12 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 		s->use_tma = value != 0;
 	else if (n == "tma_prefetch")
 		s->tma_prefetch = value != 0;
+	else if (n == "tma_pairs")
+	{
+		if (value < 0 || value > 2)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "tma_pairs takes 0, 1 or 2");
+		s->tma_pairs = (int)value;
+	}
 	else if (n == "fused_dirichlet")
 		s->dir_fused = value != 0;
 	else if (n == "fused_gradient")

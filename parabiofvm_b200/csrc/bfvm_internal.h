@@ -192,6 +192,9 @@ struct bfvm_solver
 	long long launches = 0;
 	bool use_tma = true;		 // stage sweeps through shared memory with the TMA where the shape allows
 	bool tma_prefetch = false;	 // staged sweeps also prefetch into L2 the tile after the one they copy
+	// staged sweeps whose two warp groups share 64-column stages (sweep_tma.cu): 0 none, 1 the z
+	// sweep (measured 2-3 % faster), 2 the y and z sweeps (the y sweep measured 2 % slower)
+	int tma_pairs = 1;
 	// measured slower than the scatter kernel and the gradient kernel at 320^3 x 16 (the extra work
 	// in every tile of a latency-bound sweep costs more than the launches it saves), so off unless
 	// asked for with bfvm_set_option

@@ -58,11 +58,15 @@ struct tma_tile
 	int evict_first;
 	// with each refill, an L2 prefetch of the tile after it (option tma_prefetch)
 	int prefetch;
+	// y/z: two warp groups share each stage, which holds a pair of adjacent tiles (64 columns, one
+	// TMA box row of 256 bytes per plane); slots = pairs then, else slots = items
+	int pair;
+	long long slots;
 };
 
-// Issue the copies of tile w into `dst`, completing on `bar` (one thread).  The line elements land
-// after the virtual front: row rl of an x tile at rl * row_pitch + front, and the columns of a y/z
-// tile from stage row `pad` on.
+// Issue the copies of slot w (a tile, or with tt.pair the tile pair 2w, 2w + 1) into `dst`,
+// completing on `bar` (one thread).  The line elements land after the virtual front: row rl of an
+// x tile at rl * row_pitch + front, and the columns of a y/z slot from stage row `pad` on.
 __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMap* map, const tma_tile& tt, long long w,
 										   float* dst, uint64_t* bar)
 {
@@ -78,20 +82,22 @@ __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMa
 			bulk_load(dst + r * tt.row_pitch + tt.front, a.data + (row0 + r) * tt.XS, row_bytes, bar);
 		return;
 	}
-	const long long outer = w / tt.col_tiles;
-	const int c0 = (int)((w % tt.col_tiles) * 32);
-	mbar_expect_tx(bar, (uint32_t)(tt.nbox * tt.box_h * 32 * sizeof(float)));
-	if (w == a.drop_tile_copy)
+	const int width = tt.pair ? 64 : 32;
+	const long long t = tt.pair ? 2 * w : w; // first tile of the slot
+	const long long outer = t / tt.col_tiles;
+	const int c0 = (int)((t % tt.col_tiles) * 32);
+	mbar_expect_tx(bar, (uint32_t)(tt.nbox * tt.box_h * width * sizeof(float)));
+	if (t == a.drop_tile_copy || (tt.pair && t + 1 == a.drop_tile_copy))
 		return; // test of the bounded wait: the barrier expects bytes that never come
-	float* base = dst + a.pad * 32;
+	float* base = dst + a.pad * width;
 	for (int b = 0; b < tt.nbox; b++)
 	{
 		if (tt.axis == 1)
-			tma_load_3d(base + b * tt.box_h * 32, map, c0, b * tt.box_h, (int)outer, bar);
+			tma_load_3d(base + b * tt.box_h * width, map, c0, b * tt.box_h, (int)outer, bar);
 		else if (tt.evict_first)
-			tma_load_2d_hint(base + b * tt.box_h * 32, map, c0, b * tt.box_h, bar, l2_evict_first_policy());
+			tma_load_2d_hint(base + b * tt.box_h * width, map, c0, b * tt.box_h, bar, l2_evict_first_policy());
 		else
-			tma_load_2d(base + b * tt.box_h * 32, map, c0, b * tt.box_h, bar);
+			tma_load_2d(base + b * tt.box_h * width, map, c0, b * tt.box_h, bar);
 	}
 }
 
@@ -172,7 +178,7 @@ __device__ __forceinline__ void prefetch_tile(const sweep_args& a, const CUtenso
 __device__ __forceinline__ void refill(const sweep_args& a, const CUtensorMap& map, const tma_tile& tt, long long wn,
 									   float* stage, uint64_t* bar, long long wstride)
 {
-	if (wn >= tt.items)
+	if (wn >= tt.slots)
 		return;
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 	issue_tile(a, &map, tt, wn, stage, bar);
@@ -598,7 +604,10 @@ __global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constan
 // X instead of zero, with the tables of precompute_padded_range.
 // GRAD (z sweep, P > 1): the gradient of the step inside the sweep (grad_fuse); 1 the scalar form,
 // 4 the four-substrate form (S % 4 == 0).
-template <bool ROWS, bool NOALLOC, int SLAB, int GRAD, bool DIR>
+// PAIR (y/z, plain sweeps only): groups 2u and 2u + 1 share their stages, each slot a pair of tiles
+// of which group 2u + h solves tile 2 * slot + h; the group that finishes reading a stage second
+// refills it (a counter per stage in shared memory, arrivals acquire-release ordered).
+template <bool ROWS, bool NOALLOC, int SLAB, int GRAD, bool DIR, bool PAIR>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt, const __grid_constant__ grad_fuse gf)
@@ -608,12 +617,13 @@ __global__ void __launch_bounds__(640, 1)
 	// G * NST stages on a 128-byte boundary (TMA destinations), then tables, carries, barriers
 	const int NST = tt.stages;
 	const int G = tt.groups;
+	const int U = PAIR ? G / 2 : G; // stage owners: groups, or pairs of groups
 	float* const stages0 = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
 	const int S = a.S;
 	const int P = a.vP;
 	const int N = 32 * P;
 	const int NP = N + 1;
-	float* tab = stages0 + (size_t)G * NST * tt.stage_floats;
+	float* tab = stages0 + (size_t)U * NST * tt.stage_floats;
 	float2* tgtab = reinterpret_cast<float2*>(tab); // [S][NP] (tg, G)
 	float* btab = tab + 2 * S * NP;					// [S][NP] b'
 	float* ctab = btab + S * NP;					// [S]
@@ -622,7 +632,8 @@ __global__ void __launch_bounds__(640, 1)
 	const float* Gptab = tgptab + P * S;				 // [P][S], global
 	float* carries = tab + staged_table_floats(P, S); // [G][2][P][32]
 	uint64_t* bars0 = reinterpret_cast<uint64_t*>(
-		(reinterpret_cast<uintptr_t>(carries + (size_t)G * 2 * P * 32) + 7) & ~uintptr_t(7)); // [G][NST]
+		(reinterpret_cast<uintptr_t>(carries + (size_t)G * 2 * P * 32) + 7) & ~uintptr_t(7)); // [U][NST]
+	unsigned* const pair_count = reinterpret_cast<unsigned*>(bars0 + U * NST);			   // [U][NST] (PAIR)
 
 	const int lane = threadIdx.x;
 	const int j = threadIdx.y;
@@ -632,15 +643,21 @@ __global__ void __launch_bounds__(640, 1)
 	const int gthr = 32 * P; // threads of a group
 	const int bar_id = 1 + g;
 	const bool leader = lane == 0 && j == 0; // of the group
-	float* const stages = stages0 + (size_t)g * NST * tt.stage_floats;
-	uint64_t* const bars = bars0 + g * NST;
+	const int u = PAIR ? g >> 1 : g;
+	const int h = PAIR ? g & 1 : 0;
+	float* const stages = stages0 + (size_t)u * NST * tt.stage_floats;
+	uint64_t* const bars = bars0 + u * NST;
 	float* const carry_f = carries + (size_t)g * 2 * P * 32;
 	float* const carry_t = carry_f + P * 32;
 
 	if (tid == 0)
 	{
-		for (int k = 0; k < G * NST; k++)
+		for (int k = 0; k < U * NST; k++)
+		{
 			mbar_init(&bars0[k], 1);
+			if (PAIR)
+				pair_count[k] = 0;
+		}
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	{
@@ -657,39 +674,41 @@ __global__ void __launch_bounds__(640, 1)
 		for (int t = tid; t < S; t += nthr)
 			ctab[t] = gr[t];
 		// the virtual fronts read as zeros; the copies never write them
-		for (int k = 0; k < G * NST; k++)
+		for (int k = 0; k < U * NST; k++)
 			for (int r = 0; r < tt.front_count; r++)
 				for (int t = tid; t < tt.front_floats; t += nthr)
 					stages0[(size_t)k * tt.stage_floats + r * tt.front_pitch + t] = 0.f;
 	}
 	__syncthreads(); // also publishes the barrier init
 
-	// tiles of this group: w0, w0 + stride, ...
-	const long long w0 = tt.first + (long long)blockIdx.x * G + g;
-	const long long wstride = (long long)gridDim.x * G;
+	// slots of this stage owner: sl0, sl0 + slstride, ...; this group's tiles w0, w0 + wstride, ...
+	const long long sl0 = (PAIR ? tt.first / 2 : tt.first) + (long long)blockIdx.x * U + u;
+	const long long slstride = (long long)gridDim.x * U;
+	const long long w0 = PAIR ? 2 * sl0 + h : sl0;
+	const long long wstride = PAIR ? 2 * slstride : slstride;
 
-	// prologue: the first NST tiles of this group, one per stage
-	if (leader)
+	// prologue: the first NST slots, one per stage
+	if (leader && h == 0)
 	{
 		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 		for (int k = 0; k < NST; k++)
 		{
-			const long long wk = w0 + (long long)k * wstride;
-			if (wk < tt.items)
-				issue_tile(a, &map, tt, wk, stages + (size_t)k * tt.stage_floats, &bars[k]);
+			const long long sk = sl0 + (long long)k * slstride;
+			if (sk < tt.slots)
+				issue_tile(a, &map, tt, sk, stages + (size_t)k * tt.stage_floats, &bars[k]);
 		}
 	}
 
 	const int p = 32 * j;
 	bool failed = false;
 	int it = 0;
-	long long w = w0;
+	long long w = w0, sl = sl0;
 	// the Dirichlet entries of the previous tile (written after the first barrier of this one):
 	// their list offsets, loaded an iteration before the entries, and the entries themselves
 	int dir_prev[4] = { 0, 0, 0, 0 };
 	dir_regs dir_hold;
 	int face_tile_next = (SLAB == 0 && GRAD == 0 && !DIR && a.face_apply && w < tt.items) ? __ldg(&a.face_tiles[w]) : 0;
-	for (; w < tt.items; w += wstride, it++)
+	for (; w < tt.items; w += wstride, sl += slstride, it++)
 	{
 		const int st = it % NST;
 		const uint32_t parity = (uint32_t)((it / NST) & 1);
@@ -710,8 +729,8 @@ __global__ void __launch_bounds__(640, 1)
 			tile_line tl;
 			tl.locate(a, tt, w, lane);
 			s = tl.s;
-			sbase = tl.sbase;
-			sstride = ROWS ? tl.sstride : 32;
+			sbase = PAIR ? tl.sbase + 32 * h : tl.sbase;
+			sstride = ROWS ? tl.sstride : (PAIR ? 64 : 32);
 		}
 		// the line's face conditions, looked up while the tile's copy is in flight (the plain
 		// sweeps of the step only)
@@ -756,7 +775,22 @@ __global__ void __launch_bounds__(640, 1)
 		// consumed by the recurrences before the barrier): refill the stage with the tile NST
 		// ahead, so NST tiles stay in flight through the rest of this tile's solve
 		if (leader)
-			refill(a, map, tt, w + (long long)NST * wstride, stages + (size_t)st * tt.stage_floats, &bars[st], wstride);
+		{
+			bool last_reader = true;
+			if (PAIR)
+			{
+				// the second group of the pair to finish reading the stage refills it
+				unsigned old;
+				asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;"
+							 : "=r"(old)
+							 : "r"(smem_addr(&pair_count[u * NST + st]))
+							 : "memory");
+				last_reader = (old & 1) != 0;
+			}
+			if (last_reader)
+				refill(a, map, tt, sl + (long long)NST * slstride, stages + (size_t)st * tt.stage_floats, &bars[st],
+					   wstride);
+		}
 		// the barrier also ordered the previous tile's stores: its Dirichlet entries go on top
 		if (DIR && a.dir.items > 0 && it > 0)
 			dir_hold.store(a.dir, dir_prev, a.data, lane + 32 * j, gthr);
@@ -885,12 +919,12 @@ __global__ void __launch_bounds__(640, 1)
 	if (failed && leader)
 	{
 		atomicOr(a.err, DEVERR_TIMEOUT);
-		// let the group's copies already issued (tiles w .. w + (NST-1) * stride) land before the
-		// CTA exits (bounded waits)
+		// let the copies already issued (slots sl .. sl + (NST-1) * stride) land before the CTA
+		// exits (bounded waits)
 		for (int k = 0; k < NST; k++)
 		{
-			const long long wk = w + (long long)k * wstride;
-			if (wk < tt.items)
+			const long long sk = sl + (long long)k * slstride;
+			if (sk < tt.slots)
 				mbar_wait(&bars[(it + k) % NST], (uint32_t)(((it + k) / NST) & 1), a.wait_limit);
 		}
 	}
@@ -919,15 +953,51 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 
 static constexpr int TMA_MAX_P = 16;
 
-template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0, bool DIR = false>
+// The tensor map of a y sweep (3D over [Z][Y][XS]) or a z sweep (2D over [Z][Y*XS]): boxes of
+// `width` columns x box_h rows.
+static CUresult encode_box(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap& map, int axis, float* dens,
+						   long long X, long long Y, long long Z, long long S, int width, int box_h)
+{
+	const long long XS = X * S;
+	cuuint64_t dims[3], strides[2];
+	cuuint32_t box[3], estr[3] = { 1, 1, 1 };
+	cuuint32_t rank;
+	if (axis == 1)
+	{
+		rank = 3;
+		dims[0] = (cuuint64_t)XS;
+		dims[1] = (cuuint64_t)Y;
+		dims[2] = (cuuint64_t)Z;
+		strides[0] = (cuuint64_t)(XS * sizeof(float));
+		strides[1] = (cuuint64_t)(Y * XS * sizeof(float));
+		box[0] = (cuuint32_t)width;
+		box[1] = (cuuint32_t)box_h;
+		box[2] = 1;
+	}
+	else
+	{
+		rank = 2;
+		dims[0] = (cuuint64_t)(Y * XS);
+		dims[1] = (cuuint64_t)Z;
+		strides[0] = (cuuint64_t)(Y * XS * sizeof(float));
+		box[0] = (cuuint32_t)width;
+		box[1] = (cuuint32_t)box_h;
+	}
+	return encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, dens, dims, strides, box, estr,
+				  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+				  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+
+template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0, bool DIR = false, bool PAIR = false>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem, const grad_fuse* gfp = nullptr)
 {
-	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD, DIR>;
+	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD, DIR, PAIR>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
 	const int threads = 32 * a.vP * tt.groups;
+	// one CTA per G tiles (per G / 2 slots of two tiles when paired)
 	const int grid =
 		persistent_grid(kernel, threads, smem, (tt.items - tt.first + tt.groups - 1) / tt.groups, st->device);
 	grad_fuse gf;
@@ -1011,34 +1081,7 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.front_floats = a.pad * 32;
 		tt.front_count = 1;
 		tt.front_pitch = 0;
-		cuuint64_t dims[3], strides[2];
-		cuuint32_t box[3], estr[3] = { 1, 1, 1 };
-		cuuint32_t rank;
-		if (axis == 1)
-		{
-			rank = 3;
-			dims[0] = (cuuint64_t)XS;
-			dims[1] = (cuuint64_t)Y;
-			dims[2] = (cuuint64_t)Z;
-			strides[0] = (cuuint64_t)(XS * sizeof(float));
-			strides[1] = (cuuint64_t)(Y * XS * sizeof(float));
-			box[0] = 32;
-			box[1] = (cuuint32_t)tt.box_h;
-			box[2] = 1;
-		}
-		else
-		{
-			rank = 2;
-			dims[0] = (cuuint64_t)(Y * XS);
-			dims[1] = (cuuint64_t)Z;
-			strides[0] = (cuuint64_t)(Y * XS * sizeof(float));
-			box[0] = 32;
-			box[1] = (cuuint32_t)tt.box_h;
-		}
-		CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, st->dens, dims, strides, box, estr,
-							CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-							CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-		if (r != CUDA_SUCCESS)
+		if (encode_box(encode, map, axis, st->dens, X, Y, Z, S, 32, tt.box_h) != CUDA_SUCCESS)
 			return BFVM_OK; // fall back to the direct kernels
 	}
 	int dev = 0, optin = 0;
@@ -1050,7 +1093,7 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	const size_t stage_bytes = (size_t)tt.stage_floats * sizeof(float);
 	auto fixed_bytes = [&](int G) {
 		return 128 + (staged_table_floats(a.vP, (int)S) + (size_t)G * 2 * a.vP * 32) * sizeof(float) + 8
-			   + (size_t)G * 4 * sizeof(uint64_t);
+			   + (size_t)G * 4 * (sizeof(uint64_t) + sizeof(unsigned));
 	};
 	const int Gmax = std::max(1, std::min(8, 20 / a.vP));
 	auto max_stages = [&](int G) { return (int)std::min<size_t>(4, ((size_t)optin - std::min((size_t)optin, fixed_bytes(G))) / ((size_t)G * stage_bytes)); };
@@ -1082,6 +1125,23 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	tt.stages = NST;
 	tt.prefetch = st->tma_prefetch ? 1 : 0;
 	const size_t smem = fixed_bytes(G) + (size_t)G * tt.stages * stage_bytes;
+	// pairs of groups sharing 64-column stages (the same shared memory: half the stages, twice the
+	// width): the plain y and z sweeps over the whole field, an even number of groups, and for y an
+	// even number of tiles per plane so that no pair spans two planes
+	const bool pair = (axis == 2 ? st->tma_pairs >= 1 : axis == 1 && st->tma_pairs == 2) && !slab_solve && !gf && a.dir.items == 0 && w_begin == 0 && w_end < 0
+					  && G % 2 == 0 && (axis == 2 || tt.col_tiles % 2 == 0);
+	if (pair)
+	{
+		CUtensorMap pmap;
+		if (encode_box(encode, pmap, axis, st->dens, X, Y, Z, S, 64, tt.box_h) != CUDA_SUCCESS)
+			return BFVM_OK; // the unpaired map was accepted above; a refusal here is not expected
+		map = pmap;
+		tt.pair = 1;
+		tt.prefetch = 0;
+		tt.slots = (tt.items + 1) / 2;
+		tt.stage_floats *= 2;
+		tt.front_floats *= 2;
+	}
 	if (w_end >= 0 || w_begin != 0)
 	{
 		if (w_end < 0)
@@ -1094,6 +1154,8 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.first = w_begin;
 		tt.items = w_end;
 	}
+	if (!tt.pair)
+		tt.slots = tt.items;
 
 	handled = true;
 	// the kernels that write Dirichlet lists per tile are separate instances, so the default ones
@@ -1103,8 +1165,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		return dir ? launch_tma_variant<true, true, 0, 0, true>(st, a, map, tt, smem)
 				   : launch_tma_variant<true, true>(st, a, map, tt, smem);
 	if (axis == 1)
-		return dir ? launch_tma_variant<false, true, 0, 0, true>(st, a, map, tt, smem)
-				   : launch_tma_variant<false, true>(st, a, map, tt, smem);
+		return pair ? launch_tma_variant<false, true, 0, 0, false, true>(st, a, map, tt, smem)
+					: (dir ? launch_tma_variant<false, true, 0, 0, true>(st, a, map, tt, smem)
+						   : launch_tma_variant<false, true>(st, a, map, tt, smem));
 	if (slab_solve)
 		return launch_tma_variant<false, false, 1>(st, a, map, tt, smem);
 	if (gf && a.vP > 1)
@@ -1117,8 +1180,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	handled = !gf; // a gradient was asked for and this shape cannot compute it: the caller sweeps
 	if (!handled)
 		return BFVM_OK;
-	return dir ? launch_tma_variant<false, false, 0, 0, true>(st, a, map, tt, smem)
-			   : launch_tma_variant<false, false>(st, a, map, tt, smem);
+	return pair ? launch_tma_variant<false, false, 0, 0, false, true>(st, a, map, tt, smem)
+				: (dir ? launch_tma_variant<false, false, 0, 0, true>(st, a, map, tt, smem)
+					   : launch_tma_variant<false, false>(st, a, map, tt, smem));
 }
 
 } // namespace bfvm
