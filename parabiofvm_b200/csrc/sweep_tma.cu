@@ -110,12 +110,13 @@ struct tile_line
 	float* line;
 	long long gstride;
 
+	template <bool ROWS>
 	__device__ __forceinline__ void locate(const sweep_args& a, const tma_tile& tt, long long w, int lane)
 	{
 		const int S = a.S;
-		if (tt.axis == 0)
+		if (ROWS)
 		{
-			const int rl = lane / S;
+			const int rl = (32 % S == 0) ? lane >> (31 - __clz(S)) : lane / S;
 			s = lane - rl * S;
 			const long long row = w * tt.R + rl;
 			active = rl < tt.R && row < tt.nrows;
@@ -128,14 +129,18 @@ struct tile_line
 		}
 		else
 		{
-			const long long outer = w / tt.col_tiles;
-			const long long q = (w % tt.col_tiles) * 32 + lane;
-			active = q < tt.ncols;
-			const long long qq = active ? q : 0;
-			s = (int)(qq % S);
+			// tile and column indices below 2^31 (launch_sweep_tma declines other shapes): 32-bit
+			// divisions, several times cheaper than 64-bit ones, and this runs twice per tile
+			// (the z sweep's tiles cover one plane; when S divides 32, a lane's substrate is fixed)
+			const unsigned wu = (unsigned)w, ct = (unsigned)tt.col_tiles;
+			const unsigned outer = tt.axis == 2 ? 0u : wu / ct;
+			const unsigned q = (wu - outer * ct) * 32u + (unsigned)lane;
+			active = q < (unsigned)tt.ncols;
+			const unsigned qq = active ? q : 0u;
+			s = (32 % S == 0) ? (lane & (S - 1)) : (int)(qq % (unsigned)S);
 			sbase = lane;
 			sstride = 32;
-			line = a.data + outer * tt.outer_stride + qq;
+			line = a.data + (long long)outer * tt.outer_stride + qq;
 			gstride = tt.line_stride;
 		}
 	}
@@ -607,7 +612,10 @@ __global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constan
 // PAIR (y/z, plain sweeps only): groups 2u and 2u + 1 share their stages, each slot a pair of tiles
 // of which group 2u + h solves tile 2 * slot + h; the group that finishes reading a stage second
 // refills it (a counter per stage in shared memory, arrivals acquire-release ordered).
-template <bool ROWS, bool NOALLOC, int SLAB, int GRAD, bool DIR, bool PAIR>
+// MODE: 0 the plain sweep, 1 with the per-tile Dirichlet lists (sweep_args::dir), 2 with the face
+// conditions by position (sweep_args::face_apply); separate instances, so the plain sweep holds no
+// registers for either.
+template <bool ROWS, bool NOALLOC, int SLAB, int GRAD, int MODE, bool PAIR>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt, const __grid_constant__ grad_fuse gf)
@@ -707,11 +715,14 @@ __global__ void __launch_bounds__(640, 1)
 	// their list offsets, loaded an iteration before the entries, and the entries themselves
 	int dir_prev[4] = { 0, 0, 0, 0 };
 	dir_regs dir_hold;
-	int face_tile_next = (SLAB == 0 && GRAD == 0 && !DIR && a.face_apply && w < tt.items) ? __ldg(&a.face_tiles[w]) : 0;
-	for (; w < tt.items; w += wstride, sl += slstride, it++)
+	constexpr bool DIR = MODE == 1;
+	constexpr bool FACES = MODE == 2 && SLAB == 0 && GRAD == 0;
+	int face_tile_next = (FACES && a.face_apply && w < tt.items) ? __ldg(&a.face_tiles[w]) : 0;
+	// stage st = it % NST and its phase parity (it / NST) & 1, advanced without divisions
+	int st = 0;
+	uint32_t parity = 0;
+	for (; w < tt.items; w += wstride, sl += slstride, it++, st = st + 1 == NST ? 0 : st + 1, parity ^= st == 0 ? 1u : 0u)
 	{
-		const int st = it % NST;
-		const uint32_t parity = (uint32_t)((it / NST) & 1);
 		int dir_cur[4] = { 0, 0, 0, 0 };
 		if (DIR && a.dir.items > 0)
 		{
@@ -727,14 +738,12 @@ __global__ void __launch_bounds__(640, 1)
 		int s, sbase, sstride;
 		{
 			tile_line tl;
-			tl.locate(a, tt, w, lane);
+			tl.template locate<ROWS>(a, tt, w, lane);
 			s = tl.s;
 			sbase = PAIR ? tl.sbase + 32 * h : tl.sbase;
 			sstride = ROWS ? tl.sstride : (PAIR ? 64 : 32);
 		}
-		// the line's face conditions, looked up while the tile's copy is in flight (the plain
-		// sweeps of the step only)
-		constexpr bool FACES = SLAB == 0 && GRAD == 0 && !DIR;
+		// the line's face conditions, looked up while the tile's copy is in flight
 		// (face_tiles[w] was loaded a tile ahead, so its latency hides behind the previous tile)
 		int faces = 0;
 		if (FACES && a.face_apply)
@@ -864,7 +873,7 @@ __global__ void __launch_bounds__(640, 1)
 			long long w2;
 			asm volatile("mov.b64 %0, %1;" : "=l"(w2) : "l"(w));
 			tile_line tl2;
-			tl2.locate(a, tt, w2, lane);
+			tl2.template locate<ROWS>(a, tt, w2, lane);
 			if (tl2.active)
 			{
 				if (j > 0 || a.pad == 0)
@@ -988,11 +997,11 @@ static CUresult encode_box(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap
 				  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
-template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0, bool DIR = false, bool PAIR = false>
+template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0, int MODE = 0, bool PAIR = false>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem, const grad_fuse* gfp = nullptr)
 {
-	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD, DIR, PAIR>;
+	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD, MODE, PAIR>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
@@ -1073,6 +1082,10 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.ncols = axis == 1 ? XS : Y * XS;
 		tt.col_tiles = (tt.ncols + 31) / 32;
 		tt.items = (axis == 1 ? Z : 1) * tt.col_tiles;
+		// tile indices and columns within 31 bits (tile_line::locate; 2^31 columns of a plane is
+		// far beyond any field that fits the device)
+		if (tt.items >= (1LL << 31) || tt.col_tiles * 32 >= (1LL << 31))
+			return BFVM_OK;
 		tt.outer_stride = axis == 1 ? Y * XS : 0;
 		tt.line_stride = axis == 1 ? XS : Y * XS;
 		// stage rows: the virtual front, then the boxes (the last may run past the line end and is
@@ -1128,8 +1141,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	// pairs of groups sharing 64-column stages (the same shared memory: half the stages, twice the
 	// width): the plain y and z sweeps over the whole field, an even number of groups, and for y an
 	// even number of tiles per plane so that no pair spans two planes
-	const bool pair = (axis == 2 ? st->tma_pairs >= 1 : axis == 1 && st->tma_pairs == 2) && !slab_solve && !gf && a.dir.items == 0 && w_begin == 0 && w_end < 0
-					  && G % 2 == 0 && (axis == 2 || tt.col_tiles % 2 == 0);
+	const int mode = a.dir.items > 0 ? 1 : (a.face_apply ? 2 : 0);
+	const bool pair = (axis == 2 ? st->tma_pairs >= 1 : axis == 1 && st->tma_pairs == 2) && !slab_solve && !gf
+					  && mode != 1 && w_begin == 0 && w_end < 0 && G % 2 == 0 && (axis == 2 || tt.col_tiles % 2 == 0);
 	if (pair)
 	{
 		CUtensorMap pmap;
@@ -1158,31 +1172,37 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.slots = tt.items;
 
 	handled = true;
-	// the kernels that write Dirichlet lists per tile are separate instances, so the default ones
-	// keep those registers for the solve
-	const bool dir = a.dir.items > 0;
 	if (axis == 0)
-		return dir ? launch_tma_variant<true, true, 0, 0, true>(st, a, map, tt, smem)
-				   : launch_tma_variant<true, true>(st, a, map, tt, smem);
+		return mode == 1   ? launch_tma_variant<true, true, 0, 0, 1>(st, a, map, tt, smem)
+			   : mode == 2 ? launch_tma_variant<true, true, 0, 0, 2>(st, a, map, tt, smem)
+						   : launch_tma_variant<true, true>(st, a, map, tt, smem);
 	if (axis == 1)
-		return pair ? launch_tma_variant<false, true, 0, 0, false, true>(st, a, map, tt, smem)
-					: (dir ? launch_tma_variant<false, true, 0, 0, true>(st, a, map, tt, smem)
-						   : launch_tma_variant<false, true>(st, a, map, tt, smem));
+	{
+		if (pair)
+			return mode == 2 ? launch_tma_variant<false, true, 0, 0, 2, true>(st, a, map, tt, smem)
+							 : launch_tma_variant<false, true, 0, 0, 0, true>(st, a, map, tt, smem);
+		return mode == 1   ? launch_tma_variant<false, true, 0, 0, 1>(st, a, map, tt, smem)
+			   : mode == 2 ? launch_tma_variant<false, true, 0, 0, 2>(st, a, map, tt, smem)
+						   : launch_tma_variant<false, true>(st, a, map, tt, smem);
+	}
 	if (slab_solve)
 		return launch_tma_variant<false, false, 1>(st, a, map, tt, smem);
 	if (gf && a.vP > 1)
 	{
 		tt.evict_first = st->grad_evict_first ? 1 : 0;
 		if (S % 4 == 0)
-			return launch_tma_variant<false, false, 0, 4, true>(st, a, map, tt, smem, gf);
-		return launch_tma_variant<false, false, 0, 1, true>(st, a, map, tt, smem, gf);
+			return launch_tma_variant<false, false, 0, 4, 1>(st, a, map, tt, smem, gf);
+		return launch_tma_variant<false, false, 0, 1, 1>(st, a, map, tt, smem, gf);
 	}
 	handled = !gf; // a gradient was asked for and this shape cannot compute it: the caller sweeps
 	if (!handled)
 		return BFVM_OK;
-	return pair ? launch_tma_variant<false, false, 0, 0, false, true>(st, a, map, tt, smem)
-				: (dir ? launch_tma_variant<false, false, 0, 0, true>(st, a, map, tt, smem)
-					   : launch_tma_variant<false, false>(st, a, map, tt, smem));
+	if (pair)
+		return mode == 2 ? launch_tma_variant<false, false, 0, 0, 2, true>(st, a, map, tt, smem)
+						 : launch_tma_variant<false, false, 0, 0, 0, true>(st, a, map, tt, smem);
+	return mode == 1   ? launch_tma_variant<false, false, 0, 0, 1>(st, a, map, tt, smem)
+		   : mode == 2 ? launch_tma_variant<false, false, 0, 0, 2>(st, a, map, tt, smem)
+					   : launch_tma_variant<false, false>(st, a, map, tt, smem);
 }
 
 } // namespace bfvm
