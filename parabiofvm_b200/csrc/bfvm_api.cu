@@ -69,6 +69,8 @@ static int upload_plan(bfvm_solver* s, int axis)
 		if ((st = device_alloc(&p.vtab, vt.size())))
 			return st;
 		BFVM_CUDA(cudaMemcpy(p.vtab, vt.data(), vt.size() * sizeof(float), cudaMemcpyHostToDevice));
+		if (s->slab_global_z == 0 && (st = build_chunks(s, axis, bp, c)))
+			return st;
 	}
 	return BFVM_OK;
 }
@@ -80,6 +82,7 @@ static void free_plan(sweep_plan& p)
 	device_free(p.gq);
 	device_free(p.Gp);
 	device_free(p.vtab);
+	free_chunks(p);
 }
 
 static void free_graphs(bfvm_solver* s)
@@ -1065,6 +1068,14 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 		s->use_tma = value != 0;
 	else if (n == "tma_prefetch")
 		s->tma_prefetch = value != 0;
+	else if (n == "chunk_elements")
+	{
+		if (value < 64 || value > 512)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "chunk_elements must lie in [64, 512]");
+		s->chunk_elements = (int)value;
+		free_graphs(s);
+		return rebuild_chunks(s);
+	}
 	else if (n == "tma_pairs")
 	{
 		if (value < 0 || value > 2)

@@ -62,6 +62,24 @@ struct sweep_plan
 	int vP = 1;
 	int pad = 0;
 	float* vtab = nullptr; // padded_table_floats(vP, S) floats
+	// lines longer than the staged sweep takes, cut into chunks that it takes (chunks.cu): chunk k
+	// holds elements [bounds[k], bounds[k + 1]) of every line; count 0 when the axis is not chunked
+	struct chunks_t
+	{
+		int count = 0;
+		std::vector<int> bounds;
+		std::vector<float*> vtab; // per chunk, the tables of precompute_padded_range
+		std::vector<int> vP, pad;
+		// the carries pass (slab_reduce_weights): per chunk, A over elements [a_first, a_first + na)
+		// and B over [bounds[k], bounds[k] + nb), with weights at rw + w_off[k] ([na][S], then [nb][S])
+		std::vector<int> a_first, na, nb;
+		std::vector<long long> w_off;
+		float* rw = nullptr;
+		float* coef = nullptr;	// [count][3][S] (slab_coefficients)
+		float* carry = nullptr; // [count][2][lines]: each chunk's carries C, X of every line
+		float* ex = nullptr;	// [count - 1][2][lines]: the end sums A, B at each chunk boundary
+		long long lines = 0;
+	} chunks;
 };
 
 // Radix-sort / scan scratch for the agent binning.
@@ -205,6 +223,9 @@ struct bfvm_solver
 	// y sweeps band by band of `xy_band_planes` z planes, the z sweep and the gradient band by band
 	// of `zg_band_rows` y rows (sweep.cu)
 	int xy_band_planes = 0;
+	// the longest chunk of a line that the staged sweep takes as a chunk (chunks.cu): lines longer
+	// than this are cut into chunks (lines of more than 512 elements always are)
+	int chunk_elements = 512;
 	int zg_band_rows = 0;
 	int* grad_tile_done = nullptr; // [z tiles] and [1 + z tiles] of the gradient inside the z sweep
 	int* grad_deferred = nullptr;
@@ -267,7 +288,7 @@ void slab_coefficients(int n, int S, const std::vector<float>& bp, const std::ve
 					   const int* bounds, std::vector<float>& out);
 // the weights of A and B of the slab holding elements [i0, i1), over the planes that matter
 void slab_reduce_weights(int n, int i0, int i1, int S, const std::vector<float>& bp, const std::vector<float>& c,
-						 std::vector<float>& w, int& a_first, int& na, int& nb);
+						 std::vector<float>& w, int& a_first, int& na, int& nb, int drop_log2 = -50);
 
 // bfvm_api.cu
 int one_step(bfvm_solver* s, bool recompute); // diffusion, gradient, secretion on the solver's stream
@@ -287,6 +308,12 @@ int launch_staged_sweep(bfvm_solver* s, int axis, const sweep_tuning& tune, bool
 std::vector<sweep_tuning> staged_sweep_shapes(bfvm_solver* s, int axis);
 // autotune.cu: a tuned launch shape of an equal mesh, from the process-wide cache
 bool cached_tuning(const bfvm_solver* s, int axis, sweep_tuning& out);
+// chunks.cu: the chunk plan of an axis whose lines the staged sweep cannot take whole (from the
+// line's b' and c), its release, and the chunked sweep (`handled` false when it cannot run)
+int build_chunks(bfvm_solver* s, int axis, const std::vector<float>& bp, const std::vector<float>& c);
+int rebuild_chunks(bfvm_solver* s); // every axis, after the chunk length changed (outside any capture)
+void free_chunks(sweep_plan& p);
+int launch_chunked_sweep(bfvm_solver* s, int axis, bool& handled);
 // the solve pass of a slab solver's z sweep, with the carries in s->slab_carry
 int launch_slab_z(bfvm_solver* s);
 // dirichlet.cu

@@ -260,16 +260,16 @@ void slab_coefficients(int n, int S, const std::vector<float>& bp, const std::ve
 // forward value f_k in the backward substitution's first element.  The weights shrink
 // geometrically away from the end each sum belongs to, so the sums keep only the planes whose
 // weights matter: planes are dropped from the far end while the dropped weights (the largest over
-// the substrates, summed) stay at most 2^-50.  That moves A and B by at most 2^-50 of the line's
-// largest |d|.  A is needed only below a neighbour (i1 < n), B only above one (i0 > 0); a sum not
+// the substrates, summed) stay at most 2^drop_log2 (2^-50 by default).  That moves A and B by at
+// most that fraction of the line's largest |d|.  A is needed only below a neighbour (i1 < n), B only above one (i0 > 0); a sum not
 // needed keeps no planes.
 // Output w = alpha of planes [a_first, i1) as [na][S], then omega of planes [i0, i0 + nb) as
 // [nb][S], evaluated in double from the float b' and e and rounded once.
 void slab_reduce_weights(int n, int i0, int i1, int S, const std::vector<float>& bp, const std::vector<float>& c,
-						 std::vector<float>& w, int& a_first, int& na, int& nb)
+						 std::vector<float>& w, int& a_first, int& na, int& nb, int drop_log2)
 {
 	const int nl = i1 - i0;
-	const double drop = std::ldexp(1.0, -50);
+	const double drop = std::ldexp(1.0, drop_log2);
 	std::vector<double> alpha((size_t)nl * S), omega((size_t)nl * S), phi((size_t)nl);
 	for (int s = 0; s < S; s++)
 	{

@@ -248,14 +248,23 @@ int launch_slab_z(bfvm_solver* st)
 }
 
 // The sweep of one axis by the first kernel that takes its shape: the TMA-staged sweep (which sets
-// `staged`; with gf, only if it also computes the gradient), the ensemble sweep on this mesh alone,
-// or the direct kernels.
+// `staged`; with gf, only if it also computes the gradient), the staged sweep of the line's chunks,
+// the ensemble sweep on this mesh alone, or the direct kernels.
 static int sweep_axis(bfvm_solver* st, int axis, const sweep_args& a, bool& staged, const grad_fuse* gf = nullptr)
 {
 	const sweep_plan& pl = st->plan[axis];
 	int rc = BFVM_OK;
 	bool handled = false;
 	staged = false;
+	// lines longer than the chunk length (chunk_elements; always beyond 512): the staged sweep of
+	// their chunks with their carries (chunks.cu).  Not `staged` for the caller: the chunks write no
+	// per-tile overwrite, face condition or gradient.
+	if (st->use_tma && pl.chunks.count > 0)
+	{
+		rc = launch_chunked_sweep(st, axis, handled);
+		if (rc || handled)
+			return rc;
+	}
 	if (st->use_tma)
 		rc = launch_sweep_tma(st, axis, a, handled, &st->tune[axis], nullptr, false, gf);
 	if (!rc && !handled && gf)

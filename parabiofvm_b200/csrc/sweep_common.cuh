@@ -222,14 +222,31 @@ struct grad_fuse
 	long long spin_limit;
 };
 
+// Chunks of the lines along an axis (a line longer than the staged sweep takes, cut into chunks
+// that it does take), swept in one launch: chunk k holds elements [e0[k], e0[k] + len) of every
+// line, with its tables vtab[k] (precompute_padded_range; every chunk of a launch has the same
+// length, so the same blocks and front), and the carries that enter each line, carry[k][2][lines]
+// (C, X), indexed by line: x, row * S + s; y, z * X * S + column; z, column of the y*x*s plane.
+struct line_chunks
+{
+	int count = 0;
+	long long e0[8] = {};
+	long long len = 0;
+	const float* vtab[8] = {};
+	int vP = 1, pad = 0;
+	const float* carry = nullptr;
+	long long lines = 0;
+};
+
 // slab_solve (z axis only): the solve pass of a z-slab's sweep.  gf (z axis only): compute the
 // gradient inside the sweep; `handled` then also means the gradient is (being) computed.
 // [w_begin, w_end): sweep only these tiles (w_end -1: to the last tile; not with gf or slab_solve).
-// The launch shape is the one chosen for the whole field.
+// The launch shape is the one chosen for the whole field.  chunks: sweep these chunks of every line
+// (their solve pass, entering each line with the chunk's carries).
 int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled,
 					 const sweep_tuning* tune = nullptr, std::vector<sweep_tuning>* shapes = nullptr,
 					 bool slab_solve = false, const grad_fuse* gf = nullptr, long long w_begin = 0,
-					 long long w_end = -1);
+					 long long w_end = -1, const line_chunks* chunk = nullptr);
 
 // The tiles of the staged sweep along `axis` (sweep_tma.cu and the Dirichlet tile lists): x,
 // R = 32 / S whole rows; y, 32 columns of the x*s plane of one z plane; z, 32 columns of the y*x*s

@@ -45,6 +45,7 @@ struct tma_tile
 	long long outer_stride, line_stride;
 	int box_h, nbox;	 // TMA boxes along the line (y, z)
 	int R, row_pitch;	 // rows per tile and padded row length in floats (x)
+	long long row_elems; // x: floats of a row that a tile stages (XS, or the chunk's part of it)
 	int front;			 // x: floats before each staged row (holds its virtual front, 16-byte multiple)
 	long long nrows;
 	long long XS;
@@ -62,24 +63,31 @@ struct tma_tile
 	// TMA box row of 256 bytes per plane); slots = pairs then, else slots = items
 	int pair;
 	long long slots;
+	// the equal chunks of longer lines in one launch (SLAB 2): CTA b sweeps chunk b % chunks, whose
+	// elements start chunk_e0 elements along the line, chunk_e0 * e_stride floats into the field,
+	// with the tables chunk_vtab
+	int chunks;
+	long long e_stride;
+	long long chunk_e0[8];
+	const float* chunk_vtab[8];
 };
 
 // Issue the copies of slot w (a tile, or with tt.pair the tile pair 2w, 2w + 1) into `dst`,
 // completing on `bar` (one thread).  The line elements land after the virtual front: row rl of an
 // x tile at rl * row_pitch + front, and the columns of a y/z slot from stage row `pad` on.
 __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMap* map, const tma_tile& tt, long long w,
-										   float* dst, uint64_t* bar)
+										   float* dst, uint64_t* bar, long long coff = 0, int crow = 0)
 {
 	if (tt.axis == 0)
 	{
 		const long long row0 = w * tt.R;
 		const int rows = (int)min((long long)tt.R, tt.nrows - row0);
-		const uint32_t row_bytes = (uint32_t)(tt.XS * sizeof(float));
+		const uint32_t row_bytes = (uint32_t)(tt.row_elems * sizeof(float));
 		mbar_expect_tx(bar, row_bytes * rows);
 		if (w == a.drop_tile_copy)
 			return; // test of the bounded wait: the barrier expects bytes that never come
 		for (int r = 0; r < rows; r++)
-			bulk_load(dst + r * tt.row_pitch + tt.front, a.data + (row0 + r) * tt.XS, row_bytes, bar);
+			bulk_load(dst + r * tt.row_pitch + tt.front, a.data + coff + (row0 + r) * tt.XS, row_bytes, bar);
 		return;
 	}
 	const int width = tt.pair ? 64 : 32;
@@ -93,11 +101,11 @@ __device__ __forceinline__ void issue_tile(const sweep_args& a, const CUtensorMa
 	for (int b = 0; b < tt.nbox; b++)
 	{
 		if (tt.axis == 1)
-			tma_load_3d(base + b * tt.box_h * width, map, c0, b * tt.box_h, (int)outer, bar);
+			tma_load_3d(base + b * tt.box_h * width, map, c0, crow + b * tt.box_h, (int)outer, bar);
 		else if (tt.evict_first)
-			tma_load_2d_hint(base + b * tt.box_h * width, map, c0, b * tt.box_h, bar, l2_evict_first_policy());
+			tma_load_2d_hint(base + b * tt.box_h * width, map, c0, crow + b * tt.box_h, bar, l2_evict_first_policy());
 		else
-			tma_load_2d(base + b * tt.box_h * width, map, c0, b * tt.box_h, bar);
+			tma_load_2d(base + b * tt.box_h * width, map, c0, crow + b * tt.box_h, bar);
 	}
 }
 
@@ -111,7 +119,8 @@ struct tile_line
 	long long gstride;
 
 	template <bool ROWS>
-	__device__ __forceinline__ void locate(const sweep_args& a, const tma_tile& tt, long long w, int lane)
+	__device__ __forceinline__ void locate(const sweep_args& a, const tma_tile& tt, long long w, int lane,
+										   long long coff = 0)
 	{
 		const int S = a.S;
 		if (ROWS)
@@ -124,7 +133,7 @@ struct tile_line
 			// lanes past the last row of the tile read row 0
 			sbase = (rl < tt.R ? rl : 0) * tt.row_pitch + tt.front - a.pad * S + s;
 			sstride = S;
-			line = a.data + rr * tt.XS + s;
+			line = a.data + coff + rr * tt.XS + s;
 			gstride = S;
 		}
 		else
@@ -140,7 +149,7 @@ struct tile_line
 			s = (32 % S == 0) ? (lane & (S - 1)) : (int)(qq % (unsigned)S);
 			sbase = lane;
 			sstride = 32;
-			line = a.data + (long long)outer * tt.outer_stride + qq;
+			line = a.data + coff + (long long)outer * tt.outer_stride + qq;
 			gstride = tt.line_stride;
 		}
 	}
@@ -166,7 +175,8 @@ __device__ __forceinline__ void prefetch_tile(const sweep_args& a, const CUtenso
 	{
 		const long long row0 = w * tt.R;
 		const int rows = (int)min((long long)tt.R, tt.nrows - row0);
-		bulk_prefetch(a.data + row0 * tt.XS, (uint32_t)(rows * tt.XS * sizeof(float)));
+		for (int r = 0; r < rows; r++)
+			bulk_prefetch(a.data + (row0 + r) * tt.XS, (uint32_t)(tt.row_elems * sizeof(float)));
 		return;
 	}
 	const long long outer = w / tt.col_tiles;
@@ -181,12 +191,12 @@ __device__ __forceinline__ void prefetch_tile(const sweep_args& a, const CUtenso
 }
 
 __device__ __forceinline__ void refill(const sweep_args& a, const CUtensorMap& map, const tma_tile& tt, long long wn,
-									   float* stage, uint64_t* bar, long long wstride)
+									   float* stage, uint64_t* bar, long long wstride, long long coff = 0, int crow = 0)
 {
 	if (wn >= tt.slots)
 		return;
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-	issue_tile(a, &map, tt, wn, stage, bar);
+	issue_tile(a, &map, tt, wn, stage, bar, coff, crow);
 	if (tt.prefetch)
 		prefetch_tile(a, &map, tt, wn + wstride);
 }
@@ -604,9 +614,11 @@ __global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constan
 	}
 }
 
-// SLAB (y/z tiles only): 0 a plain sweep; 1 the solve pass of a z-slab, which enters every line
-// with the carries C (left) and X (right) of slab_carry: it always runs the carry folds, from C and
-// X instead of zero, with the tables of precompute_padded_range.
+// SLAB: 0 a plain sweep; 1 the solve pass of a z-slab or of a chunk of longer lines
+// (line_chunk), which enters every line with the carries C (left) and X (right) of slab_carry: it
+// always runs the carry folds, from C and X instead of zero, with the tables of
+// precompute_padded_range; 2 the same for all the equal chunks of longer lines in one launch, the
+// CTAs split among the chunks (tma_tile::chunks).
 // GRAD (z sweep, P > 1): the gradient of the step inside the sweep (grad_fuse); 1 the scalar form,
 // 4 the four-substrate form (S % 4 == 0).
 // PAIR (y/z, plain sweeps only): groups 2u and 2u + 1 share their stages, each slot a pair of tiles
@@ -631,11 +643,19 @@ __global__ void __launch_bounds__(640, 1)
 	const int P = a.vP;
 	const int N = 32 * P;
 	const int NP = N + 1;
+	// SLAB 2: this CTA's chunk, its place among the chunk's CTAs, offsets, tables and carries
+	const int kc = SLAB == 2 ? (int)(blockIdx.x % tt.chunks) : 0;
+	const long long cta = SLAB == 2 ? blockIdx.x / tt.chunks : blockIdx.x;
+	const long long ncta = SLAB == 2 ? gridDim.x / tt.chunks : gridDim.x;
+	const long long coff = SLAB == 2 ? tt.chunk_e0[kc] * tt.e_stride : 0;
+	const int crow = SLAB == 2 ? (int)tt.chunk_e0[kc] : 0;
+	const float* const vtab = SLAB == 2 ? tt.chunk_vtab[kc] : a.vtab;
+	const float* const carry_in = SLAB == 2 ? a.slab_carry + (size_t)kc * 2 * a.slab_lines : a.slab_carry;
 	float* tab = stages0 + (size_t)U * NST * tt.stage_floats;
 	float2* tgtab = reinterpret_cast<float2*>(tab); // [S][NP] (tg, G)
 	float* btab = tab + 2 * S * NP;					// [S][NP] b'
 	float* ctab = btab + S * NP;					// [S]
-	const float* gqtab = a.vtab + (size_t)3 * N * S + S; // [P][S], global
+	const float* gqtab = vtab + (size_t)3 * N * S + S; // [P][S], global
 	const float* tgptab = gqtab + P * S;				 // [P][S], global
 	const float* Gptab = tgptab + P * S;				 // [P][S], global
 	float* carries = tab + staged_table_floats(P, S); // [G][2][P][32]
@@ -670,15 +690,15 @@ __global__ void __launch_bounds__(640, 1)
 	}
 	{
 		// tables: global [v][S] -> shared [S][NP]
-		const float* gb = a.vtab;
-		const float2* gt = reinterpret_cast<const float2*>(a.vtab + (size_t)N * S);
+		const float* gb = vtab;
+		const float2* gt = reinterpret_cast<const float2*>(vtab + (size_t)N * S);
 		for (int t = tid; t < N * S; t += nthr)
 		{
 			const int v = t / S, s = t - v * S;
 			btab[s * NP + v] = gb[t];
 			tgtab[s * NP + v] = gt[t];
 		}
-		const float* gr = a.vtab + (size_t)3 * N * S;
+		const float* gr = vtab + (size_t)3 * N * S;
 		for (int t = tid; t < S; t += nthr)
 			ctab[t] = gr[t];
 		// the virtual fronts read as zeros; the copies never write them
@@ -690,8 +710,8 @@ __global__ void __launch_bounds__(640, 1)
 	__syncthreads(); // also publishes the barrier init
 
 	// slots of this stage owner: sl0, sl0 + slstride, ...; this group's tiles w0, w0 + wstride, ...
-	const long long sl0 = (PAIR ? tt.first / 2 : tt.first) + (long long)blockIdx.x * U + u;
-	const long long slstride = (long long)gridDim.x * U;
+	const long long sl0 = (PAIR ? tt.first / 2 : tt.first) + cta * U + u;
+	const long long slstride = ncta * U;
 	const long long w0 = PAIR ? 2 * sl0 + h : sl0;
 	const long long wstride = PAIR ? 2 * slstride : slstride;
 
@@ -703,7 +723,7 @@ __global__ void __launch_bounds__(640, 1)
 		{
 			const long long sk = sl0 + (long long)k * slstride;
 			if (sk < tt.slots)
-				issue_tile(a, &map, tt, sk, stages + (size_t)k * tt.stage_floats, &bars[k]);
+				issue_tile(a, &map, tt, sk, stages + (size_t)k * tt.stage_floats, &bars[k], coff, crow);
 		}
 	}
 
@@ -738,7 +758,7 @@ __global__ void __launch_bounds__(640, 1)
 		int s, sbase, sstride;
 		{
 			tile_line tl;
-			tl.template locate<ROWS>(a, tt, w, lane);
+			tl.template locate<ROWS>(a, tt, w, lane, coff);
 			s = tl.s;
 			sbase = PAIR ? tl.sbase + 32 * h : tl.sbase;
 			sstride = ROWS ? tl.sstride : (PAIR ? 64 : 32);
@@ -798,7 +818,7 @@ __global__ void __launch_bounds__(640, 1)
 			}
 			if (last_reader)
 				refill(a, map, tt, sl + (long long)NST * slstride, stages + (size_t)st * tt.stage_floats, &bars[st],
-					   wstride);
+					   wstride, coff, crow);
 		}
 		// the barrier also ordered the previous tile's stores: its Dirichlet entries go on top
 		if (DIR && a.dir.items > 0 && it > 0)
@@ -806,14 +826,29 @@ __global__ void __launch_bounds__(640, 1)
 
 		if (SLAB != 0)
 		{
-			// the slab's line: column q of the y*x*s plane
-			const long long q = (w % tt.col_tiles) * 32 + lane;
-			const bool active = q < tt.ncols;
+			// the line's carries: x, row * S + s; y, plane * X * S + column; z, column of the y*x*s
+			// plane
+			long long lid;
+			bool active;
+			if (ROWS)
+			{
+				const int rl = lane / S;
+				const long long row = w * tt.R + rl;
+				active = rl < tt.R && row < tt.nrows;
+				lid = row * S + (lane - rl * S);
+			}
+			else
+			{
+				const long long outer = w / tt.col_tiles;
+				const long long q = (w % tt.col_tiles) * 32 + lane;
+				active = q < tt.ncols;
+				lid = outer * tt.ncols + q;
+			}
 			float C = 0.f, Xc = 0.f;
 			if (active)
 			{
-				C = __ldg(&a.slab_carry[q]);
-				Xc = __ldg(&a.slab_carry[a.slab_lines + q]);
+				C = __ldg(&carry_in[lid]);
+				Xc = __ldg(&carry_in[a.slab_lines + lid]);
 			}
 			// C_k = f^{k-1}_q + gq_{k-1} C_{k-1} from C_0 = the slab's left carry
 			for (int k = 0; k < j; k++)
@@ -873,7 +908,7 @@ __global__ void __launch_bounds__(640, 1)
 			long long w2;
 			asm volatile("mov.b64 %0, %1;" : "=l"(w2) : "l"(w));
 			tile_line tl2;
-			tl2.template locate<ROWS>(a, tt, w2, lane);
+			tl2.template locate<ROWS>(a, tt, w2, lane, coff);
 			if (tl2.active)
 			{
 				if (j > 0 || a.pad == 0)
@@ -962,10 +997,11 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 
 static constexpr int TMA_MAX_P = 16;
 
-// The tensor map of a y sweep (3D over [Z][Y][XS]) or a z sweep (2D over [Z][Y*XS]): boxes of
-// `width` columns x box_h rows.
-static CUresult encode_box(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap& map, int axis, float* dens,
-						   long long X, long long Y, long long Z, long long S, int width, int box_h)
+// The tensor map of a y sweep (3D over [Z][n][XS] from `base`, planes Y * XS apart) or a z sweep
+// (2D over [n][Y*XS]): boxes of `width` columns x box_h rows; n is the line length of the launch
+// (Y or Z, or a chunk's).
+static CUresult encode_box(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap& map, int axis, float* base,
+						   long long X, long long Y, long long Z, long long S, long long n, int width, int box_h)
 {
 	const long long XS = X * S;
 	cuuint64_t dims[3], strides[2];
@@ -975,7 +1011,7 @@ static CUresult encode_box(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap
 	{
 		rank = 3;
 		dims[0] = (cuuint64_t)XS;
-		dims[1] = (cuuint64_t)Y;
+		dims[1] = (cuuint64_t)n;
 		dims[2] = (cuuint64_t)Z;
 		strides[0] = (cuuint64_t)(XS * sizeof(float));
 		strides[1] = (cuuint64_t)(Y * XS * sizeof(float));
@@ -987,12 +1023,12 @@ static CUresult encode_box(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap
 	{
 		rank = 2;
 		dims[0] = (cuuint64_t)(Y * XS);
-		dims[1] = (cuuint64_t)Z;
+		dims[1] = (cuuint64_t)n;
 		strides[0] = (cuuint64_t)(Y * XS * sizeof(float));
 		box[0] = (cuuint32_t)width;
 		box[1] = (cuuint32_t)box_h;
 	}
-	return encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, dens, dims, strides, box, estr,
+	return encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, base, dims, strides, box, estr,
 				  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
 				  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
@@ -1006,9 +1042,17 @@ static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtens
 	if (rc)
 		return rc;
 	const int threads = 32 * a.vP * tt.groups;
-	// one CTA per G tiles (per G / 2 slots of two tiles when paired)
-	const int grid =
+	// one CTA per G tiles (per G / 2 slots of two tiles when paired); chunks in one launch (SLAB 2)
+	// split the resident CTAs evenly among them
+	int grid =
 		persistent_grid(kernel, threads, smem, (tt.items - tt.first + tt.groups - 1) / tt.groups, st->device);
+	if (SLAB == 2)
+	{
+		const int resident = persistent_grid(kernel, threads, smem, 1LL << 40, st->device);
+		const long long per_chunk = std::max<long long>(
+			1, std::min<long long>(resident / tt.chunks, (tt.items + tt.groups - 1) / tt.groups));
+		grid = (int)(per_chunk * tt.chunks);
+	}
 	grad_fuse gf;
 	std::memset(&gf, 0, sizeof(gf));
 	if (GRAD)
@@ -1033,17 +1077,39 @@ static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtens
 
 // tune: launch shape to use (groups 0: the built-in choice).  shapes: when given, nothing is
 // launched; the launch shapes that fit are listed instead.
-int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handled, const sweep_tuning* tune,
+int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a_in, bool& handled, const sweep_tuning* tune,
 					 std::vector<sweep_tuning>* shapes, bool slab_solve, const grad_fuse* gf, long long w_begin,
-					 long long w_end)
+					 long long w_end, const line_chunks* chunk)
 {
 	if (slab_solve && axis != 2)
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "slab passes exist for the z sweep only");
-	if ((w_begin != 0 || w_end >= 0) && (slab_solve || gf))
+	if ((w_begin != 0 || w_end >= 0) && (slab_solve || gf || chunk))
 		return fail(BFVM_ERR_INVALID_ARGUMENT, "a range of tiles is swept only by the plain staged sweeps");
+	if (chunk && (slab_solve || gf))
+		return fail(BFVM_ERR_INVALID_ARGUMENT, "a chunk of the lines is swept by the plain staged sweeps only");
 	handled = false;
 	const long long X = st->grid[0], Y = st->grid[1], Z = st->grid[2], S = st->S;
 	const long long XS = X * S;
+	// the line length of this launch, and for a chunk its field view, tables and carries
+	const long long n_line = chunk ? chunk->len : st->grid[axis];
+	sweep_args a = a_in;
+	float* base = st->dens;
+	if (chunk)
+	{
+		if (chunk->count < 1 || chunk->count > 8)
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "1 to 8 chunks per launch");
+		a.data = st->dens;
+		a.n = (int)chunk->len;
+		a.vtab = chunk->vtab[0];
+		a.vP = chunk->vP;
+		a.pad = chunk->pad;
+		a.slab_carry = chunk->carry;
+		a.slab_lines = chunk->lines;
+		// an x chunk's part of a row is one bulk copy: it must start and end on 16-byte boundaries
+		for (int k = 0; k < chunk->count; k++)
+			if (axis == 0 && ((chunk->e0[k] * S) % 4 != 0 || (chunk->len * S) % 4 != 0))
+				return BFVM_OK;
+	}
 	// shapes the TMA path covers: 16-byte row strides, at most 16 blocks of 32 per line, and for
 	// the x sweep whole rows of at most 32 substrate lines per tile
 	if (!a.vtab || a.vP > TMA_MAX_P || XS % 4 != 0 || (axis == 0 && S > 32) || a.n < 2)
@@ -1056,6 +1122,7 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	std::memset(&tt, 0, sizeof(tt));
 	tt.axis = axis;
 	tt.XS = XS;
+	tt.row_elems = n_line * S;
 	CUtensorMap map;
 	std::memset(&map, 0, sizeof(map));
 	if (axis == 0)
@@ -1066,9 +1133,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		// each staged row: the virtual front rounded up to 16 bytes, the row, and padding so that
 		// lane (r, s) -> r * pitch + s spreads over the banks
 		tt.front = (int)((a.pad * S + 3) / 4 * 4);
-		int bank = (int)(((S - tt.front - XS) % 32 + 64) % 32);
+		int bank = (int)(((S - tt.front - tt.row_elems) % 32 + 64) % 32);
 		bank = (bank + 3) / 4 * 4;
-		tt.row_pitch = tt.front + (int)XS + bank;
+		tt.row_pitch = tt.front + (int)tt.row_elems + bank;
 		tt.stage_floats = (tt.R * tt.row_pitch + 31) / 32 * 32;
 		tt.front_floats = tt.front;
 		tt.front_count = tt.R;
@@ -1076,7 +1143,7 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	}
 	else
 	{
-		const long long n = axis == 1 ? Y : Z;
+		const long long n = n_line;
 		tt.nbox = (int)((n + 255) / 256);
 		tt.box_h = (int)((n + tt.nbox - 1) / tt.nbox);
 		tt.ncols = axis == 1 ? XS : Y * XS;
@@ -1094,7 +1161,9 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.front_floats = a.pad * 32;
 		tt.front_count = 1;
 		tt.front_pitch = 0;
-		if (encode_box(encode, map, axis, st->dens, X, Y, Z, S, 32, tt.box_h) != CUDA_SUCCESS)
+		// (chunks: the map spans the whole line; each CTA's boxes start at its chunk's first row)
+		if (encode_box(encode, map, axis, base, X, Y, Z, S, chunk ? (long long)st->grid[axis] : n, 32, tt.box_h)
+			!= CUDA_SUCCESS)
 			return BFVM_OK; // fall back to the direct kernels
 	}
 	int dev = 0, optin = 0;
@@ -1142,12 +1211,12 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 	// width): the plain y and z sweeps over the whole field, an even number of groups, and for y an
 	// even number of tiles per plane so that no pair spans two planes
 	const int mode = a.dir.items > 0 ? 1 : (a.face_apply ? 2 : 0);
-	const bool pair = (axis == 2 ? st->tma_pairs >= 1 : axis == 1 && st->tma_pairs == 2) && !slab_solve && !gf
+	const bool pair = (axis == 2 ? st->tma_pairs >= 1 : axis == 1 && st->tma_pairs == 2) && !slab_solve && !gf && !chunk
 					  && mode != 1 && w_begin == 0 && w_end < 0 && G % 2 == 0 && (axis == 2 || tt.col_tiles % 2 == 0);
 	if (pair)
 	{
 		CUtensorMap pmap;
-		if (encode_box(encode, pmap, axis, st->dens, X, Y, Z, S, 64, tt.box_h) != CUDA_SUCCESS)
+		if (encode_box(encode, pmap, axis, base, X, Y, Z, S, n_line, 64, tt.box_h) != CUDA_SUCCESS)
 			return BFVM_OK; // the unpaired map was accepted above; a refusal here is not expected
 		map = pmap;
 		tt.pair = 1;
@@ -1172,6 +1241,19 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a, bool& handl
 		tt.slots = tt.items;
 
 	handled = true;
+	if (chunk)
+	{
+		tt.chunks = chunk->count;
+		tt.e_stride = axis == 0 ? S : (axis == 1 ? XS : Y * XS);
+		for (int k = 0; k < chunk->count; k++)
+		{
+			tt.chunk_e0[k] = chunk->e0[k];
+			tt.chunk_vtab[k] = chunk->vtab[k];
+		}
+		return axis == 0   ? launch_tma_variant<true, true, 2>(st, a, map, tt, smem)
+			   : axis == 1 ? launch_tma_variant<false, true, 2>(st, a, map, tt, smem)
+						   : launch_tma_variant<false, false, 2>(st, a, map, tt, smem);
+	}
 	if (axis == 0)
 		return mode == 1   ? launch_tma_variant<true, true, 0, 0, 1>(st, a, map, tt, smem)
 			   : mode == 2 ? launch_tma_variant<true, true, 0, 0, 2>(st, a, map, tt, smem)
