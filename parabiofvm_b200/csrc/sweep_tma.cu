@@ -233,6 +233,28 @@ __device__ __forceinline__ void store_element(float* p, float v)
 		*p = v;
 }
 
+// Stores of elements K.. of a register block at `p` + k * STRIDE floats, with the offsets as
+// immediates of the store instructions (a stride fixed at compile time: the x sweep of SC
+// substrates).
+template <bool NOALLOC, int OFF>
+__device__ __forceinline__ void store_element_at(float* p, float v)
+{
+	if (NOALLOC)
+		asm volatile("st.global.L1::no_allocate.f32 [%0+%2], %1;" ::"l"(p), "f"(v), "n"(OFF * 4) : "memory");
+	else
+		p[OFF] = v;
+}
+
+template <bool NOALLOC, int STRIDE, int M, int K = 0>
+__device__ __forceinline__ void store_block(float* p, const float (&d)[M])
+{
+	if constexpr (K < M)
+	{
+		store_element_at<NOALLOC, K * STRIDE>(p, d[K]);
+		store_block<NOALLOC, STRIDE, M, K + 1>(p, d);
+	}
+}
+
 // The Dirichlet entries of tile w (sweep_args::dir), written by the gthr threads of a warp group.
 // The caller has ordered them after every store of the tile with a barrier of the group, so an
 // entry's value replaces the solved one, as the overwrite after the sweep does.
@@ -627,7 +649,9 @@ __global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constan
 // MODE: 0 the plain sweep, 1 with the per-tile Dirichlet lists (sweep_args::dir), 2 with the face
 // conditions by position (sweep_args::face_apply); separate instances, so the plain sweep holds no
 // registers for either.
-template <bool ROWS, bool NOALLOC, int SLAB, int GRAD, int MODE, bool PAIR>
+// SC (x sweep): the substrate count when the launch fixes it at compile time (0: read at run time),
+// so that the element strides in shared and global memory become immediate offsets.
+template <bool ROWS, bool NOALLOC, int SLAB, int GRAD, int MODE, bool PAIR, int SC = 0>
 __global__ void __launch_bounds__(640, 1)
 	sweep_tma_kernel(const __grid_constant__ sweep_args a, const __grid_constant__ CUtensorMap map,
 					 const __grid_constant__ tma_tile tt, const __grid_constant__ grad_fuse gf)
@@ -761,7 +785,7 @@ __global__ void __launch_bounds__(640, 1)
 			tl.template locate<ROWS>(a, tt, w, lane, coff);
 			s = tl.s;
 			sbase = PAIR ? tl.sbase + 32 * h : tl.sbase;
-			sstride = ROWS ? tl.sstride : (PAIR ? 64 : 32);
+			sstride = ROWS ? (SC ? SC : tl.sstride) : (PAIR ? 64 : 32);
 		}
 		// the line's face conditions, looked up while the tile's copy is in flight
 		// (face_tiles[w] was loaded a tile ahead, so its latency hides behind the previous tile)
@@ -911,7 +935,9 @@ __global__ void __launch_bounds__(640, 1)
 			tl2.template locate<ROWS>(a, tt, w2, lane, coff);
 			if (tl2.active)
 			{
-				if (j > 0 || a.pad == 0)
+				if ((j > 0 || a.pad == 0) && ROWS && SC)
+					store_block<NOALLOC, SC>(tl2.line + (long long)(p - a.pad) * SC, d);
+				else if (j > 0 || a.pad == 0)
 				{
 					float* ptr = tl2.line + (long long)(p - a.pad) * tl2.gstride;
 #pragma unroll
@@ -1033,11 +1059,11 @@ static CUresult encode_box(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap
 				  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
-template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0, int MODE = 0, bool PAIR = false>
+template <bool ROWS, bool NOALLOC, int SLAB = 0, int GRAD = 0, int MODE = 0, bool PAIR = false, int SC = 0>
 static int launch_tma_variant(bfvm_solver* st, const sweep_args& a, const CUtensorMap& map, const tma_tile& tt,
 							  size_t smem, const grad_fuse* gfp = nullptr)
 {
-	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD, MODE, PAIR>;
+	auto kernel = sweep_tma_kernel<ROWS, NOALLOC, SLAB, GRAD, MODE, PAIR, SC>;
 	int rc = set_smem(kernel, smem);
 	if (rc)
 		return rc;
@@ -1257,7 +1283,10 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a_in, bool& ha
 	if (axis == 0)
 		return mode == 1   ? launch_tma_variant<true, true, 0, 0, 1>(st, a, map, tt, smem)
 			   : mode == 2 ? launch_tma_variant<true, true, 0, 0, 2>(st, a, map, tt, smem)
-						   : launch_tma_variant<true, true>(st, a, map, tt, smem);
+						   : (S == 16  ? launch_tma_variant<true, true, 0, 0, 0, false, 16>(st, a, map, tt, smem)
+							  : S == 8 ? launch_tma_variant<true, true, 0, 0, 0, false, 8>(st, a, map, tt, smem)
+							  : S == 4 ? launch_tma_variant<true, true, 0, 0, 0, false, 4>(st, a, map, tt, smem)
+									   : launch_tma_variant<true, true>(st, a, map, tt, smem));
 	if (axis == 1)
 	{
 		if (pair)
