@@ -37,12 +37,13 @@ __device__ __forceinline__ int find_mesh(const long long* __restrict__ first, in
 // Dirichlet overwrite, gradient, secretion: 256-element blocks
 
 __global__ void __launch_bounds__(256) ens_dirichlet_kernel(const ens_inst* __restrict__ inst,
-															 const long long* __restrict__ first, int count,
-															 long long units, int phase)
+															 const long long* __restrict__ first,
+															 const int* __restrict__ umesh, long long units,
+															 int phase)
 {
 	for (long long u = blockIdx.x; u < units; u += gridDim.x)
 	{
-		const int i = find_mesh(first, count, u);
+		const int i = __ldg(&umesh[u]);
 		const ens_inst& m = inst[i];
 		if (phase > m.dims)
 			continue;
@@ -171,11 +172,12 @@ __device__ __forceinline__ void ens_gradient_3d(const ens_inst& m, const float* 
 template <bool ALL3D, int ZU>
 __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const ens_inst* __restrict__ inst,
 																		   const long long* __restrict__ first,
-																		   int count, long long units, int ZC)
+																		   const int* __restrict__ umesh,
+																		   long long units, int ZC)
 {
 	for (long long u = blockIdx.x; u < units; u += gridDim.x)
 	{
-		const int i = find_mesh(first, count, u);
+		const int i = __ldg(&umesh[u]);
 		const ens_inst& m = inst[i];
 		const int S = m.S, X = m.X, Y = m.Y, Z = m.Z, dims = m.dims;
 		const int XS = X * S;
@@ -268,12 +270,12 @@ __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const 
 }
 
 __global__ void __launch_bounds__(256) ens_secretion_kernel(const ens_inst* __restrict__ inst,
-															 const long long* __restrict__ first, int count,
-															 long long units)
+															 const long long* __restrict__ first,
+															 const int* __restrict__ umesh, long long units)
 {
 	for (long long u = blockIdx.x; u < units; u += gridDim.x)
 	{
-		const int i = find_mesh(first, count, u);
+		const int i = __ldg(&umesh[u]);
 		const ens_inst& m = inst[i];
 		const long long t = (u - first[i]) * 256 + threadIdx.x;
 		if (t >= m.AS)
@@ -486,6 +488,8 @@ void ensemble_free(ensemble_plan& plan)
 	device_free(plan.inst);
 	for (auto& f : plan.first)
 		device_free(f);
+	for (auto& u : plan.unit_mesh)
+		device_free(u);
 	for (auto& f : plan.first_h)
 		f.clear();
 	plan.count = 0;
@@ -577,6 +581,16 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes,
 		BFVM_CUDA(cudaMemcpy(plan.first[ph], plan.first_h[ph].data(), (n + 1) * sizeof(long long),
 							 cudaMemcpyHostToDevice));
 	}
+	for (int ph : { (int)ENS_DIRICHLET, (int)ENS_GRADIENT, (int)ENS_SECRETION })
+	{
+		const std::vector<long long>& f = plan.first_h[ph];
+		std::vector<int> um((size_t)std::max<long long>(f[n], 1), 0);
+		for (int i = 0; i < n; i++)
+			std::fill(um.begin() + f[i], um.begin() + f[i + 1], i);
+		if ((st = device_alloc(&plan.unit_mesh[ph], um.size())))
+			return st;
+		BFVM_CUDA(cudaMemcpy(plan.unit_mesh[ph], um.data(), um.size() * sizeof(int), cudaMemcpyHostToDevice));
+	}
 	plan.count = n;
 	return BFVM_OK;
 }
@@ -604,8 +618,8 @@ int ensemble_dirichlet(const ensemble_plan& plan, int phase, cudaStream_t stream
 	const long long units = plan.count ? plan.first_h[ENS_DIRICHLET][plan.count] : 0;
 	if (units == 0)
 		return BFVM_OK;
-	ens_dirichlet_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_DIRICHLET], plan.count,
-																   units, phase);
+	ens_dirichlet_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_DIRICHLET],
+																   plan.unit_mesh[ENS_DIRICHLET], units, phase);
 	return launched("ens_dirichlet_kernel");
 }
 
@@ -613,11 +627,11 @@ template <int ZU>
 static void launch_ens_gradient(const ensemble_plan& plan, long long units, cudaStream_t stream)
 {
 	if (plan.all3d)
-		ens_gradient_kernel<true, ZU><<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_GRADIENT],
-																			   plan.count, units, plan.tune.grad_zc);
+		ens_gradient_kernel<true, ZU><<<element_grid(units), 256, 0, stream>>>(
+			plan.inst, plan.first[ENS_GRADIENT], plan.unit_mesh[ENS_GRADIENT], units, plan.tune.grad_zc);
 	else
 		ens_gradient_kernel<false, ZU><<<element_grid(units), 256, 0, stream>>>(
-			plan.inst, plan.first[ENS_GRADIENT], plan.count, units, plan.tune.grad_zc);
+			plan.inst, plan.first[ENS_GRADIENT], plan.unit_mesh[ENS_GRADIENT], units, plan.tune.grad_zc);
 }
 
 int ensemble_gradient(const ensemble_plan& plan, cudaStream_t stream)
@@ -637,8 +651,8 @@ int ensemble_secretion(const ensemble_plan& plan, cudaStream_t stream)
 	const long long units = plan.count ? plan.first_h[ENS_SECRETION][plan.count] : 0;
 	if (units == 0)
 		return BFVM_OK;
-	ens_secretion_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_SECRETION], plan.count,
-																   units);
+	ens_secretion_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_SECRETION],
+																   plan.unit_mesh[ENS_SECRETION], units);
 	return launched("ens_secretion_kernel");
 }
 

@@ -71,6 +71,9 @@ struct ensemble_plan
 	int count = 0;					 // meshes in the ensemble
 	ens_inst* inst = nullptr;		 // device [count]
 	long long* first[ENS_PHASES] = {}; // device [count + 1]
+	// the mesh of every unit of the per-element phases (Dirichlet, gradient, secretion), so a unit
+	// finds its mesh with one load instead of a binary search over `first`; device [units]
+	int* unit_mesh[ENS_PHASES] = {};
 	std::vector<long long> first_h[ENS_PHASES];
 	int maxP[3] = { 1, 1, 1 };		 // largest vP per axis
 	int maxS = 1;
