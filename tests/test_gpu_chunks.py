@@ -49,3 +49,47 @@ def test_chunked_lines_against_the_ensemble_sweep(grid, S):
     np.testing.assert_array_equal(a.densities(), c.densities())
     for r in (a, b, c):
         r.close()
+
+
+@pytest.mark.parametrize("grid,S,dims", [((2000, 1, 1), 4, 1), ((1100, 40, 1), 4, 2), ((1200, 30, 1), 8, 2)])
+def test_chunked_lines_in_1d_and_2d(grid, S, dims):
+    """1-D and 2-D meshes with long x lines: the chunks' x rows, with Dirichlet 1.0 on substrate 0
+    at both x faces, against the FP32 oracle over a few full steps."""
+    from parabiofvm_b200.workloads import Workload
+
+    rng = np.random.default_rng(sum(grid) + S)
+    w = Workload(dims=dims, bbox_min=(0, 0, 0), bbox_max=(20 * grid[0], 20 * grid[1], 20),
+                 voxel_shape=(20, 20, 20),
+                 diffusion_coefficients=list(np.exp(rng.uniform(np.log(1e3), np.log(1e5), S))),
+                 decay_rates=list(rng.uniform(0.01, 1.0, S)), time_step=0.01, initial_conditions=[0.0] * S)
+    w.densities = rng.uniform(0, 1, grid[0] * grid[1] * S).astype(np.float32)
+    vals = np.zeros(S)
+    conds = np.zeros(S, dtype=bool)
+    vals[0], conds[0] = 1.0, True
+    for is_max in (False, True):
+        w.boundary[(0, is_max)] = (vals, conds)
+    o = make_oracle(w, np.float32)
+    g = gpu_runner(w)
+    o.run_steps(3, 0)
+    g.run_steps(3, 0)
+    assert rel_err(g.densities(), o.densities()) < 1e-5
+    g.close()
+
+
+def test_chunk_length_option():
+    """Lines of 300 cut into chunks of at most 160 (option chunk_elements) agree to rounding with
+    the same lines swept whole, and the option is checked."""
+    from parabiofvm_b200 import BfvmError
+
+    w = _box((300, 60, 40), 8, seed=99)
+    whole = gpu_runner(w)
+    cut = gpu_runner(w)
+    cut.s.set_option("chunk_elements", 160)
+    whole.run_steps(3, 0)
+    cut.run_steps(3, 0)
+    assert rel_err(cut.densities(), whole.densities()) < 1e-5
+    for bad in (63, 513):
+        with pytest.raises(BfvmError):
+            cut.s.set_option("chunk_elements", bad)
+    whole.close()
+    cut.close()
