@@ -196,9 +196,10 @@ int bfvm_synchronize(bfvm_solver* s);
  *   the kernels that read the field directly).  Results agree to rounding either way.
  * - "tma_prefetch" 0/1: each staged-sweep refill also prefetches into L2 the tile after the one it
  *   copies (default 0).  Results are identical either way.
- * - "chunk_elements" N in [64, 512] (default 512): lines longer than N are swept as chunks of at
- *   most N elements by the staged sweep, joined by per-line carries (lines longer than 512 always
- *   are, when the shape allows).  Results agree to rounding with the sweep of whole lines.
+ * - "chunk_elements" N in [64, 512], or 0 (the default, automatic): lines longer than N are swept as
+ *   chunks of at most N elements by the staged sweep, joined by per-line carries; automatic cuts
+ *   lines longer than 512 into chunks of at most 320 along x and 512 along y and z.  Results agree
+ *   to rounding with the sweep of whole lines.
  * - "tma_pairs" 0/1/2: staged sweeps whose two warp groups share each shared-memory stage, which then
  *   holds two adjacent tiles copied as one 64-column box: 1 (the default) the z sweep, 2 the y and z
  *   sweeps, 0 neither.  Results are identical either way.

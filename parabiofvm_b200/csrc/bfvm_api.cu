@@ -1070,8 +1070,8 @@ int bfvm_set_option(bfvm_solver* s, const char* name, int64_t value)
 		s->tma_prefetch = value != 0;
 	else if (n == "chunk_elements")
 	{
-		if (value < 64 || value > 512)
-			return fail(BFVM_ERR_INVALID_ARGUMENT, "chunk_elements must lie in [64, 512]");
+		if (value != 0 && (value < 64 || value > 512))
+			return fail(BFVM_ERR_INVALID_ARGUMENT, "chunk_elements must be 0 (automatic) or lie in [64, 512]");
 		s->chunk_elements = (int)value;
 		free_graphs(s);
 		return rebuild_chunks(s);

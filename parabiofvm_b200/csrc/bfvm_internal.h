@@ -224,8 +224,8 @@ struct bfvm_solver
 	// of `zg_band_rows` y rows (sweep.cu)
 	int xy_band_planes = 0;
 	// the longest chunk of a line that the staged sweep takes as a chunk (chunks.cu): lines longer
-	// than this are cut into chunks (lines of more than 512 elements always are)
-	int chunk_elements = 512;
+	// than this are cut into chunks; 0: automatic (lines beyond 512 elements, x chunks of at most 320)
+	int chunk_elements = 0;
 	int zg_band_rows = 0;
 	int* grad_tile_done = nullptr; // [z tiles] and [1 + z tiles] of the gradient inside the z sweep
 	int* grad_deferred = nullptr;

@@ -170,8 +170,13 @@ int build_chunks(bfvm_solver* s, int axis, const std::vector<float>& bp, const s
 	free_chunks(p);
 	const int n = s->grid[axis];
 	const long long S = s->S, XS = (long long)s->grid[0] * S;
-	const int max_len = std::min(s->chunk_elements, 512); // the staged sweep takes 16 blocks of 32
-	if (axis >= s->dims || n <= max_len || XS % 4 != 0 || (axis == 0 && S > 32) || s->slab_global_z > 0)
+	// chunk_elements 0 (automatic): lines beyond 512 elements (the staged sweep's 16 blocks of 32) in
+	// chunks of at most 320 along x and 512 along y and z, the fastest measured at 640-1024
+	// elements (an x chunk of 512 and 4 substrates is 64 KB of stage); otherwise lines beyond
+	// chunk_elements in chunks of at most that
+	const int max_len = s->chunk_elements > 0 ? s->chunk_elements : (axis == 0 ? 320 : 512);
+	const int longest_whole = s->chunk_elements > 0 ? s->chunk_elements : 512;
+	if (axis >= s->dims || n <= longest_whole || XS % 4 != 0 || (axis == 0 && S > 32) || s->slab_global_z > 0)
 		return BFVM_OK;
 	const int align = axis == 0 ? 4 / std::gcd(4, (int)S) : 1;
 	const std::vector<int> bounds = chunk_bounds(n, align, max_len);

@@ -1276,9 +1276,13 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a_in, bool& ha
 			tt.chunk_e0[k] = chunk->e0[k];
 			tt.chunk_vtab[k] = chunk->vtab[k];
 		}
-		return axis == 0   ? launch_tma_variant<true, true, 2>(st, a, map, tt, smem)
-			   : axis == 1 ? launch_tma_variant<false, true, 2>(st, a, map, tt, smem)
-						   : launch_tma_variant<false, false, 2>(st, a, map, tt, smem);
+		if (axis == 0)
+			return S == 16  ? launch_tma_variant<true, true, 2, 0, 0, false, 16>(st, a, map, tt, smem)
+				   : S == 8 ? launch_tma_variant<true, true, 2, 0, 0, false, 8>(st, a, map, tt, smem)
+				   : S == 4 ? launch_tma_variant<true, true, 2, 0, 0, false, 4>(st, a, map, tt, smem)
+							: launch_tma_variant<true, true, 2>(st, a, map, tt, smem);
+		return axis == 1 ? launch_tma_variant<false, true, 2>(st, a, map, tt, smem)
+						 : launch_tma_variant<false, false, 2>(st, a, map, tt, smem);
 	}
 	if (axis == 0)
 		return mode == 1   ? launch_tma_variant<true, true, 0, 0, 1>(st, a, map, tt, smem)

@@ -88,8 +88,9 @@ def test_chunk_length_option():
     whole.run_steps(3, 0)
     cut.run_steps(3, 0)
     assert rel_err(cut.densities(), whole.densities()) < 1e-5
-    for bad in (63, 513):
+    for bad in (63, 513, -1):
         with pytest.raises(BfvmError):
             cut.s.set_option("chunk_elements", bad)
+    cut.s.set_option("chunk_elements", 0)
     whole.close()
     cut.close()
