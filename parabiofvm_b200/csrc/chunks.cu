@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 
 #include "bfvm_internal.h"
 #include "sweep_common.cuh"
@@ -50,43 +51,80 @@ __device__ __forceinline__ long long line_base(long long l, int S, long long XS,
 	return (l / S) * XS + l % S;
 }
 
-// The end sums of the chunks, one thread per (line, chunk boundary, side): at boundary k (between
-// chunks k and k + 1), side 0 is chunk k's A (its last forward value), side 1 chunk k + 1's B (its
-// first solution), both from zero carries; ex[k][side][lines].  Each sum runs from its smallest
-// weights to its largest (towards the end it belongs to), the order of the slab reduce pass.
-template <int AXIS>
+// The end sums of the chunks, one thread per (V lines, chunk boundary, side): at boundary k
+// (between chunks k and k + 1), side 0 is chunk k's A (its last forward value), side 1 chunk
+// k + 1's B (its first solution), both from zero carries; ex[k][side][lines].  Each sum runs from
+// its smallest weights to its largest (towards the end it belongs to), the order of the slab
+// reduce pass.  V = 4 when S % 4 == 0: four consecutive lines, whose elements (and weights) are
+// four consecutive floats, read as one 16-byte load.
+template <int V>
+__device__ __forceinline__ void load_v(const float* p, float (&x)[V])
+{
+	if constexpr (V == 4)
+	{
+		const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+		x[0] = v.x;
+		x[1] = v.y;
+		x[2] = v.z;
+		x[3] = v.w;
+	}
+	else
+		x[0] = __ldg(p);
+}
+
+template <int AXIS, int V>
 __global__ void __launch_bounds__(256) chunk_sums_kernel(const float* __restrict__ u, const float* __restrict__ rw,
 														  float* __restrict__ ex, long long lines, int S, long long XS,
 														  long long YXS, chunk_meta m)
 {
-	const long long total = lines * 2 * (m.count - 1);
+	const long long groups = lines / V;
+	const long long total = groups * 2 * (m.count - 1);
 	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
 		 t += (long long)gridDim.x * blockDim.x)
 	{
-		const long long l = t % lines;
-		const int bs = (int)(t / lines); // 2 * boundary + side
+		const long long l = (t % groups) * V;
+		const int bs = (int)(t / groups); // 2 * boundary + side
 		const int k = bs >> 1, side = bs & 1;
 		const int s = (int)(l % S);
 		const long long es = AXIS == 2 ? YXS : (AXIS == 1 ? XS : S);
 		const long long base = line_base<AXIS>(l, S, XS, YXS);
-		float acc = 0.f;
+		float acc[V];
+#pragma unroll
+		for (int v = 0; v < V; v++)
+			acc[v] = 0.f;
 		if (side == 0)
 		{
 			const float* wa = rw + m.w_off[k];
 			const float* p = u + base + (long long)m.a_first[k] * es;
-#pragma unroll 16
+#pragma unroll 8
 			for (int i = 0; i < m.na[k]; i++)
-				acc = fmaf(__ldg(&wa[(size_t)i * S + s]), __ldg(p + (long long)i * es), acc);
+			{
+				float x[V], w[V];
+				load_v<V>(p + (long long)i * es, x);
+				load_v<V>(wa + (size_t)i * S + s, w);
+#pragma unroll
+				for (int v = 0; v < V; v++)
+					acc[v] = fmaf(w[v], x[v], acc[v]);
+			}
 		}
 		else
 		{
 			const float* wb = rw + m.w_off[k + 1] + (size_t)m.na[k + 1] * S;
 			const float* p = u + base + (long long)m.b0[k + 1] * es;
-#pragma unroll 16
+#pragma unroll 8
 			for (int i = m.nb[k + 1] - 1; i >= 0; i--)
-				acc = fmaf(__ldg(&wb[(size_t)i * S + s]), __ldg(p + (long long)i * es), acc);
+			{
+				float x[V], w[V];
+				load_v<V>(p + (long long)i * es, x);
+				load_v<V>(wb + (size_t)i * S + s, w);
+#pragma unroll
+				for (int v = 0; v < V; v++)
+					acc[v] = fmaf(w[v], x[v], acc[v]);
+			}
 		}
-		ex[(size_t)bs * lines + l] = acc;
+#pragma unroll
+		for (int v = 0; v < V; v++)
+			ex[(size_t)bs * lines + l + v] = acc[v];
 	}
 }
 
@@ -316,14 +354,25 @@ int launch_chunked_sweep(bfvm_solver* st, int axis, bool& handled)
 	}
 	const long long XS = (long long)st->grid[0] * st->S, YXS = XS * st->grid[1];
 	const int threads = 256;
-	const long long sums = ch.lines * 2 * (ch.count - 1);
+	// four lines per thread when S % 4 == 0 (their elements and weights are 16-byte aligned runs)
+	const int V = st->S % 4 == 0 ? 4 : 1;
+	const long long sums = ch.lines / V * 2 * (ch.count - 1);
 	const unsigned blocks = (unsigned)std::min<long long>((sums + threads - 1) / threads, 148LL * 32);
+	auto sums_kernel = [&](auto axis_tag, auto v_tag) {
+		constexpr int AX = decltype(axis_tag)::value, VV = decltype(v_tag)::value;
+		chunk_sums_kernel<AX, VV><<<blocks, threads, 0, st->stream>>>(st->dens, ch.rw, ch.ex, ch.lines, st->S, XS, YXS, m);
+	};
+	using A0 = std::integral_constant<int, 0>;
+	using A1 = std::integral_constant<int, 1>;
+	using A2 = std::integral_constant<int, 2>;
+	using V1 = std::integral_constant<int, 1>;
+	using V4 = std::integral_constant<int, 4>;
 	if (axis == 0)
-		chunk_sums_kernel<0><<<blocks, threads, 0, st->stream>>>(st->dens, ch.rw, ch.ex, ch.lines, st->S, XS, YXS, m);
+		V == 4 ? sums_kernel(A0(), V4()) : sums_kernel(A0(), V1());
 	else if (axis == 1)
-		chunk_sums_kernel<1><<<blocks, threads, 0, st->stream>>>(st->dens, ch.rw, ch.ex, ch.lines, st->S, XS, YXS, m);
+		V == 4 ? sums_kernel(A1(), V4()) : sums_kernel(A1(), V1());
 	else
-		chunk_sums_kernel<2><<<blocks, threads, 0, st->stream>>>(st->dens, ch.rw, ch.ex, ch.lines, st->S, XS, YXS, m);
+		V == 4 ? sums_kernel(A2(), V4()) : sums_kernel(A2(), V1());
 	int rc = check_launch(st, "chunk_sums_kernel");
 	if (rc)
 		return rc;

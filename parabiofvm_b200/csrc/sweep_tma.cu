@@ -796,6 +796,34 @@ __global__ void __launch_bounds__(640, 1)
 			face_tile_next = w + wstride < tt.items ? __ldg(&a.face_tiles[w + wstride]) : 0;
 			faces = face_code<ROWS>(a, tt, w, lane, s, ftile);
 		}
+		// SLAB: the line's carries, loaded while the tile's copy is in flight.  Lines: x, row * S + s;
+		// y, plane * X * S + column; z, column of the y*x*s plane
+		float slab_c = 0.f, slab_x = 0.f;
+		if (SLAB != 0)
+		{
+			long long lid;
+			bool active;
+			if (ROWS)
+			{
+				const int rl = lane / S;
+				const long long row = w * tt.R + rl;
+				active = rl < tt.R && row < tt.nrows;
+				lid = row * S + (lane - rl * S);
+			}
+			else
+			{
+				const unsigned wu = (unsigned)w, ct = (unsigned)tt.col_tiles;
+				const unsigned outer = tt.axis == 2 ? 0u : wu / ct;
+				const unsigned q = (wu - outer * ct) * 32u + (unsigned)lane;
+				active = q < (unsigned)tt.ncols;
+				lid = (long long)outer * tt.ncols + q;
+			}
+			if (active)
+			{
+				slab_c = __ldg(&carry_in[lid]);
+				slab_x = __ldg(&carry_in[a.slab_lines + lid]);
+			}
+		}
 		const bool ok = mbar_wait(&bars[st], parity, a.wait_limit);
 
 		const float cs = ctab[s];
@@ -850,30 +878,7 @@ __global__ void __launch_bounds__(640, 1)
 
 		if (SLAB != 0)
 		{
-			// the line's carries: x, row * S + s; y, plane * X * S + column; z, column of the y*x*s
-			// plane
-			long long lid;
-			bool active;
-			if (ROWS)
-			{
-				const int rl = lane / S;
-				const long long row = w * tt.R + rl;
-				active = rl < tt.R && row < tt.nrows;
-				lid = row * S + (lane - rl * S);
-			}
-			else
-			{
-				const long long outer = w / tt.col_tiles;
-				const long long q = (w % tt.col_tiles) * 32 + lane;
-				active = q < tt.ncols;
-				lid = outer * tt.ncols + q;
-			}
-			float C = 0.f, Xc = 0.f;
-			if (active)
-			{
-				C = __ldg(&carry_in[lid]);
-				Xc = __ldg(&carry_in[a.slab_lines + lid]);
-			}
+			float C = slab_c, Xc = slab_x;
 			// C_k = f^{k-1}_q + gq_{k-1} C_{k-1} from C_0 = the slab's left carry
 			for (int k = 0; k < j; k++)
 				C = fmaf(__ldg(&gqtab[k * S + s]), C, carry_f[k * 32 + lane]);
