@@ -255,6 +255,43 @@ __device__ __forceinline__ void store_block(float* p, const float (&d)[M])
 	}
 }
 
+// The x sweep of SC substrates (R = 32 / SC rows per tile): the stores of a block transposed
+// across the warp, so that each store instruction writes 128 contiguous bytes of one row (R
+// consecutive elements of its SC substrates) instead of SC * 4 bytes in each of R rows.  Lane
+// L = g * SC + s holds row g, substrate s.  For each run of R elements K .. K + R - 1, a butterfly
+// of log2 R shuffle stages turns lane (g, s)'s values v[m] = element K + m of row g into v[r] =
+// element K + g of row r (substrate s), which row r's store then writes at lane L.  r0 points at
+// element 0 of the block in row 0 plus the lane; rows are XS floats apart; `rows` of them exist.
+template <bool NOALLOC, int SC, int M, int K = 0>
+__device__ __forceinline__ void store_block_rows(float* r0, long long XS, float (&d)[M], int g, int rows)
+{
+	constexpr int R = 32 / SC;
+	if constexpr (K < M)
+	{
+#pragma unroll
+		for (int b = 1; b < R; b <<= 1)
+		{
+			const bool hi = (g & b) != 0;
+#pragma unroll
+			for (int m = 0; m < R; m++)
+				if (!(m & b))
+				{
+					const float send = hi ? d[K + m] : d[K + m + b];
+					const float got = __shfl_xor_sync(0xffffffffu, send, b * SC);
+					if (hi)
+						d[K + m] = got;
+					else
+						d[K + m + b] = got;
+				}
+		}
+#pragma unroll
+		for (int r = 0; r < R; r++)
+			if (r < rows)
+				store_element_at<NOALLOC, K * SC>(r0 + r * XS, d[K + r]);
+		store_block_rows<NOALLOC, SC, M, K + R>(r0, XS, d, g, rows);
+	}
+}
+
 // The Dirichlet entries of tile w (sweep_args::dir), written by the gthr threads of a warp group.
 // The caller has ordered them after every store of the tile with a barrier of the group, so an
 // entry's value replaces the solved one, as the overwrite after the sweep does.
@@ -938,7 +975,16 @@ __global__ void __launch_bounds__(640, 1)
 			asm volatile("mov.b64 %0, %1;" : "=l"(w2) : "l"(w));
 			tile_line tl2;
 			tl2.template locate<ROWS>(a, tt, w2, lane, coff);
-			if (tl2.active)
+			if (ROWS && SC >= 4 && (j > 0 || a.pad == 0))
+			{
+				// every lane takes part in the shuffles; the rows' existence predicates the stores
+				constexpr int R = SC ? 32 / SC : 1;
+				const long long row0 = w2 * R;
+				float* r0 = a.data + coff + row0 * tt.XS + (long long)(p - a.pad) * SC + lane;
+				const int rows = (int)min((long long)R, tt.nrows - row0);
+				store_block_rows<NOALLOC, (SC ? SC : 32)>(r0, tt.XS, d, lane / (SC ? SC : 32), rows);
+			}
+			else if (tl2.active)
 			{
 				if ((j > 0 || a.pad == 0) && ROWS && SC)
 					store_block<NOALLOC, SC>(tl2.line + (long long)(p - a.pad) * SC, d);
