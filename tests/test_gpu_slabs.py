@@ -109,6 +109,23 @@ def test_slabs_match_the_single_solver(planes, bounds):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("planes,bounds", [(100, [0, 37, 70, 100]), (130, [0, 2, 66, 68, 130])])
+def test_slabs_against_the_oracle(planes, bounds):
+    """The split mesh stepped against the FP32 oracle directly (not only against the single CUDA
+    solver): the field at the multi-block bar after three full steps, and the agents' internalized
+    amounts."""
+    from scenarios import make_oracle
+
+    w = _workload(16, planes, 4, 400, seed=planes + 7 * len(bounds))
+    dens, grad, intern = _run(w, bounds, 3)
+    o = make_oracle(w, np.float32)
+    o.run_steps(3, 0)
+    assert rel_err(dens, o.densities()) < 2e-5
+    assert rel_l2(grad, o.gradients()) < 2e-5
+    assert rel_l2(intern, o.internalized().reshape(-1, w.S)) < 2e-5
+
+
+@pytest.mark.gpu
 def test_slab_substrates_not_multiple_of_four_in_x():
     # X * S = 15 * 3: not a multiple of 4, which the staged slab sweep needs
     from parabiofvm_b200 import slabs as sl
