@@ -166,6 +166,51 @@ __device__ __forceinline__ void ens_gradient_3d(const ens_inst& m, const float* 
 	}
 }
 
+// The z march of a 3-D mesh of 4k substrates, four substrates per thread (gradient3d_vec4_kernel of
+// gradient.cu): p4 and g4 point at plane z0 of the thread's float4 column; neighbour offsets in
+// float4s.  The same arithmetic per element as the scalar march, so the same bits.
+__device__ __forceinline__ float4 ens_f4sub_mul(float4 a, float4 b, float f)
+{
+	return make_float4(__fmul_rn(__fsub_rn(a.x, b.x), f), __fmul_rn(__fsub_rn(a.y, b.y), f),
+					   __fmul_rn(__fsub_rn(a.z, b.z), f), __fmul_rn(__fsub_rn(a.w, b.w), f));
+}
+
+__device__ __forceinline__ void ens_gradient_3d_vec4(const ens_inst& m, const float4* __restrict__ p4,
+													 float4* __restrict__ g4, long long plane4, int z0, int z1,
+													 long long xlo, long long xhi, float fx, long long ylo,
+													 long long yhi, float fy)
+{
+	const int Z = m.Z;
+	const long long total4 = plane4 * Z;
+	const bool hasx = m.X > 1, hasy = m.Y > 1;
+	const float bz = m.bgrad[2], cz = m.cgrad[2];
+	const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+	float4 prev = z0 > 0 ? __ldg(p4 - plane4) : zero;
+	float4 cur = __ldg(p4);
+	for (int z = z0; z < z1; z++)
+	{
+		const float4 next = z + 1 < Z ? __ldg(p4 + plane4) : cur;
+		const float4 gx = hasx ? ens_f4sub_mul(__ldg(p4 + xhi), __ldg(p4 + xlo), fx) : zero;
+		const float4 gy = hasy ? ens_f4sub_mul(__ldg(p4 + yhi), __ldg(p4 + ylo), fy) : zero;
+		float4 gz;
+		if (Z == 1)
+			gz = zero;
+		else if (z == 0)
+			gz = ens_f4sub_mul(next, cur, bz);
+		else if (z == Z - 1)
+			gz = ens_f4sub_mul(cur, prev, bz);
+		else
+			gz = ens_f4sub_mul(next, prev, cz);
+		__stcs(g4, gx);
+		__stcs(g4 + total4, gy);
+		__stcs(g4 + 2 * total4, gz);
+		prev = cur;
+		cur = next;
+		p4 += plane4;
+		g4 += plane4;
+	}
+}
+
 // ALL3D: every mesh is 3-D.  The kernel then holds the 3-D march alone, which fits 64 registers, so
 // four CTAs share an SM: twice the loads in flight of the kernel that also holds the 1-D and 2-D
 // forms (held to 128 registers, two CTAs).
@@ -181,6 +226,30 @@ __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const 
 		const ens_inst& m = inst[i];
 		const int S = m.S, X = m.X, Y = m.Y, Z = m.Z, dims = m.dims;
 		const int XS = X * S;
+		if (dims == 3 && (S & 3) == 0)
+		{
+			// four substrates per thread: a unit is 256 float4 columns of the (y, x, s) plane
+			const int S4 = S >> 2, XS4 = XS >> 2;
+			const int cols4 = XS4 * Y;
+			const int ncx = (cols4 + 255) / 256;
+			const int local = (int)(u - first[i]);
+			const int z0 = (local / ncx) * ZC;
+			const int c4 = (local % ncx) * 256 + threadIdx.x;
+			if (c4 >= cols4)
+				continue;
+			const int y = c4 / XS4;
+			const int q4 = c4 - y * XS4;
+			const int x = q4 / S4;
+			const long long plane4 = (long long)cols4;
+			long long xlo, xhi, ylo, yhi;
+			float fx, fy;
+			axis_form(x, X, S4, m.bgrad[0], m.cgrad[0], xlo, xhi, fx);
+			axis_form(y, Y, XS4, m.bgrad[1], m.cgrad[1], ylo, yhi, fy);
+			const long long e4 = (long long)z0 * plane4 + c4;
+			ens_gradient_3d_vec4(m, reinterpret_cast<const float4*>(m.dens) + e4, reinterpret_cast<float4*>(m.grad) + e4,
+								 plane4, z0, min(Z, z0 + ZC), xlo, xhi, fx, ylo, yhi, fy);
+			continue;
+		}
 		const int plane_cols = XS * Y;
 		const int ncx = (plane_cols + 255) / 256;
 		const int local = (int)(u - first[i]);
@@ -559,7 +628,9 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes,
 		units[ENS_SWEEP_X] = R > 0 ? (Y * Z + R - 1) / R : 0;
 		units[ENS_SWEEP_Y] = s->dims >= 2 ? Z * ((XS + 31) / 32) : 0;
 		units[ENS_SWEEP_Z] = s->dims >= 3 ? (Y * XS + 31) / 32 : 0;
-		units[ENS_GRADIENT] = ((XS * Y + 255) / 256) * ((Z + tune.grad_zc - 1) / tune.grad_zc);
+		// 3-D meshes of 4k substrates: 256 float4 columns per unit (ens_gradient_kernel)
+		const long long grad_cols = (s->dims == 3 && S % 4 == 0) ? XS * Y / 4 : XS * Y;
+		units[ENS_GRADIENT] = ((grad_cols + 255) / 256) * ((Z + tune.grad_zc - 1) / tune.grad_zc);
 		units[ENS_SECRETION] = (m.AS + 255) / 256;
 		for (int ph = 0; ph < ENS_PHASES; ph++)
 			plan.first_h[ph][i + 1] = plan.first_h[ph][i] + units[ph];
