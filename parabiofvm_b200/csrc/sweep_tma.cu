@@ -5,8 +5,11 @@
 // lines).  Each warp group keeps up to four tiles in flight, one per shared-memory stage: a stage is
 // refilled with the tile NST ahead as soon as the group holds its current tile in registers, so
 // the HBM reads overlap the whole solve.
-// Results are written straight from registers with coalesced stores.  The Dirichlet overwrites
-// run before and after the sweeps (dirichlet.cu), so this kernel is a pure line solve.
+// Results are written straight from registers with coalesced stores (the x sweep of 16, 8 or 4
+// substrates through a warp transpose, store_block_rows).  The Dirichlet overwrites run before and
+// after the sweeps (dirichlet.cu; as options, the per-tile lists or the face conditions inside
+// the sweeps), so this kernel is otherwise a pure line solve.  Instances also sweep the chunks of
+// longer lines (chunks.cu) and the slabs of a split mesh (slab.cu), entering lines with carries.
 //
 // Lines use the front-padded partition of precompute.cpp: P blocks of exactly 32 elements, the
 // first `pad` of them virtual (b' = 0, read as zeros from a front of the stage that the copies
@@ -674,7 +677,7 @@ __global__ void __launch_bounds__(512) grad_deferred_kernel(const __grid_constan
 }
 
 // SLAB: 0 a plain sweep; 1 the solve pass of a z-slab or of a chunk of longer lines
-// (line_chunk), which enters every line with the carries C (left) and X (right) of slab_carry: it
+// (line_chunks), which enters every line with the carries C (left) and X (right) of slab_carry: it
 // always runs the carry folds, from C and X instead of zero, with the tables of
 // precompute_padded_range; 2 the same for all the equal chunks of longer lines in one launch, the
 // CTAs split among the chunks (tma_tile::chunks).
