@@ -66,6 +66,10 @@ struct tma_tile
 	// TMA box row of 256 bytes per plane); slots = pairs then, else slots = items
 	int pair;
 	long long slots;
+	// y: tile index / col_tiles as (umulhi(ct_magic, w) + w) >> ct_shift (Granlund and Montgomery,
+	// "Division by invariant integers using multiplication", 1994: exact for w < 2^31)
+	unsigned ct_magic;
+	int ct_shift;
 	// the equal chunks of longer lines in one launch (SLAB 2): CTA b sweeps chunk b % chunks, whose
 	// elements start chunk_e0 elements along the line, chunk_e0 * e_stride floats into the field,
 	// with the tables chunk_vtab
@@ -145,7 +149,7 @@ struct tile_line
 			// divisions, several times cheaper than 64-bit ones, and this runs twice per tile
 			// (the z sweep's tiles cover one plane; when S divides 32, a lane's substrate is fixed)
 			const unsigned wu = (unsigned)w, ct = (unsigned)tt.col_tiles;
-			const unsigned outer = tt.axis == 2 ? 0u : wu / ct;
+			const unsigned outer = tt.axis == 2 ? 0u : (__umulhi(tt.ct_magic, wu) + wu) >> tt.ct_shift;
 			const unsigned q = (wu - outer * ct) * 32u + (unsigned)lane;
 			active = q < (unsigned)tt.ncols;
 			const unsigned qq = active ? q : 0u;
@@ -853,7 +857,7 @@ __global__ void __launch_bounds__(640, 1)
 			else
 			{
 				const unsigned wu = (unsigned)w, ct = (unsigned)tt.col_tiles;
-				const unsigned outer = tt.axis == 2 ? 0u : wu / ct;
+				const unsigned outer = tt.axis == 2 ? 0u : (__umulhi(tt.ct_magic, wu) + wu) >> tt.ct_shift;
 				const unsigned q = (wu - outer * ct) * 32u + (unsigned)lane;
 				active = q < (unsigned)tt.ncols;
 				lid = (long long)outer * tt.ncols + q;
@@ -1233,6 +1237,15 @@ int launch_sweep_tma(bfvm_solver* st, int axis, const sweep_args& a_in, bool& ha
 		// far beyond any field that fits the device)
 		if (tt.items >= (1LL << 31) || tt.col_tiles * 32 >= (1LL << 31))
 			return BFVM_OK;
+		// the multiplier and shift that divide a tile index by col_tiles
+		{
+			const unsigned long long d = (unsigned long long)tt.col_tiles;
+			int l = 0;
+			while ((1ULL << l) < d)
+				l++;
+			tt.ct_shift = l;
+			tt.ct_magic = (unsigned)(((1ULL << 32) * ((1ULL << l) - d)) / d + 1);
+		}
 		tt.outer_stride = axis == 1 ? Y * XS : 0;
 		tt.line_stride = axis == 1 ? XS : Y * XS;
 		// stage rows: the virtual front, then the boxes (the last may run past the line end and is
