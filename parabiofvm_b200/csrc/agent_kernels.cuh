@@ -94,6 +94,74 @@ __device__ __forceinline__ void secrete_element(long long t, int S, float* __res
 	dens[dv] = __fadd_rn(__fdiv_rn(__fadd_rn(D, rn), rd), rf);
 }
 
+// The sorted update four substrates at a time (S % 4 == 0): thread t < segments * S / 4 owns a
+// (segment, four substrates) pair and moves every row as 16-byte accesses (secrete_sorted4_kernel of
+// cell.cu, and the ensemble update of batch_kernels.cu).  The arithmetic is secrete_element's, per
+// substrate, in the same order.
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+__device__ __forceinline__ float fused_term(float D, float rn, float rd, float rf)
+{
+	return __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(__fsub_rn(1.f, rd), D), rn), rd), rf);
+}
+
+__device__ __forceinline__ float agent_term(float D, float num, float den, float fac)
+{
+	return __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(-den, D), num), __fadd_rn(1.f, den)), fac);
+}
+
+__device__ __forceinline__ void secrete_sorted4_element(long long t, int S, float* __restrict__ dens,
+														const int* __restrict__ counts,
+														const int* __restrict__ seg_start,
+														const unsigned int* __restrict__ keys,
+														const float* __restrict__ snum, const float* __restrict__ sden,
+														const float* __restrict__ sfac, const float* __restrict__ red_num,
+														const float* __restrict__ red_den,
+														const float* __restrict__ red_fac, float* __restrict__ sintern,
+														float voxel_volume)
+{
+	const int S4 = S >> 2;
+	const int seg = (int)(t / S4);
+	const int s0 = (int)(t - (long long)seg * S4) * 4;
+	const int b = seg_start[seg];
+	const size_t dv = (size_t)keys[b] * S + s0;
+	const size_t r = (size_t)seg * S + s0;
+	const float4 D = ld4(dens + dv);
+	const float4 rn = ld4(red_num + r), rd = ld4(red_den + r), rf = ld4(red_fac + r);
+	if (counts[2] == 0)
+	{
+		// compute_fused: the voxel holds this one agent
+		float* ip = sintern + (size_t)b * S + s0;
+		float4 I = ld4(ip);
+		I.x = __fsub_rn(I.x, __fmul_rn(voxel_volume, fused_term(D.x, rn.x, rd.x, rf.x)));
+		I.y = __fsub_rn(I.y, __fmul_rn(voxel_volume, fused_term(D.y, rn.y, rd.y, rf.y)));
+		I.z = __fsub_rn(I.z, __fmul_rn(voxel_volume, fused_term(D.z, rn.z, rd.z, rf.z)));
+		I.w = __fsub_rn(I.w, __fmul_rn(voxel_volume, fused_term(D.w, rn.w, rd.w, rf.w)));
+		st4(ip, I);
+	}
+	else
+	{
+		// compute_internalized for every agent of the voxel, with its own intermediates
+		const int e = seg_start[seg + 1];
+		for (int p = b; p < e; p++)
+		{
+			const size_t k = (size_t)p * S + s0;
+			const float4 nu = ld4(snum + k), de = ld4(sden + k), fa = ld4(sfac + k);
+			float4 I = ld4(sintern + k);
+			I.x = __fsub_rn(I.x, __fmul_rn(voxel_volume, agent_term(D.x, nu.x, de.x, fa.x)));
+			I.y = __fsub_rn(I.y, __fmul_rn(voxel_volume, agent_term(D.y, nu.y, de.y, fa.y)));
+			I.z = __fsub_rn(I.z, __fmul_rn(voxel_volume, agent_term(D.z, nu.z, de.z, fa.z)));
+			I.w = __fsub_rn(I.w, __fmul_rn(voxel_volume, agent_term(D.w, nu.w, de.w, fa.w)));
+			st4(sintern + k, I);
+		}
+	}
+	st4(dens + dv, make_float4(__fadd_rn(__fdiv_rn(__fadd_rn(D.x, rn.x), rd.x), rf.x),
+							   __fadd_rn(__fdiv_rn(__fadd_rn(D.y, rn.y), rd.y), rf.y),
+							   __fadd_rn(__fdiv_rn(__fadd_rn(D.z, rn.z), rd.z), rf.z),
+							   __fadd_rn(__fdiv_rn(__fadd_rn(D.w, rn.w), rd.w), rf.w)));
+}
+
 __global__ void __launch_bounds__(SCAN_THREADS) scan_tile_kernel(const int* in, int* out, long long n, int* tile_sums);
 __global__ void scan_add_kernel(int* out, long long n, const int* tile_offsets);
 

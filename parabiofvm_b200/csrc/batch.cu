@@ -31,6 +31,9 @@ struct bfvm_batch
 	cudaGraphExec_t graph[2] = { nullptr, nullptr }; // [recompute]
 	std::vector<long long> kernels[2];	 // kernel nodes of each instance in graph[rc]
 	std::vector<long long> epochs[2];	 // instance graph epochs when graph[rc] was captured
+	// whether each instance's agent terms were in sorted order before graph[rc] (what it launches
+	// depends on it) and are after it (the host state advances as the captured step did)
+	std::vector<char> sorted_before[2], sorted_after[2];
 	bfvm::ensemble_plan ens[2];			 // descriptors of the ensemble meshes captured in graph[rc]
 	long long ens_kernels[2] = { 0, 0 }; // ensemble launches in graph[rc] (counted on the first mesh)
 	bool holds_refs = false;			 // the instances count this batch in batch_refs
@@ -52,7 +55,7 @@ static bool batch_graph_current(const bfvm_batch* b, int rc)
 	if (!b->graph[rc])
 		return false;
 	for (size_t i = 0; i < b->inst.size(); i++)
-		if (b->epochs[rc][i] != b->inst[i]->graph_epoch)
+		if (b->epochs[rc][i] != b->inst[i]->graph_epoch || b->sorted_before[rc][i] != (b->inst[i]->ag.sorted ? 1 : 0))
 			return false;
 	return true;
 }
@@ -100,6 +103,10 @@ static int batch_capture(bfvm_batch* b, int rc)
 	const size_t n = b->inst.size();
 	b->kernels[rc].assign(n, 0);
 	b->epochs[rc].assign(n, 0);
+	b->sorted_before[rc].assign(n, 0);
+	b->sorted_after[rc].assign(n, 0);
+	for (size_t i = 0; i < n; i++)
+		b->sorted_before[rc][i] = b->inst[i]->ag.sorted ? 1 : 0;
 	std::vector<bfvm_solver*> members;
 	std::vector<char> in_ens(n, 0);
 	for (size_t i = 0; i < n; i++)
@@ -108,7 +115,9 @@ static int batch_capture(bfvm_batch* b, int rc)
 			members.push_back(b->inst[i]);
 			in_ens[i] = 1;
 		}
-	int st = ensemble_build(b->ens[rc], members, batch_tuning(b, members));
+	// a recompute step rebins every ensemble mesh with agents first (in a side branch), which
+	// leaves its agent terms sorted when it tracks internalized substrates
+	int st = ensemble_build(b->ens[rc], members, batch_tuning(b, members), nullptr, rc == 1);
 	if (st)
 		return st;
 	const ensemble_plan& plan = b->ens[rc];
@@ -136,7 +145,7 @@ static int batch_capture(bfvm_batch* b, int rc)
 		cudaStream_t own = s->stream;
 		s->stream = br;
 		const long long before = s->launches;
-		st = rebin ? rebuild_bins(s) : one_step(s, rc == 1);
+		st = rebin ? prepare_agent_terms(s, true) : one_step(s, rc == 1);
 		b->kernels[rc][i] = s->launches - before;
 		s->launches = before;
 		s->stream = own;
@@ -191,6 +200,11 @@ static int batch_capture(bfvm_batch* b, int rc)
 	}
 	if (g)
 		cudaGraphDestroy(g);
+	for (size_t i = 0; i < n; i++)
+	{
+		b->sorted_after[rc][i] = b->inst[i]->ag.sorted ? 1 : 0;
+		b->inst[i]->ag.sorted = b->sorted_before[rc][i] != 0; // set again after every launch of the graph
+	}
 	if (st)
 		return st;
 	b->ens_kernels[rc] = ens_launches;
@@ -268,15 +282,9 @@ int bfvm_batch_create(bfvm_batch** out, int32_t count, bfvm_solver* const* solve
 	}
 	if (e != cudaSuccess)
 		st = cuda_fail(e, "batch stream and events");
-	// the ensemble kernels use the agent terms in agent order: the instances hand back any sorted
-	// internalized amounts, and their own step graphs (which may use sorted terms) are dropped
+	// the instances' own step graphs are dropped (what they capture depends on batch_refs)
 	for (int32_t i = 0; i < count && !st; i++)
-	{
-		bfvm_solver* s = b->inst[i];
-		st = agents_unsort(s, false);
-		if (!st)
-			st = solver_drop_graphs(s);
-	}
+		st = solver_drop_graphs(b->inst[i]);
 	if (!st)
 	{
 		for (bfvm_solver* s : b->inst)
@@ -305,7 +313,7 @@ int bfvm_batch_destroy(bfvm_batch* b)
 		for (bfvm_solver* s : b->inst)
 		{
 			s->batch_refs--;
-			solver_drop_graphs(s); // stepping alone again may sort the agent terms
+			solver_drop_graphs(s); // what its own step graphs capture depends on batch_refs
 		}
 	ensemble_free(b->ens[0]);
 	ensemble_free(b->ens[1]);
@@ -351,11 +359,40 @@ int bfvm_batch_run_steps(bfvm_batch* b, int32_t steps, int32_t first_step)
 				return st;
 			continue;
 		}
+		if (rc)
+		{
+			// a recompute graph writes sorted agent terms back to agent order before it rebins, so
+			// what it launches depends on the order it finds.  Instances with internalized
+			// substrates whose terms are not sorted yet (agents never binned) are binned and sorted
+			// on their own streams first, so this graph finds the order every later recompute step
+			// finds and is captured once.
+			bool sort_first = false;
+			for (bfvm_solver* s : b->inst)
+				sort_first = sort_first || (s->ag.count > 0 && s->internalized && !s->ag.sorted);
+			if (sort_first)
+			{
+				if ((st = instances_wait_batch(b)))
+					return st;
+				for (bfvm_solver* s : b->inst)
+					if (s->ag.count > 0 && s->internalized && !s->ag.sorted && (st = prepare_agent_terms(s, false)))
+						return st;
+				if ((st = batch_wait_instances(b)))
+					return st;
+			}
+		}
 		if (!batch_graph_current(b, rc) && (st = batch_capture(b, rc)))
 			return st;
 		BFVM_CUDA(cudaGraphLaunch(b->graph[rc], b->stream));
 		for (size_t k = 0; k < b->inst.size(); k++)
-			b->inst[k]->launches += b->kernels[rc][k];
+		{
+			bfvm_solver* s = b->inst[k];
+			s->launches += b->kernels[rc][k];
+			if (s->ag.count > 0)
+			{
+				s->ag.binned = true;
+				s->ag.sorted = b->sorted_after[rc][k] != 0;
+			}
+		}
 		b->inst[0]->launches += b->ens_kernels[rc];
 	}
 	return instances_wait_batch(b);

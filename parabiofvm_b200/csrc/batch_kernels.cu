@@ -347,10 +347,21 @@ __global__ void __launch_bounds__(256) ens_secretion_kernel(const ens_inst* __re
 		const int i = __ldg(&umesh[u]);
 		const ens_inst& m = inst[i];
 		const long long t = (u - first[i]) * 256 + threadIdx.x;
-		if (t >= m.AS)
-			continue;
-		secrete_element(t, m.S, m.dens, m.counts, m.seg_start, m.order, m.keys, m.num, m.den, m.fac, m.red_num,
-						m.red_den, m.red_fac, m.intern, m.internalized, m.voxel_volume);
+		if (m.vec4)
+		{
+			if (t < (long long)__ldg(m.counts) * (m.S >> 2))
+				secrete_sorted4_element(t, m.S, m.dens, m.counts, m.seg_start, m.keys, m.num, m.den, m.fac, m.red_num,
+										m.red_den, m.red_fac, m.intern, m.voxel_volume);
+		}
+		else if (t < m.AS)
+		{
+			if (m.sorted)
+				secrete_element<true>(t, m.S, m.dens, m.counts, m.seg_start, nullptr, m.keys, m.num, m.den, m.fac,
+									  m.red_num, m.red_den, m.red_fac, m.intern, 1, m.voxel_volume);
+			else
+				secrete_element(t, m.S, m.dens, m.counts, m.seg_start, m.order, m.keys, m.num, m.den, m.fac,
+								m.red_num, m.red_den, m.red_fac, m.intern, m.internalized, m.voxel_volume);
+		}
 	}
 }
 
@@ -565,7 +576,7 @@ void ensemble_free(ensemble_plan& plan)
 }
 
 int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes, const ens_tuning& tune,
-				   const std::vector<std::pair<float*, float*>>* buffers)
+				   const std::vector<std::pair<float*, float*>>* buffers, bool rebinned)
 {
 	ensemble_free(plan);
 	plan.tune = tune;
@@ -613,13 +624,16 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes,
 		m.seg_start = a.seg_start;
 		m.order = a.vals;
 		m.keys = a.keys;
-		m.num = a.num;
-		m.den = a.den;
-		m.fac = a.fac;
+		const bool sorted = a.count > 0 && (rebinned ? s->internalized : a.sorted);
+		m.sorted = sorted ? 1 : 0;
+		m.vec4 = sorted && s->S % 4 == 0 ? 1 : 0;
+		m.num = sorted ? a.snum : a.num;
+		m.den = sorted ? a.sden : a.den;
+		m.fac = sorted ? a.sfac : a.fac;
 		m.red_num = a.red_num;
 		m.red_den = a.red_den;
 		m.red_fac = a.red_fac;
-		m.intern = a.intern;
+		m.intern = sorted ? a.sintern : a.intern;
 
 		const long long X = m.X, Y = m.Y, Z = m.Z, S = m.S, XS = X * S;
 		long long units[ENS_PHASES] = { 0, 0, 0, 0, 0, 0 };
@@ -631,7 +645,7 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes,
 		// 3-D meshes of 4k substrates: 256 float4 columns per unit (ens_gradient_kernel)
 		const long long grad_cols = (s->dims == 3 && S % 4 == 0) ? XS * Y / 4 : XS * Y;
 		units[ENS_GRADIENT] = ((grad_cols + 255) / 256) * ((Z + tune.grad_zc - 1) / tune.grad_zc);
-		units[ENS_SECRETION] = (m.AS + 255) / 256;
+		units[ENS_SECRETION] = ((m.vec4 ? m.AS / 4 : m.AS) + 255) / 256;
 		for (int ph = 0; ph < ENS_PHASES; ph++)
 			plan.first_h[ph][i + 1] = plan.first_h[ph][i] + units[ph];
 		for (int d = 0; d < s->dims; d++)

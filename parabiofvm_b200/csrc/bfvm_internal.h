@@ -239,7 +239,7 @@ struct bfvm_solver
 	cudaGraphExec_t step_graph[4] = { nullptr, nullptr, nullptr, nullptr };
 	long long graph_kernels[4] = { 0, 0, 0, 0 }; // kernel nodes per step graph
 	bool graph_sorted_after[4] = { false, false, false, false }; // agent terms sorted after the step
-	int batch_refs = 0; // batches holding this solver: their ensemble kernels use agent order
+	int batch_refs = 0; // batches holding this solver (its own step graphs leave the gradient unfused then)
 	bool graphs_dirty = true;
 	long long graph_epoch = 0; // advances whenever captured buffers or launch shapes may have changed
 
@@ -338,6 +338,8 @@ void free_bulk(bfvm_solver* s);
 int cell_alloc(bfvm_solver* s, int count);
 void cell_free(bfvm_solver* s);
 int launch_secretion(bfvm_solver* s, bool recompute);
+// the binning and the agent terms' order a secretion update needs (a rebinning when `recompute`)
+int prepare_agent_terms(bfvm_solver* s, bool recompute);
 int agents_unsort(bfvm_solver* s, bool keep_sorted); // internalized amounts back to agent order (cell.cu)
 int solver_drop_graphs(bfvm_solver* s);			  // after queued work, drop the step graphs (bfvm_api.cu)
 int agents_resort_internalized(bfvm_solver* s);	  // stored internalized amounts into sorted order

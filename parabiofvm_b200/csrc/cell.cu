@@ -344,23 +344,9 @@ __global__ void release_kernel(int index, int S, int dims, const float* __restri
 	intern[k] = 0.f;
 }
 
-// The sorted update four substrates at a time (S % 4 == 0): one thread owns a (segment, four
-// substrates) pair and moves every row as 16-byte accesses.  Its threads stride over the segments
-// the binning found (counts[0], read on the device), so no thread is launched for agents that
-// share a voxel.  The arithmetic is secrete_element's, per substrate, in the same order.
-__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
-__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
-
-__device__ __forceinline__ float fused_term(float D, float rn, float rd, float rf)
-{
-	return __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(__fsub_rn(1.f, rd), D), rn), rd), rf);
-}
-
-__device__ __forceinline__ float agent_term(float D, float num, float den, float fac)
-{
-	return __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(-den, D), num), __fadd_rn(1.f, den)), fac);
-}
-
+// The sorted update four substrates at a time (S % 4 == 0; secrete_sorted4_element).  Its threads
+// stride over the segments the binning found (counts[0], read on the device), so no thread is
+// launched for agents that share a voxel.
 __global__ void __launch_bounds__(256) secrete_sorted4_kernel(int S, float* __restrict__ dens,
 															  const int* __restrict__ counts,
 															  const int* __restrict__ seg_start,
@@ -372,50 +358,10 @@ __global__ void __launch_bounds__(256) secrete_sorted4_kernel(int S, float* __re
 															  const float* __restrict__ red_fac,
 															  float* __restrict__ sintern, float voxel_volume)
 {
-	const int S4 = S >> 2;
-	const long long n = (long long)counts[0] * S4;
-	const bool conflict = counts[2] != 0;
+	const long long n = (long long)counts[0] * (S >> 2);
 	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-	{
-		const int seg = (int)(t / S4);
-		const int s0 = (int)(t - (long long)seg * S4) * 4;
-		const int b = seg_start[seg];
-		const size_t dv = (size_t)keys[b] * S + s0;
-		const size_t r = (size_t)seg * S + s0;
-		const float4 D = ld4(dens + dv);
-		const float4 rn = ld4(red_num + r), rd = ld4(red_den + r), rf = ld4(red_fac + r);
-		if (!conflict)
-		{
-			// compute_fused: the voxel holds this one agent
-			float* ip = sintern + (size_t)b * S + s0;
-			float4 I = ld4(ip);
-			I.x = __fsub_rn(I.x, __fmul_rn(voxel_volume, fused_term(D.x, rn.x, rd.x, rf.x)));
-			I.y = __fsub_rn(I.y, __fmul_rn(voxel_volume, fused_term(D.y, rn.y, rd.y, rf.y)));
-			I.z = __fsub_rn(I.z, __fmul_rn(voxel_volume, fused_term(D.z, rn.z, rd.z, rf.z)));
-			I.w = __fsub_rn(I.w, __fmul_rn(voxel_volume, fused_term(D.w, rn.w, rd.w, rf.w)));
-			st4(ip, I);
-		}
-		else
-		{
-			// compute_internalized for every agent of the voxel, with its own intermediates
-			const int e = seg_start[seg + 1];
-			for (int p = b; p < e; p++)
-			{
-				const size_t k = (size_t)p * S + s0;
-				const float4 nu = ld4(snum + k), de = ld4(sden + k), fa = ld4(sfac + k);
-				float4 I = ld4(sintern + k);
-				I.x = __fsub_rn(I.x, __fmul_rn(voxel_volume, agent_term(D.x, nu.x, de.x, fa.x)));
-				I.y = __fsub_rn(I.y, __fmul_rn(voxel_volume, agent_term(D.y, nu.y, de.y, fa.y)));
-				I.z = __fsub_rn(I.z, __fmul_rn(voxel_volume, agent_term(D.z, nu.z, de.z, fa.z)));
-				I.w = __fsub_rn(I.w, __fmul_rn(voxel_volume, agent_term(D.w, nu.w, de.w, fa.w)));
-				st4(sintern + k, I);
-			}
-		}
-		st4(dens + dv, make_float4(__fadd_rn(__fdiv_rn(__fadd_rn(D.x, rn.x), rd.x), rf.x),
-								   __fadd_rn(__fdiv_rn(__fadd_rn(D.y, rn.y), rd.y), rf.y),
-								   __fadd_rn(__fdiv_rn(__fadd_rn(D.z, rn.z), rd.z), rf.z),
-								   __fadd_rn(__fdiv_rn(__fadd_rn(D.w, rn.w), rd.w), rf.w)));
-	}
+		secrete_sorted4_element(t, S, dens, counts, seg_start, keys, snum, sden, sfac, red_num, red_den, red_fac, sintern,
+								voxel_volume);
 }
 
 // The same release with the internalized amounts in sorted order: agent `index` is at row rank[index].
@@ -620,16 +566,17 @@ int agents_resort_internalized(bfvm_solver* s)
 	return permute_rows(s, a.intern, a.sintern, true);
 }
 
-// A solver stepping alone with internalized substrates runs secretion on sorted agent terms: a
+// With internalized substrates the secretion runs on sorted agent terms, alone or in a batch: a
 // rebinning sorts them (after writing the internalized amounts back to agent order with the old
-// order), and a solver binned but not sorted (a batch stepped it) sorts them once.  Solvers held
-// by a batch, and solvers without internalized substrates, keep agent order.
-int launch_secretion(bfvm_solver* s, bool recompute)
+// order), and a solver binned but not sorted (stored amounts of an unchanged count) sorts them
+// once.  Solvers without internalized substrates keep agent order (only the per-voxel sums are
+// read then).
+int prepare_agent_terms(bfvm_solver* s, bool recompute)
 {
 	agent_state& a = s->ag;
 	if (a.count == 0)
 		return BFVM_OK;
-	const bool use_sorted = s->internalized && s->batch_refs == 0;
+	const bool use_sorted = s->internalized;
 	int st;
 	if (recompute || !a.binned || (a.sorted && !use_sorted))
 	{
@@ -651,6 +598,17 @@ int launch_secretion(bfvm_solver* s, bool recompute)
 			return st;
 		a.sorted = true;
 	}
+	return BFVM_OK;
+}
+
+int launch_secretion(bfvm_solver* s, bool recompute)
+{
+	agent_state& a = s->ag;
+	if (a.count == 0)
+		return BFVM_OK;
+	int st;
+	if ((st = prepare_agent_terms(s, recompute)))
+		return st;
 	const long long AS = (long long)a.count * s->S;
 	const float vv = (float)(s->voxel[0] * s->voxel[1] * s->voxel[2]);
 	if (a.sorted && s->S % 4 == 0)

@@ -28,9 +28,12 @@ struct ens_inst
 	const long long* dir_idx; // single elements
 	const float* dir_val;
 	long long dir_count;
-	// secretion (the binning of the mesh's cell solver)
+	// secretion (the binning of the mesh's cell solver).  sorted: num/den/fac/intern are the agent
+	// terms in the binning's sorted order (agent_state::snum ...), else in agent order; vec4: sorted
+	// with S % 4 == 0, a unit is 256 (segment, four substrates) pairs
 	long long AS; // agents * S (0 without agents)
 	int internalized;
+	int sorted, vec4;
 	float voxel_volume;
 	const int* counts;
 	const int* seg_start;
@@ -86,9 +89,11 @@ struct ensemble_plan
 // at most 32 substrates.
 bool ensemble_eligible(const bfvm_solver* s);
 // buffers: when given, the field and gradient buffers of each mesh instead of the solvers' own
-// (the autotuner times candidates on scratch copies)
+// (the autotuner times candidates on scratch copies).  rebinned: the secretion update runs after
+// a rebinning of every mesh with agents (prepare_agent_terms), so it finds their agent terms in
+// the order that leaves (sorted with internalized substrates) rather than in today's.
 int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes, const ens_tuning& tune = ens_tuning(),
-				   const std::vector<std::pair<float*, float*>>* buffers = nullptr);
+				   const std::vector<std::pair<float*, float*>>* buffers = nullptr, bool rebinned = false);
 void ensemble_free(ensemble_plan& plan);
 // One phase for every mesh of the plan, on `stream`.  `dirichlet_phase` k applies the overwrite to
 // meshes with k <= dims (before sweep k, or after the last sweep).

@@ -19,6 +19,7 @@ def _ensemble():
         synthetic(33, 8, 500, seed=5, clustered=True, sigma=40.0, internalized=False),
         synthetic(64, 1, 100, seed=6),
         synthetic(48, 3, 0, seed=7, dims=1),
+        synthetic(40, 8, 60, seed=8, interior_fraction=0.01),
     ]
     return ws
 
@@ -84,9 +85,9 @@ def test_batch_follows_changes_to_an_instance():
 
 
 def test_solver_alone_then_batched_then_alone():
-    """A solver stepping alone keeps its agent terms in the binning's sorted order; joining a batch
-    hands them back in agent order for the ensemble kernels, and leaving it sorts them again.  Every
-    hand-over keeps the results bit for bit those of a solver that only ever stepped alone."""
+    """A solver with internalized substrates keeps its agent terms in the binning's sorted order,
+    alone and in a batch (whose ensemble update reads them sorted too).  Joining and leaving a batch
+    keeps the results bit for bit those of a solver that only ever stepped alone."""
     ws = _ensemble()[:3]
     solvers = [make_solver(w) for w in ws]
     ref = make_solver(ws[0])
@@ -130,4 +131,42 @@ def test_autotuned_batch_matches_each_solver_alone():
             np.testing.assert_array_equal(g, a, err_msg=f"instance {i}")
     b.close()
     for s in solvers:
+        s.close()
+
+
+def test_batch_members_changed_between_steps():
+    """Between batch steps, two members release an agent's internalized substrates (found through
+    the agent's rank while the terms are sorted) and a third has its internalized amounts loaded
+    and stored back, across a recompute step that rebins and sorts again: the members end where
+    solvers stepped alone with the same calls end, bit for bit.  Covers the four-substrate sorted
+    update with and without voxels shared by agents (meshes 2 and 7)."""
+    ws = _ensemble()
+    solvers = [make_solver(w) for w in ws]
+    ref = [make_solver(w) for w in ws]
+    b = Batch(solvers)
+
+    def changes(group):
+        group[2].release(3)
+        group[7].release(11)
+        a = ws[1].agents
+        amounts = group[1].load_internalized().copy()
+        group[1].store_agents(a.secretion_rates, a.saturation_densities, a.uptake_rates, a.net_export_rates,
+                              amounts, a.fraction_released, a.volumes, a.positions)
+
+    b.run_steps(6, 0)
+    b.synchronize()
+    changes(solvers)
+    b.run_steps(8, 6)
+    b.synchronize()
+    for r in ref:
+        r.run_steps(6, 0)
+    changes(ref)
+    for r in ref:
+        r.run_steps(8, 6)
+        r.synchronize()
+    for i, (s, r) in enumerate(zip(solvers, ref)):
+        for g, e in zip(_state(s), _state(r)):
+            np.testing.assert_array_equal(g, e, err_msg=f"instance {i}")
+    b.close()
+    for s in solvers + ref:
         s.close()
