@@ -117,7 +117,9 @@ static int batch_capture(bfvm_batch* b, int rc)
 		}
 	// a recompute step rebins every ensemble mesh with agents first (in a side branch), which
 	// leaves its agent terms sorted when it tracks internalized substrates
-	int st = ensemble_build(b->ens[rc], members, batch_tuning(b, members), nullptr, rc == 1);
+	int st = ensemble_build(b->ens[rc], members, batch_tuning(b, members), nullptr, rc == 1, true);
+	if (!st)
+		st = ensemble_build_dirichlet(b->ens[rc]);
 	if (st)
 		return st;
 	const ensemble_plan& plan = b->ens[rc];
@@ -164,14 +166,21 @@ static int batch_capture(bfvm_batch* b, int rc)
 		int maxdims = 0;
 		for (bfvm_solver* m : members)
 			maxdims = std::max(maxdims, m->dims);
+		// the overwrites after the sweeps launch nothing when the sweeps write every condition
+		auto overwrite = [&](int phase) {
+			const int r = ensemble_dirichlet(plan, phase, b->stream);
+			if (!r && ensemble_dirichlet_entries(plan, phase) > 0)
+				ens_launches++;
+			return r;
+		};
 		for (int axis = 0; axis < maxdims && !st; axis++)
 		{
-			if ((st = count(ensemble_dirichlet(plan, axis, b->stream))))
+			if ((st = overwrite(axis)))
 				break;
 			st = count(ensemble_sweep(plan, axis, b->stream));
 		}
 		if (!st)
-			st = count(ensemble_dirichlet(plan, maxdims, b->stream));
+			st = overwrite(maxdims);
 		if (!st)
 			st = count(ensemble_gradient(plan, b->stream));
 		// the secretion update waits for the rebinning branches
@@ -438,7 +447,7 @@ int bfvm_batch_autotune(bfvm_batch* b, int32_t* choices)
 		ensemble_plan plan;
 		// device time of `phase` under tuning t: one launch to warm up, the mean of three
 		auto time_phase = [&](const ens_tuning& t, auto phase, float& ms) -> int {
-			int r = ensemble_build(plan, members, t, &bufs);
+			int r = ensemble_build(plan, members, t, &bufs, false, true);
 			if (!r)
 				r = phase(plan);
 			for (int k = 0; k < 3 && !r; k++)

@@ -1,8 +1,10 @@
 // Ensemble kernels: one launch per phase of the step (Dirichlet overwrite, the sweeps, gradient,
 // secretion update) for every mesh of a batch.  Each phase has a prefix list of work units over the
-// meshes; a CTA maps its unit to the mesh that owns it (binary search of the prefix list) and runs
-// that mesh's arithmetic, the same as the mesh's own kernels, so a batch reproduces every mesh
-// stepped alone bit for bit.
+// meshes; a CTA maps its unit to the mesh that owns it (a unit -> mesh table, or for the sweeps a
+// binary search of the prefix list when a CTA's run of tiles enters the next mesh) and runs that
+// mesh's arithmetic, the same as the mesh's own kernels, so a batch reproduces every mesh stepped
+// alone bit for bit.  The Dirichlet overwrites run on flat lists of (address, value), and the
+// sweeps write the face conditions of the overwrites that follow them where a mesh allows it.
 //
 // The sweep kernel reads its lines straight from global memory (coalesced 128-byte rows, 32
 // independent loads per thread) rather than through TMA stages: ensemble meshes are small, and
@@ -36,23 +38,82 @@ __device__ __forceinline__ int find_mesh(const long long* __restrict__ first, in
 // ------------------------------------------------------------------------------------------------
 // Dirichlet overwrite, gradient, secretion: 256-element blocks
 
-__global__ void __launch_bounds__(256) ens_dirichlet_kernel(const ens_inst* __restrict__ inst,
-															 const long long* __restrict__ first,
-															 const int* __restrict__ umesh, long long units,
-															 int phase)
+// Dirichlet overwrite: the members' lists are gathered once per plan into flat lists of
+// (address, value), so the overwrite is one load of an entry and one store, with no lookup of the
+// entry's mesh.  Every position occurs once per mesh list, so the order of the stores does not
+// matter.
+
+// one mesh's list to gather: its runs of four and single elements and their place in the flat list
+struct ens_dir_src
+{
+	float* dens;
+	const long long* qidx;
+	const float4* qval;
+	long long qcount;
+	const long long* idx;
+	const float* val;
+	long long count;
+	long long qflat, sflat;
+};
+
+// unit u (256 entries) of the list of mesh umesh[u], whose units start at ufirst[mesh]
+__global__ void __launch_bounds__(256) ens_dirichlet_flatten_kernel(const ens_dir_src* __restrict__ src,
+																	 const long long* __restrict__ ufirst,
+																	 const int* __restrict__ umesh, long long units,
+																	 float4** __restrict__ qptr, float4* __restrict__ qval,
+																	 float** __restrict__ sptr, float* __restrict__ sval)
 {
 	for (long long u = blockIdx.x; u < units; u += gridDim.x)
 	{
-		const int i = __ldg(&umesh[u]);
-		const ens_inst& m = inst[i];
-		if (phase > m.dims)
-			continue;
-		const long long e = (u - first[i]) * 256 + threadIdx.x;
-		if (e < m.dir_qcount)
-			*reinterpret_cast<float4*>(m.dens + __ldg(&m.dir_qidx[e])) = __ldg(&m.dir_qval[e]);
-		else if (e - m.dir_qcount < m.dir_count)
-			m.dens[__ldg(&m.dir_idx[e - m.dir_qcount])] = __ldg(&m.dir_val[e - m.dir_qcount]);
+		const int i = umesh[u];
+		const ens_dir_src& m = src[i];
+		const long long e = (u - ufirst[i]) * 256 + threadIdx.x;
+		if (e < m.qcount)
+		{
+			qptr[m.qflat + e] = reinterpret_cast<float4*>(m.dens + m.qidx[e]);
+			qval[m.qflat + e] = m.qval[e];
+		}
+		else if (e - m.qcount < m.count)
+		{
+			const long long k = e - m.qcount;
+			sptr[m.sflat + k] = m.dens + m.idx[k];
+			sval[m.sflat + k] = m.val[k];
+		}
 	}
+}
+
+// *ptr[t] = val[t] for t < n, grid-stride, four entries per thread loaded before their stores
+template <typename V>
+__device__ __forceinline__ void scatter_entries(V* const* __restrict__ ptr, const V* __restrict__ val, long long n)
+{
+	const long long T = (long long)gridDim.x * blockDim.x;
+	long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	const unsigned long long* praw = reinterpret_cast<const unsigned long long*>(ptr);
+	for (; t + 3 * T < n; t += 4 * T)
+	{
+		V* p[4];
+		V v[4];
+#pragma unroll
+		for (int k = 0; k < 4; k++)
+		{
+			p[k] = reinterpret_cast<V*>(__ldg(&praw[t + k * T]));
+			v[k] = __ldg(&val[t + k * T]);
+		}
+#pragma unroll
+		for (int k = 0; k < 4; k++)
+			*p[k] = v[k];
+	}
+	for (; t < n; t += T)
+		*reinterpret_cast<V*>(__ldg(&praw[t])) = __ldg(&val[t]);
+}
+
+__global__ void __launch_bounds__(256) ens_dirichlet_kernel(float4* const* __restrict__ qptr,
+															 const float4* __restrict__ qval, long long nq,
+															 float* const* __restrict__ sptr,
+															 const float* __restrict__ sval, long long ns)
+{
+	scatter_entries(qptr, qval, nq);
+	scatter_entries(sptr, sval, ns);
 }
 
 // central differences (gradient.cu); output layouts 1D [x][s][1], 2D [y][x][s][2], 3D [3][z][y][x][s].
@@ -368,13 +429,18 @@ __global__ void __launch_bounds__(256) ens_secretion_kernel(const ens_inst* __re
 // ------------------------------------------------------------------------------------------------
 // sweeps: one unit = one tile of 32 lines (the tiles of sweep_tma.cu), blockDim = (32, maxP)
 
-// staged tables of one mesh and axis: (tg, G) pairs and b' as [S][NP], NP = 32P + 1, then c [S]
-__device__ __forceinline__ void ens_stage_tables(const float* __restrict__ vtab, int P, int S, float* tab)
+// staged tables of one mesh and axis: (tg, G) pairs and b' as [S][NP], NP = 32P + 1, then c [S],
+// the face bits [S] (0 where the sweeps write no faces) and the face values [6][S]
+__device__ __forceinline__ void ens_stage_tables(const ens_inst& m, int AXIS, float* tab)
 {
+	const float* __restrict__ vtab = m.vtab[AXIS];
+	const int P = m.vP[AXIS], S = m.S;
 	const int N = 32 * P, NP = N + 1;
 	float2* tgtab = reinterpret_cast<float2*>(tab);
 	float* btab = tab + 2 * S * NP;
 	float* ctab = btab + S * NP;
+	int* fbits = reinterpret_cast<int*>(ctab + S);
+	float* fvals = ctab + 2 * S;
 	const float2* gt = reinterpret_cast<const float2*>(vtab + (size_t)N * S);
 	const int nthr = blockDim.x * blockDim.y;
 	const int tid = threadIdx.x + blockDim.x * threadIdx.y;
@@ -385,7 +451,64 @@ __device__ __forceinline__ void ens_stage_tables(const float* __restrict__ vtab,
 		tgtab[s * NP + v] = __ldg(&gt[t]);
 	}
 	for (int t = tid; t < S; t += nthr)
+	{
 		ctab[t] = __ldg(&vtab[(size_t)3 * N * S + t]);
+		fbits[t] = m.faces ? __ldg(&m.face_bits[t]) : 0;
+	}
+	for (int t = tid; t < 6 * S; t += nthr)
+		fvals[t] = m.faces ? __ldg(&m.face_vals[t]) : 0.f;
+}
+
+// The face conditions of the line along AXIS at coordinates (cx, cy, cz) (AXIS's own is unused),
+// for substrate bits `mb` (face_code of sweep_tma.cu): bits 2 and 3, the faces of AXIS at the
+// line's first and last element; bits 0-1, 1 when a face of an earlier axis covers the whole line
+// (the ends then take AXIS's faces), 2 when a face of a later axis does (it wins everywhere); bits
+// 4+, that face, the latest of its kind (later faces win where faces meet).
+template <int AXIS>
+__device__ __forceinline__ int ens_face_code(int mb, int cx, int cy, int cz, int X, int Y, int Z)
+{
+	int code = ((mb >> (2 * AXIS)) & 3) << 2;
+	int lb = 0;
+	if (AXIS != 0)
+		lb |= (cx == 0 ? 1 : 0) | (cx == X - 1 ? 2 : 0);
+	if (AXIS != 1)
+		lb |= (cy == 0 ? 4 : 0) | (cy == Y - 1 ? 8 : 0);
+	if (AXIS != 2)
+		lb |= (cz == 0 ? 16 : 0) | (cz == Z - 1 ? 32 : 0);
+	lb &= mb;
+	const int after = lb >> (2 * AXIS + 2), before = lb & ((1 << (2 * AXIS)) - 1);
+	if (after)
+		code |= 2 | ((31 - __clz(after) + 2 * AXIS + 2) << 4);
+	else if (before)
+		code |= 1 | ((31 - __clz(before)) << 4);
+	return code;
+}
+
+// Store the face conditions over block j of a line whose solved values were just stored (the same
+// thread stores both, so these win): the line's first element is element `pad` of block 0, its
+// last element 31 of block P - 1 (apply_faces of sweep_tma.cu, here after the stores, so the
+// solved block need not stay in registers).
+template <int AXIS>
+__device__ __forceinline__ void ens_store_faces(float* line, int stride, int code, const float* fvals, int S, int s,
+												int j, int P, int pad)
+{
+	const int lk = code & 3;
+	if (lk != 0)
+	{
+		const float lv = fvals[(code >> 4) * S + s];
+		for (int k = 0; k < 32; k++)
+		{
+			const int r = 32 * j + k - pad;
+			if (r >= 0)
+				line[r * stride] = lv;
+		}
+		if (lk == 2)
+			return;
+	}
+	if ((code & 4) && j == 0)
+		line[0] = fvals[(2 * AXIS) * S + s];
+	if ((code & 8) && j == P - 1)
+		line[(32 * P - 1 - pad) * stride] = fvals[(2 * AXIS + 1) * S + s];
 }
 
 // x tiles: rows [row0, row0 + rows) of mesh m, contiguous in the field
@@ -433,7 +556,7 @@ __global__ void __launch_bounds__(MINB == 0 ? 1024 : 512, MINB == 0 ? 1 : MINB) 
 			first_i = __ldg(&first[i]);
 			first_next = __ldg(&first[i + 1]);
 			__syncthreads(); // the previous mesh's tables are no longer read
-			ens_stage_tables(inst[i].vtab[AXIS], inst[i].vP[AXIS], inst[i].S, tab);
+			ens_stage_tables(inst[i], AXIS, tab);
 			__syncthreads();
 			cur = i;
 		}
@@ -540,6 +663,35 @@ __global__ void __launch_bounds__(MINB == 0 ? 1024 : 512, MINB == 0 ? 1 : MINB) 
 					if (r >= 0)
 						line[r * stride] = d[k];
 				}
+				// the face conditions of the overwrite after this sweep (meshes with ens_inst::faces)
+				const int mb = reinterpret_cast<const int*>(ctab + S)[s];
+				if (mb != 0)
+				{
+					int cx = 0, cy = 0, cz = 0;
+					if (AXIS == 0)
+					{
+						const int row = local * (32 / S) + lane / S;
+						cz = row / m.Y;
+						cy = row - cz * m.Y;
+					}
+					else if (AXIS == 1)
+					{
+						// line = dens + z * XS * Y + x * S + s
+						const int off = (int)(line - m.dens);
+						const int plane = XS * m.Y;
+						cz = off / plane;
+						cx = (off - cz * plane) / S;
+					}
+					else
+					{
+						const int q = local * 32 + lane;
+						cy = q / XS;
+						cx = (q - cy * XS) / S;
+					}
+					const int code = ens_face_code<AXIS>(mb, cx, cy, cz, m.X, m.Y, m.Z);
+					if (code != 0)
+						ens_store_faces<AXIS>(line, stride, code, ctab + 2 * S, S, s, j, P, pad);
+				}
 			}
 		}
 		__syncthreads(); // carries of this tile read before the next tile writes them
@@ -561,7 +713,8 @@ bool ensemble_eligible(const bfvm_solver* s)
 	return s->S <= 32 && s->V * s->S < (1LL << 31);
 }
 
-static size_t staged_floats(int P, int S) { return 3 * (size_t)S * (32 * P + 1) + S; }
+// the staged tables of ens_stage_tables: (tg, G) and b' as [S][NP], c [S], face bits [S], face values [6][S]
+static size_t staged_floats(int P, int S) { return 3 * (size_t)S * (32 * P + 1) + 8 * (size_t)S; }
 
 void ensemble_free(ensemble_plan& plan)
 {
@@ -572,11 +725,21 @@ void ensemble_free(ensemble_plan& plan)
 		device_free(u);
 	for (auto& f : plan.first_h)
 		f.clear();
+	for (ensemble_plan::flat_list& l : plan.dir)
+	{
+		device_free(l.qptr);
+		device_free(l.qval);
+		device_free(l.sptr);
+		device_free(l.sval);
+		for (int k = 0; k < 4; k++)
+			l.q_ge[k] = l.s_ge[k] = 0;
+	}
+	plan.dir_built = false;
 	plan.count = 0;
 }
 
 int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes, const ens_tuning& tune,
-				   const std::vector<std::pair<float*, float*>>* buffers, bool rebinned)
+				   const std::vector<std::pair<float*, float*>>* buffers, bool rebinned, bool faces)
 {
 	ensemble_free(plan);
 	plan.tune = tune;
@@ -616,6 +779,16 @@ int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes,
 		m.dir_idx = s->dir_idx;
 		m.dir_val = s->dir_val;
 		m.dir_count = s->dir_count;
+		const bool fp = faces && s->face_pos_ok && s->face_bits && s->face_vals_d;
+		m.faces = fp ? 1 : 0;
+		m.face_bits = fp ? s->face_bits : nullptr;
+		m.face_vals = fp ? s->face_vals_d : nullptr;
+		m.dir_iqidx = fp ? s->dir_interior.qidx : nullptr;
+		m.dir_iqval = fp ? s->dir_interior.qval : nullptr;
+		m.dir_iqcount = fp ? s->dir_interior.qcount : 0;
+		m.dir_iidx = fp ? s->dir_interior.idx : nullptr;
+		m.dir_ival = fp ? s->dir_interior.val : nullptr;
+		m.dir_icount = fp ? s->dir_interior.count : 0;
 		const agent_state& a = s->ag;
 		m.AS = (long long)a.count * s->S;
 		m.internalized = s->internalized ? 1 : 0;
@@ -698,13 +871,119 @@ static int launched(const char* what)
 	return e == cudaSuccess ? BFVM_OK : cuda_fail(e, what);
 }
 
-int ensemble_dirichlet(const ensemble_plan& plan, int phase, cudaStream_t stream)
+// Gather the lists `src` (meshes in the order of the flat list: qflat / sflat set) into `out`.
+static int flatten_lists(const std::vector<ens_dir_src>& src, ensemble_plan::flat_list& out, long long nq, long long ns)
 {
-	const long long units = plan.count ? plan.first_h[ENS_DIRICHLET][plan.count] : 0;
+	int st;
+	if ((st = device_alloc(&out.qptr, (size_t)std::max(nq, 1LL))) || (st = device_alloc(&out.qval, (size_t)std::max(nq, 1LL)))
+		|| (st = device_alloc(&out.sptr, (size_t)std::max(ns, 1LL))) || (st = device_alloc(&out.sval, (size_t)std::max(ns, 1LL))))
+		return st;
+	const int n = (int)src.size();
+	std::vector<long long> ufirst(n + 1, 0);
+	for (int i = 0; i < n; i++)
+		ufirst[i + 1] = ufirst[i] + (src[i].qcount + src[i].count + 255) / 256;
+	const long long units = ufirst[n];
 	if (units == 0)
 		return BFVM_OK;
-	ens_dirichlet_kernel<<<element_grid(units), 256, 0, stream>>>(plan.inst, plan.first[ENS_DIRICHLET],
-																   plan.unit_mesh[ENS_DIRICHLET], units, phase);
+	std::vector<int> um((size_t)units);
+	for (int i = 0; i < n; i++)
+		std::fill(um.begin() + ufirst[i], um.begin() + ufirst[i + 1], i);
+	ens_dir_src* src_d = nullptr;
+	long long* ufirst_d = nullptr;
+	int* um_d = nullptr;
+	if ((st = device_alloc(&src_d, (size_t)n)) || (st = device_alloc(&ufirst_d, (size_t)n + 1))
+		|| (st = device_alloc(&um_d, (size_t)units)))
+	{
+		device_free(src_d);
+		device_free(ufirst_d);
+		return st;
+	}
+	cudaError_t e = cudaMemcpy(src_d, src.data(), n * sizeof(ens_dir_src), cudaMemcpyHostToDevice);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(ufirst_d, ufirst.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice);
+	if (e == cudaSuccess)
+		e = cudaMemcpy(um_d, um.data(), units * sizeof(int), cudaMemcpyHostToDevice);
+	if (e == cudaSuccess)
+	{
+		ens_dirichlet_flatten_kernel<<<element_grid(units), 256>>>(src_d, ufirst_d, um_d, units, out.qptr, out.qval,
+																	out.sptr, out.sval);
+		e = cudaGetLastError();
+		if (e == cudaSuccess)
+			e = cudaStreamSynchronize(0);
+	}
+	device_free(src_d);
+	device_free(ufirst_d);
+	device_free(um_d);
+	return e == cudaSuccess ? BFVM_OK : cuda_fail(e, "ens_dirichlet_flatten_kernel");
+}
+
+int ensemble_build_dirichlet(ensemble_plan& plan)
+{
+	const int n = plan.count;
+	plan.dir_built = true;
+	if (n == 0)
+		return BFVM_OK;
+	std::vector<ens_inst> h(n);
+	BFVM_CUDA(cudaMemcpy(h.data(), plan.inst, n * sizeof(ens_inst), cudaMemcpyDeviceToHost));
+	for (int which = 0; which < 2; which++)
+	{
+		// meshes of 3, 2, then 1 dimensions; list 1 takes the interior elements alone where the
+		// sweeps write the faces
+		std::vector<ens_dir_src> src;
+		long long nq = 0, ns = 0;
+		ensemble_plan::flat_list& out = plan.dir[which];
+		for (int d = 3; d >= 0; d--)
+		{
+			for (int i = 0; i < n; i++)
+			{
+				const ens_inst& m = h[i];
+				if (m.dims != d)
+					continue;
+				const bool inner = which == 1 && m.faces;
+				ens_dir_src x;
+				x.dens = m.dens;
+				x.qidx = inner ? m.dir_iqidx : m.dir_qidx;
+				x.qval = inner ? m.dir_iqval : m.dir_qval;
+				x.qcount = inner ? m.dir_iqcount : m.dir_qcount;
+				x.idx = inner ? m.dir_iidx : m.dir_idx;
+				x.val = inner ? m.dir_ival : m.dir_val;
+				x.count = inner ? m.dir_icount : m.dir_count;
+				x.qflat = nq;
+				x.sflat = ns;
+				nq += x.qcount;
+				ns += x.count;
+				src.push_back(x);
+			}
+			out.q_ge[d] = nq;
+			out.s_ge[d] = ns;
+		}
+		int st;
+		if ((st = flatten_lists(src, out, nq, ns)))
+			return st;
+	}
+	return BFVM_OK;
+}
+
+long long ensemble_dirichlet_entries(const ensemble_plan& plan, int phase)
+{
+	const int k = std::min(std::max(phase, 0), 3);
+	const ensemble_plan::flat_list& l = plan.dir[k == 0 ? 0 : 1];
+	return l.q_ge[k] + l.s_ge[k];
+}
+
+int ensemble_dirichlet(const ensemble_plan& plan, int phase, cudaStream_t stream)
+{
+	const int k = std::min(std::max(phase, 0), 3);
+	if (!plan.dir_built && plan.count && plan.first_h[ENS_DIRICHLET][plan.count] > 0)
+		return fail(BFVM_ERR_STATE, "ensemble Dirichlet lists not built");
+	const ensemble_plan::flat_list& l = plan.dir[k == 0 ? 0 : 1];
+	const long long nq = l.q_ge[k], ns = l.s_ge[k];
+	if (nq + ns == 0)
+		return BFVM_OK;
+	// four entries per thread, at most 8 CTAs of 256 per SM
+	const long long blocks = (std::max(nq, ns) + 1023) / 1024;
+	const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, (long long)current_device_sms() * 8));
+	ens_dirichlet_kernel<<<grid, 256, 0, stream>>>(l.qptr, l.qval, nq, l.sptr, l.sval, ns);
 	return launched("ens_dirichlet_kernel");
 }
 

@@ -28,6 +28,18 @@ struct ens_inst
 	const long long* dir_idx; // single elements
 	const float* dir_val;
 	long long dir_count;
+	// faces by position (dirichlet.cu, face_pos_ok): each sweep writes the face conditions into the
+	// values it stores, so the overwrites after the sweeps take only the interior list (dir_i*).
+	// face_bits[s]: bit f when face f conditions substrate s; face_vals [6][S].  faces 0: none.
+	int faces;
+	const int* face_bits;
+	const float* face_vals;
+	const long long* dir_iqidx;
+	const float4* dir_iqval;
+	long long dir_iqcount;
+	const long long* dir_iidx;
+	const float* dir_ival;
+	long long dir_icount;
 	// secretion (the binning of the mesh's cell solver).  sorted: num/den/fac/intern are the agent
 	// terms in the binning's sorted order (agent_state::snum ...), else in agent order; vec4: sorted
 	// with S % 4 == 0, a unit is 256 (segment, four substrates) pairs
@@ -83,6 +95,22 @@ struct ensemble_plan
 	size_t table_floats[3] = { 0, 0, 0 }; // largest staged table per axis
 	bool all3d = true;					  // every mesh is 3-D (the gradient kernel without the 1-D/2-D forms)
 	ens_tuning tune;					  // launch choices (the gradient units follow tune.grad_zc)
+	// the Dirichlet overwrites of every mesh as flat lists of (address, value), runs of four and
+	// single elements (ensemble_build_dirichlet; device).  List 0 holds every mesh's whole list, for
+	// the overwrite before the x sweep; list 1 the lists of the overwrites after the sweeps (the
+	// interior elements alone for meshes whose sweeps write the faces).  Meshes of more dimensions
+	// come first, so that overwrite k covers the meshes with dims >= k: the first q_ge[k] / s_ge[k]
+	// entries.
+	struct flat_list
+	{
+		float4** qptr = nullptr;
+		float4* qval = nullptr;
+		float** sptr = nullptr;
+		float* sval = nullptr;
+		long long q_ge[4] = { 0, 0, 0, 0 }, s_ge[4] = { 0, 0, 0, 0 };
+	};
+	flat_list dir[2];
+	bool dir_built = false;
 };
 
 // Which meshes the ensemble kernels cover: every axis with n >= 2 and at most ENS_MAX_P blocks,
@@ -91,13 +119,21 @@ bool ensemble_eligible(const bfvm_solver* s);
 // buffers: when given, the field and gradient buffers of each mesh instead of the solvers' own
 // (the autotuner times candidates on scratch copies).  rebinned: the secretion update runs after
 // a rebinning of every mesh with agents (prepare_agent_terms), so it finds their agent terms in
-// the order that leaves (sorted with internalized substrates) rather than in today's.
+// the order that leaves (sorted with internalized substrates) rather than in today's.  faces: the
+// sweeps write the face conditions of the meshes that allow it (a batch step; the plan then holds
+// pointers to the members' Dirichlet tables and is rebuilt whenever they change).
 int ensemble_build(ensemble_plan& plan, const std::vector<bfvm_solver*>& meshes, const ens_tuning& tune = ens_tuning(),
-				   const std::vector<std::pair<float*, float*>>* buffers = nullptr, bool rebinned = false);
+				   const std::vector<std::pair<float*, float*>>* buffers = nullptr, bool rebinned = false,
+				   bool faces = false);
 void ensemble_free(ensemble_plan& plan);
+// The flat Dirichlet lists of a built plan, for ensemble_dirichlet (complete on return; never
+// inside a stream capture).
+int ensemble_build_dirichlet(ensemble_plan& plan);
 // One phase for every mesh of the plan, on `stream`.  `dirichlet_phase` k applies the overwrite to
-// meshes with k <= dims (before sweep k, or after the last sweep).
+// meshes with k <= dims (before sweep k, or after the last sweep); it launches nothing when
+// ensemble_dirichlet_entries is 0.
 int ensemble_dirichlet(const ensemble_plan& plan, int dirichlet_phase, cudaStream_t stream);
+long long ensemble_dirichlet_entries(const ensemble_plan& plan, int dirichlet_phase);
 int ensemble_sweep(const ensemble_plan& plan, int axis, cudaStream_t stream);
 // whether the ensemble sweep of `axis` fits the shared memory of a CTA on this device
 bool ensemble_sweep_fits(const ensemble_plan& plan, int axis);

@@ -170,3 +170,34 @@ def test_batch_members_changed_between_steps():
     b.close()
     for s in solvers + ref:
         s.close()
+
+
+def test_batch_faces_written_by_the_sweeps():
+    """The ensemble sweeps write the face conditions of each mesh whose interior Dirichlet voxels
+    stay off the faces, and the overwrites after them take only the interior elements.  Meshes with
+    a different value on every (face, substrate), random subsets of conditioned substrates per
+    face (so every precedence case where faces meet occurs), interior voxels on the faces (that
+    mesh keeps its whole list), lines that straddle tiles, 2-D and 1-D: each ends bit for bit where
+    the same solver stepped alone ends."""
+    from test_gpu_faces import _faces_workload
+
+    ws = [_faces_workload((24, 20, 18), 4, 3, seed=1), _faces_workload((30, 26, 22), 16, 3, seed=2),
+          _faces_workload((36, 36, 36), 8, 3, seed=3, interior_on_faces=True),
+          _faces_workload((70, 33, 20), 5, 3, seed=4), _faces_workload((40, 30, 1), 6, 2, seed=5),
+          _faces_workload((50, 1, 1), 3, 1, seed=6)]
+    alone = []
+    for w in ws:
+        s = make_solver(w)
+        s.run_steps(4, 0)
+        alone.append(_state(s))
+        s.close()
+    solvers = [make_solver(w) for w in ws]
+    b = Batch(solvers)
+    b.run_steps(4, 0)
+    b.synchronize()
+    for i, s in enumerate(solvers):
+        for g, a in zip(_state(s), alone[i]):
+            np.testing.assert_array_equal(g, a, err_msg=f"instance {i}")
+    b.close()
+    for s in solvers:
+        s.close()
