@@ -663,32 +663,50 @@ __global__ void __launch_bounds__(MINB == 0 ? 1024 : 512, MINB == 0 ? 1 : MINB) 
 					if (r >= 0)
 						line[r * stride] = d[k];
 				}
-				// the face conditions of the overwrite after this sweep (meshes with ens_inst::faces)
+				// the face conditions of the overwrite after this sweep (meshes with ens_inst::faces):
+				// the ends of the line from the faces of AXIS, and, on tiles that reach a face of
+				// another axis (a test on the tile's first line), the whole line from that face
 				const int mb = reinterpret_cast<const int*>(ctab + S)[s];
 				if (mb != 0)
 				{
-					int cx = 0, cy = 0, cz = 0;
-					if (AXIS == 0)
+					int code = ((mb >> (2 * AXIS)) & 3) << 2;
+					if (mb & ~(3 << (2 * AXIS)))
 					{
-						const int row = local * (32 / S) + lane / S;
-						cz = row / m.Y;
-						cy = row - cz * m.Y;
+						bool touch;
+						int cx = 0, cy = 0, cz = 0;
+						if (AXIS == 0)
+						{
+							// x tiles: each line placed directly (the tile test would cost the kernel spills)
+							touch = true;
+							const int row = local * (32 / S) + lane / S;
+							cz = row / m.Y;
+							cy = row - cz * m.Y;
+						}
+						else if (AXIS == 1)
+						{
+							const int col_tiles = (XS + 31) / 32;
+							const int z = local / col_tiles, c0 = (local - z * col_tiles) * 32;
+							touch = z == 0 || z == m.Z - 1 || c0 < S || c0 + 31 >= XS - S;
+							if (touch)
+							{
+								cz = z;
+								cx = (c0 + lane) / S;
+							}
+						}
+						else
+						{
+							const int q0 = local * 32, y0 = q0 / XS, r0 = q0 - y0 * XS;
+							touch = y0 == 0 || q0 + 31 >= (m.Y - 1) * XS || r0 < S || r0 + 31 >= XS - S;
+							if (touch)
+							{
+								const int q = q0 + lane;
+								cy = q / XS;
+								cx = (q - cy * XS) / S;
+							}
+						}
+						if (touch)
+							code = ens_face_code<AXIS>(mb, cx, cy, cz, m.X, m.Y, m.Z);
 					}
-					else if (AXIS == 1)
-					{
-						// line = dens + z * XS * Y + x * S + s
-						const int off = (int)(line - m.dens);
-						const int plane = XS * m.Y;
-						cz = off / plane;
-						cx = (off - cz * plane) / S;
-					}
-					else
-					{
-						const int q = local * 32 + lane;
-						cy = q / XS;
-						cx = (q - cy * XS) / S;
-					}
-					const int code = ens_face_code<AXIS>(mb, cx, cy, cz, m.X, m.Y, m.Z);
 					if (code != 0)
 						ens_store_faces<AXIS>(line, stride, code, ctab + 2 * S, S, s, j, P, pad);
 				}
