@@ -229,28 +229,39 @@ __device__ __forceinline__ void ens_gradient_3d(const ens_inst& m, const float* 
 
 // The z march of a 3-D mesh of 4k substrates, four substrates per thread (gradient3d_vec4_kernel of
 // gradient.cu): p4 and g4 point at plane z0 of the thread's float4 column; neighbour offsets in
-// float4s.  The same arithmetic per element as the scalar march, so the same bits.
+// float4s.  The loads of the next D planes are kept in flight ahead of the plane being written
+// (a ring of D registers, shifted and refilled as each plane is used), so D planes of each thread
+// stream from memory at once; the x and y neighbours, cache hits mostly, are loaded plane by plane.  The same arithmetic per element as the scalar march, so the same bits.
 __device__ __forceinline__ float4 ens_f4sub_mul(float4 a, float4 b, float f)
 {
 	return make_float4(__fmul_rn(__fsub_rn(a.x, b.x), f), __fmul_rn(__fsub_rn(a.y, b.y), f),
 					   __fmul_rn(__fsub_rn(a.z, b.z), f), __fmul_rn(__fsub_rn(a.w, b.w), f));
 }
 
+template <int D>
 __device__ __forceinline__ void ens_gradient_3d_vec4(const ens_inst& m, const float4* __restrict__ p4,
-													 float4* __restrict__ g4, long long plane4, int z0, int z1,
-													 long long xlo, long long xhi, float fx, long long ylo,
-													 long long yhi, float fy)
+													 float4* __restrict__ g4, int plane4, int z0, int z1, int xlo,
+													 int xhi, float fx, int ylo, int yhi, float fy)
 {
+	// offsets in float4s fit 31 bits: a mesh's elements do (ensemble_eligible)
 	const int Z = m.Z;
-	const long long total4 = plane4 * Z;
+	const int total4 = plane4 * Z;
 	const bool hasx = m.X > 1, hasy = m.Y > 1;
 	const float bz = m.bgrad[2], cz = m.cgrad[2];
 	const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
 	float4 prev = z0 > 0 ? __ldg(p4 - plane4) : zero;
 	float4 cur = __ldg(p4);
+	// ring[k]: plane z + 1 + k (the planes up to z1, the last plane's next, and no further)
+	float4 ring[D];
+#pragma unroll
+	for (int k = 0; k < D; k++)
+	{
+		const int zz = z0 + 1 + k;
+		ring[k] = (zz < Z && zz <= z1) ? __ldg(p4 + (k + 1) * plane4) : zero;
+	}
 	for (int z = z0; z < z1; z++)
 	{
-		const float4 next = z + 1 < Z ? __ldg(p4 + plane4) : cur;
+		const float4 next = z + 1 < Z ? ring[0] : cur;
 		const float4 gx = hasx ? ens_f4sub_mul(__ldg(p4 + xhi), __ldg(p4 + xlo), fx) : zero;
 		const float4 gy = hasy ? ens_f4sub_mul(__ldg(p4 + yhi), __ldg(p4 + ylo), fy) : zero;
 		float4 gz;
@@ -265,6 +276,11 @@ __device__ __forceinline__ void ens_gradient_3d_vec4(const ens_inst& m, const fl
 		__stcs(g4, gx);
 		__stcs(g4 + total4, gy);
 		__stcs(g4 + 2 * total4, gz);
+#pragma unroll
+		for (int k = 0; k + 1 < D; k++)
+			ring[k] = ring[k + 1];
+		const int zz = z + 1 + D;
+		ring[D - 1] = (zz < Z && zz <= z1) ? __ldg(p4 + (1 + D) * plane4) : zero;
 		prev = cur;
 		cur = next;
 		p4 += plane4;
@@ -301,14 +317,15 @@ __global__ void __launch_bounds__(256, ALL3D ? 4 : 2) ens_gradient_kernel(const 
 			const int y = c4 / XS4;
 			const int q4 = c4 - y * XS4;
 			const int x = q4 / S4;
-			const long long plane4 = (long long)cols4;
+			const int plane4 = cols4;
 			long long xlo, xhi, ylo, yhi;
 			float fx, fy;
 			axis_form(x, X, S4, m.bgrad[0], m.cgrad[0], xlo, xhi, fx);
 			axis_form(y, Y, XS4, m.bgrad[1], m.cgrad[1], ylo, yhi, fy);
-			const long long e4 = (long long)z0 * plane4 + c4;
-			ens_gradient_3d_vec4(m, reinterpret_cast<const float4*>(m.dens) + e4, reinterpret_cast<float4*>(m.grad) + e4,
-								 plane4, z0, min(Z, z0 + ZC), xlo, xhi, fx, ylo, yhi, fy);
+			const int e4 = z0 * plane4 + c4;
+			ens_gradient_3d_vec4<2>(m, reinterpret_cast<const float4*>(m.dens) + e4,
+										 reinterpret_cast<float4*>(m.grad) + e4, plane4, z0, min(Z, z0 + ZC), (int)xlo,
+										 (int)xhi, fx, (int)ylo, (int)yhi, fy);
 			continue;
 		}
 		const int plane_cols = XS * Y;
