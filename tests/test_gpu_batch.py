@@ -201,3 +201,32 @@ def test_batch_faces_written_by_the_sweeps():
     b.close()
     for s in solvers:
         s.close()
+
+
+def test_all_3d_batch_matches_each_solver_alone():
+    """A batch of 3-D meshes only runs the gradient kernel without the 1-D and 2-D forms (the
+    batch-256 case): meshes of 1 to 8 substrates (the four-substrate march and the one-element
+    march), z extents that do not divide the planes per work unit, agents binned on a recompute
+    step; each ends bit for bit where the same solver stepped alone ends."""
+    ws = [synthetic(24, 3, 300, seed=11, clustered=True, sigma=50.0, interior_fraction=0.02),
+          synthetic(37, 5, 800, seed=12, clustered=True, sigma=80.0),
+          synthetic(50, 4, 2000, seed=13, interior_fraction=0.01),
+          synthetic(33, 1, 500, seed=14, internalized=False),
+          synthetic(70, 7, 3000, seed=15, clustered=True, sigma=60.0),
+          synthetic(45, 8, 60, seed=16)]
+    alone = []
+    for w in ws:
+        s = make_solver(w)
+        s.run_steps(12, 0)
+        alone.append(_state(s))
+        s.close()
+    solvers = [make_solver(w) for w in ws]
+    b = Batch(solvers)
+    b.run_steps(12, 0)
+    b.synchronize()
+    for i, s in enumerate(solvers):
+        for g, a in zip(_state(s), alone[i]):
+            np.testing.assert_array_equal(g, a, err_msg=f"instance {i}")
+    b.close()
+    for s in solvers:
+        s.close()
